@@ -1,0 +1,345 @@
+"""Benchmark of GALIC's orbit-response hot path on B200.
+
+One step = one calc_all_response_fields pass (main.c:151-246 + calc_global_fit
+main.c:251-362) over a whole seeded synthetic model of the halo + disk shape
+(Hernquist halo M=95, a=30 kpc, N=1e6; exponential disk M=5, h=3.5 kpc,
+z0=0.7 kpc, N=2e5; 128x128 response grid; 256x256 force grid): every
+particle's orbit is integrated for Tint and binned into the per-type response
+grids, then the merit function is evaluated.  The metric is orbit-steps/s
+(one step = one iteration of orbit_response.c:211-458).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs its own model (weak scaling: models are
+independent), rank 0 prints one JSON line.  --impl reference times GALIC's
+own C (oracle/_ref/libgalic_ref.so, else the C restatement) on the host cores.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "orbit-steps/s (FP32 batched vs FP64 plain, same χ²); p50/p99 model latency"
+FLOP_PER_STEP = 365  # algorithmic FP ops per orbit-step (orbit_response.c:211-458 and callees)
+WORKLOAD = "halo+disk: Hernquist halo M=95 a=30 N=1e6 + exp disk M=5 h=3.5 z0=0.7 N=2e5, 128x128 DG/EG, 256^2 FG"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's particle count")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def build_workload(scale, seed):
+    from galic_b200 import synth
+
+    nh = max(int(1_000_000 * scale), 40)
+    nd = max(int(200_000 * scale), 20)
+    return synth.config_halo_disk(n_halo=nh, n_disk=nd, level=7, seed=seed)
+
+
+# ------------------------------------------------------------------ CPU side
+
+
+def _cpu_worker(args):
+    """Integrates orbits of one chunk with GALIC's own C (or the restatement)."""
+    arrays, idx, seconds, kind = args
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import oracle_lib
+    from make_golden import model_from_arrays
+
+    m = model_from_arrays(arrays)
+    runner = oracle_lib.Reference(m.params) if kind == "reference" else oracle_lib.Oracle(m.params, use_libm=True)
+    runner.load_model(m, particles=False)
+    done = []
+    t0 = time.perf_counter()
+    for i in idx:
+        runner.orbit_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])
+        done.append(i)
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    # step counts: the restatement with glibc math follows the same trajectory
+    # bit for bit, and returns its step count
+    counter = oracle_lib.Oracle(m.params, use_libm=True)
+    counter.load_model(m, particles=False)
+    steps = 0
+    for i in done:
+        steps += int(counter.orbit_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])[7][0])
+    return steps, dt, len(done)
+
+
+def cpu_orbit_steps_per_s(model, seconds, cores=None):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import oracle_lib
+    from make_golden import model_arrays
+
+    kind = "reference" if oracle_lib.reference_available() else "port"
+    cores = cores or os.cpu_count() or 1
+    arrays = model_arrays(model)
+    rng = np.random.default_rng(123)
+    perm = rng.permutation(model.n)
+    chunks = [perm[k::cores][:20000] for k in range(cores)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(arrays, c, seconds, kind) for c in chunks])
+    steps = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    orbits = sum(r[2] for r in res)
+    return steps / wall, kind, cores, orbits, steps
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------ clocks
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_fp64_peak(torch):
+    """FP64 GEMM TFLOP/s (burst, best of 5) on this GPU: the FP64 denominator."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+# ------------------------------------------------------------------ arms
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+
+    model = build_workload(args.scale, seed=2)
+    per_step = max(args.cpu_seconds / 3.0, 2.0)
+    vals = []
+    kind = cores = None
+    for k in range(args.warmup + args.steps):
+        v, kind, cores, orbits, steps = cpu_orbit_steps_per_s(model, per_step)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    sample = f"{orbits} orbits of the workload per step, {cores} processes x {per_step:.1f} s"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "orbit-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": f"{cores} host processes"},
+            "cpu_baseline": {"value": value, "unit": "orbit-steps/s", "cores": cores,
+                             "kind": "reference" if kind == "reference" else "port", "sample": sample,
+                             "cpu": cpu_model()},
+            "e2e": {"value": value, "unit": "orbit-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours_arm(args, rank, world, local_rank):
+    import torch
+
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64, Context
+    from galic_b200 import _ffi
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    form = GALIC_FORM_FP64 if args.form == "fp64" else GALIC_FORM_FP32
+    model = build_workload(args.scale, seed=2 + rank)
+    ctx = Context(model.params)
+    ctx.load_model(model)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    for _ in range(args.warmup):
+        ctx.calc_all_response_fields(form)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    dev_ms, kern_ms, steps, launches = [], [], [], 0
+    with ClockSampler(local_rank) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ctx.calc_all_response_fields(form)
+            tot, kern = ctx.last_timing()
+            dev_ms.append(tot)
+            kern_ms.append(kern)
+            steps.append(ctx.last_orbit_steps())
+            launches += ctx.last_kernel_launches()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    total_ms = sum(dev_ms)
+    total_steps = sum(steps)
+    # whole job: steps of all ranks over the slowest rank's device time
+    if dist:
+        t = torch.tensor([total_ms, float(total_steps)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms, total_steps = float(mx[0]), float(t[1])
+    value = total_steps / (total_ms * 1e-3)
+
+    # end to end through the C ABI with host buffers: upload the particle state,
+    # run the pass, read back the fit and every committed grid
+    e2e_s = []
+    h2d = sum(a.nbytes for a in (model.pos, model.vel, model.mass, model.tint, model.vesc, model.ptype,
+                                 model.ptargets))
+    types = [t for t in (1, 2, 3) if model.params.NType[t]]
+    d2h = 28 * 8 + len(types) * _ffi.GRID_COUNT * ctx.ngrid * 8
+    for _ in range(max(1, min(args.steps, 2))):
+        t1 = time.perf_counter()
+        ctx.set_particles(model.pos, model.vel, model.mass, model.tint, model.vesc, model.ptype, model.ptargets)
+        ctx.calc_all_response_fields(form)
+        ctx.fit()
+        for t in types:
+            for w in range(_ffi.GRID_COUNT):
+                ctx.response(t, w)
+        e2e_s.append(time.perf_counter() - t1)
+    e2e_value = steps[-1] * (world if dist else 1) / statistics.mean(e2e_s)
+
+    if rank == 0:
+        peak = measured_fp64_peak(torch)
+        kern_avg = sum(kern_ms) / len(kern_ms)
+        achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
+        cpu = None
+        if world == 1:
+            v, kind, cores, orbits, st = cpu_orbit_steps_per_s(model, args.cpu_seconds)
+            cpu = {"value": v, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
+                   "sample": f"{orbits} orbits ({st} orbit-steps) of this workload, {cores} processes, "
+                             f"~{args.cpu_seconds:.0f} s each", "cpu": cpu_model()}
+        line = {"metric": METRIC, "value": value, "unit": "orbit-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if form == GALIC_FORM_FP64 else "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "form": args.form, "particles_per_gpu": model.n,
+                           "orbit_steps_per_step": steps[-1], "l2": "flushed (256 MiB write) between steps",
+                           "parallelism": f"{world} independent models (one per GPU)"},
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "peak_source": "measured FP64 GEMM (torch.matmul float64 4096^3, burst); "
+                                            "MEASURED_PEAKS.json has no FP64 figure",
+                             "flop_per_orbit_step": FLOP_PER_STEP, "kernel": "k_calc_all_fp64",
+                             "kernel_ms": kern_avg},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches,
+                "clocks": clocks.summary(),
+                "wall_s": wall,
+                "max_energy_error": ctx.last_max_energy_error()}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    ours_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

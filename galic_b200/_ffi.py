@@ -1,0 +1,133 @@
+"""ctypes view of the C ABI in include/galic_gpu.h.
+
+`GalicParams` mirrors `galic_params_t` field for field; `load_library()`
+opens the in-tree libgalic_cuda.so and declares every entry point.  There is
+no fallback: if the library is missing the import fails with the build
+command to run.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgalic_cuda.so")
+
+GALIC_FORM_FP64 = 0
+GALIC_FORM_FP32 = 1
+
+# galic_grid_id
+GRID_MASS_S, GRID_R_S, GRID_T_S, GRID_Q_S, GRID_P_S = 0, 1, 2, 3, 4
+GRID_MASS_I, GRID_R_I, GRID_T_I, GRID_P_I, GRID_Q_I = 5, 6, 7, 8, 9
+GRID_COUNT = 10
+
+STATUS_NAMES = {
+    0: "GALIC_OK", 1: "GALIC_ERR_INVALID_ARGUMENT", 2: "GALIC_ERR_STEP_CAP", 3: "GALIC_ERR_CUDA",
+    4: "GALIC_ERR_NO_DEVICE", 5: "GALIC_ERR_BUDGET", 6: "GALIC_ERR_UNSUPPORTED",
+    7: "GALIC_ERR_REJECTION_CAP", 8: "GALIC_ERR_OVERFLOW", 9: "GALIC_ERR_STATE",
+}
+
+D4 = C.c_double * 4
+I4 = C.c_int * 4
+
+
+class GalicParams(C.Structure):
+    _fields_ = [
+        ("V200", C.c_double), ("M200", C.c_double), ("R200", C.c_double), ("G", C.c_double),
+        ("Halo_Mass", C.c_double), ("Halo_A", C.c_double), ("HaloStretch", C.c_double),
+        ("Disk_Mass", C.c_double),
+        ("Bulge_Mass", C.c_double), ("Bulge_A", C.c_double), ("BulgeStretch", C.c_double),
+        ("TimeStepFactorOrbit", C.c_double), ("TimeStepFactorCellCross", C.c_double),
+        ("LowerDispLimit", C.c_double), ("MaxVelInUnitsVesc", C.c_double),
+        ("SampleForceNhalo", C.c_int), ("SampleForceNdisk", C.c_int), ("SampleForceNbulge", C.c_int),
+        ("TypeOfVelocityStructure", I4),
+        ("MinParticlesPerBinForDispersionMeasurement", C.c_int),
+        ("MinParticlesPerBinForDensityMeasurement", C.c_int),
+        ("MType", D4), ("NType", I4),
+        ("fac_value_rs", D4), ("fac_value_ts", D4), ("fac_value_qs", D4), ("fac_value_ps", D4),
+        ("FG_Nbin", C.c_int), ("DG_MaxLevel", C.c_int), ("EG_MaxLevel", C.c_int),
+        ("FG_Rmin", C.c_double), ("FG_Fac", C.c_double), ("DG_Rmin", C.c_double),
+        ("DG_Fac", C.c_double), ("EG_Rmin", C.c_double), ("EG_Fac", C.c_double),
+    ]
+
+    def copy(self):
+        other = GalicParams()
+        C.memmove(C.byref(other), C.byref(self), C.sizeof(GalicParams))
+        return other
+
+
+def dptr(a):
+    """double* of a C-contiguous float64 numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "need C-contiguous float64"
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"], "need C-contiguous int32"
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def llptr(a):
+    assert a.dtype == np.int64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_longlong))
+
+
+PD = C.POINTER(C.c_double)
+PI = C.POINTER(C.c_int)
+PLL = C.POINTER(C.c_longlong)
+VP = C.c_void_p
+
+# (name, restype, argtypes) for every symbol of include/galic_gpu.h
+SIGNATURES = [
+    ("galic_ctx_create", C.c_int, [C.POINTER(GalicParams), C.POINTER(VP)]),
+    ("galic_ctx_destroy", None, [VP]),
+    ("galic_last_status", C.c_int, [VP]),
+    ("galic_status_string", C.c_char_p, [C.c_int]),
+    ("galic_set_force_grid", C.c_int, [VP, PD, PD, PD]),
+    ("galic_set_vstream", C.c_int, [VP, C.c_int, PD]),
+    ("galic_set_density_geometry", C.c_int, [VP, PD, PD]),
+    ("galic_set_targets", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD, PD]),
+    ("galic_set_particles", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD, PI, PD]),
+    ("galic_get_particles", C.c_int, [VP, PD, PI, PD]),
+    ("galic_produce_orbit_response_field_mod", C.c_double,
+     [VP, PD, PD, C.c_int, PD, PD, PD, PD, PD, C.c_double, C.c_double, PI, C.c_int]),
+    ("galic_produce_orbit_response_field", C.c_double, [VP, PD, PD, C.c_int, PD, C.c_double, C.c_double, PI]),
+    ("galic_calc_all_response_fields", C.c_int, [VP, C.c_int]),
+    ("galic_optimize_rep", C.c_int, [VP, PI, C.c_int, C.c_uint64, C.c_uint32, C.c_int]),
+    ("galic_get_fit", C.c_int, [VP, PD]),
+    ("galic_get_counters", C.c_int, [VP, PLL, PLL]),
+    ("galic_get_response", C.c_int, [VP, C.c_int, C.c_int, PD]),
+    ("galic_set_step_cap", C.c_int, [VP, C.c_longlong]),
+    ("galic_last_orbit_steps", C.c_longlong, [VP]),
+    ("galic_last_timing", C.c_int, [VP, PD, PD]),
+    ("galic_last_max_energy_error", C.c_double, [VP]),
+    ("galic_last_kernel_launches", C.c_int, [VP]),
+    ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
+    ("galic_density_geometry", C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
+    ("galic_smooth_stack", None, [PD, C.c_int]),
+]
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Open libgalic_cuda.so and declare its entry points (no fallback)."""
+    global _lib
+    if _lib is not None and path == LIB_PATH:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+            "(there is no CPU fallback for the GALIC orbit-response path)")
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path == LIB_PATH:
+        _lib = lib
+    return lib

@@ -1,0 +1,750 @@
+// C ABI of libgalic_cuda.so (include/galic_gpu.h): the context that replaces
+// GALIC's globals, uploads, and the entry points that replace the reference
+// functions.  Host code only; the kernels live in orbit_fp64.cu and
+// fit_fp64.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "galic_gpu.h"
+#include "kernels.cuh"
+#include "rep.cuh"
+
+struct galic_ctx {
+  galic_params_t prm;
+  int status = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevModel dm{};
+  int G = 0, Ns = 0, L = 0;
+  // tables
+  double2 *d_fg_acc = nullptr;
+  double *d_fg_pot = nullptr, *d_vstream[4] = {nullptr, nullptr, nullptr, nullptr};
+  double *d_cellsize = nullptr, *d_dist = nullptr;
+  double *d_targets = nullptr;    // [4][6][Ns]
+  double *d_committed = nullptr;  // [4][10][G]
+  double *d_stacks = nullptr;     // [4][10][Ns]
+  FxWord *d_fx = nullptr;         // [4][10][G]
+  int *d_shift = nullptr;         // [4][10]
+  double *d_fit = nullptr;        // [4][7] + raw [4][5]
+  int *d_firstrun = nullptr;      // [4]
+  unsigned long long *d_counters = nullptr;  // tries[4], changes[4], steps
+  int *d_status = nullptr;
+  int *d_next = nullptr;
+  double *d_maxerr = nullptr;
+  double pot_min = 0;
+  bool have_fg = false, have_geom = false, have_response = false;
+  bool have_targets[4] = {false, false, false, false};
+  // particles
+  int n = 0;
+  double *d_pos = nullptr, *d_vel = nullptr, *d_mass = nullptr, *d_tint = nullptr, *d_vesc = nullptr;
+  double *d_ptargets = nullptr, *d_vdisp = nullptr;
+  int *d_type = nullptr, *d_orbits = nullptr;
+  // scratch of the per-orbit drop-ins and the repetition
+  int scratch_orbits = 0;
+  double *d_b_pos = nullptr, *d_b_vel = nullptr, *d_b_mass = nullptr, *d_b_time = nullptr, *d_grids = nullptr;
+  double *d_b_tall = nullptr, *d_b_err = nullptr;
+  int *d_b_type = nullptr, *d_b_norbit = nullptr, *d_b_status = nullptr;
+  long long *d_b_steps = nullptr;
+  int scratch_rep = 0;
+  int *d_idx = nullptr, *d_accepted = nullptr;
+  double *d_vel_try = nullptr, *d_F = nullptr, *d_inst_v = nullptr;
+  Cell *d_inst_cell = nullptr;
+  // diagnostics
+  long long last_steps = 0;
+  int last_launches = 0;
+  double last_max_egy_err = 0;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double last_ms_total = 0, last_ms_orbit = 0;
+};
+
+namespace {
+
+const char *kStatusText[] = {"ok",
+                             "invalid argument",
+                             "an orbit exceeded the step cap",
+                             "CUDA runtime error",
+                             "no CUDA device",
+                             "request exceeds the HBM budget",
+                             "configuration not supported",
+                             "velocity proposal exceeded 100000 tries",
+                             "fixed-point response bin out of range",
+                             "call out of order"};
+
+int fail(galic_ctx *c, int st)
+{
+  if(c) c->status = st;
+  return st;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if(e_ != cudaSuccess) {                                                                       \
+      fprintf(stderr, "galic_cuda: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                          \
+      return fail(ctx, GALIC_ERR_CUDA);                                                           \
+    }                                                                                             \
+  } while(0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count)
+{
+  return cudaMalloc((void **) p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+template <class T>
+void dfree(T *&p)
+{
+  if(p) cudaFree((void *) p);
+  p = nullptr;
+}
+
+int stack_size(int L) { return ((1 << (2 + 2 * L)) - 1) / 3; }
+
+int check_params(const galic_params_t *p)
+{
+  if(!p) return GALIC_ERR_INVALID_ARGUMENT;
+  if(p->FG_Nbin < 2 || p->DG_MaxLevel < 1 || p->EG_MaxLevel < 1) return GALIC_ERR_INVALID_ARGUMENT;
+  // eval_fit_mod indexes energy stacks with DG_MaxLevel (main.c:1056) and the
+  // stacks are kept in one CTA's shared memory
+  if(p->DG_MaxLevel != p->EG_MaxLevel || p->DG_MaxLevel > 7) return GALIC_ERR_UNSUPPORTED;
+  if(!(p->FG_Rmin > 0) || !(p->FG_Fac > 1) || !(p->DG_Rmin > 0) || !(p->DG_Fac > 1) || !(p->EG_Rmin > 0) ||
+     !(p->EG_Fac > 1))
+    return GALIC_ERR_INVALID_ARGUMENT;
+  for(int t = 1; t <= 3; t++)
+    if(p->TypeOfVelocityStructure[t] < 0 || p->TypeOfVelocityStructure[t] > 3) return GALIC_ERR_INVALID_ARGUMENT;
+  // grid.c:96-97 and 174-175: analytic components must be spherical
+  if(p->Halo_Mass > 0 && p->SampleForceNhalo == 0 && p->HaloStretch != 1.0) return GALIC_ERR_UNSUPPORTED;
+  if(p->Bulge_Mass > 0 && p->SampleForceNbulge == 0 && p->BulgeStretch != 1.0) return GALIC_ERR_UNSUPPORTED;
+  if(!(p->Halo_Mass > 0)) return GALIC_ERR_UNSUPPORTED;  // off-grid fallback divides by Halo_Mass
+  return GALIC_OK;
+}
+
+int ensure_orbit_scratch(galic_ctx *ctx, int count)
+{
+  if(count <= ctx->scratch_orbits) return GALIC_OK;
+  dfree(ctx->d_b_pos); dfree(ctx->d_b_vel); dfree(ctx->d_b_mass); dfree(ctx->d_b_time); dfree(ctx->d_grids);
+  dfree(ctx->d_b_tall); dfree(ctx->d_b_err); dfree(ctx->d_b_type); dfree(ctx->d_b_norbit); dfree(ctx->d_b_status);
+  dfree(ctx->d_b_steps);
+  CK(dalloc(&ctx->d_b_pos, 3 * (size_t) count));
+  CK(dalloc(&ctx->d_b_vel, 3 * (size_t) count));
+  CK(dalloc(&ctx->d_b_mass, count));
+  CK(dalloc(&ctx->d_b_time, count));
+  CK(dalloc(&ctx->d_grids, (size_t) count * NF_ORBIT * ctx->G));
+  CK(dalloc(&ctx->d_b_tall, count));
+  CK(dalloc(&ctx->d_b_err, count));
+  CK(dalloc(&ctx->d_b_type, count));
+  CK(dalloc(&ctx->d_b_norbit, count));
+  CK(dalloc(&ctx->d_b_status, count));
+  CK(dalloc(&ctx->d_b_steps, count));
+  ctx->scratch_orbits = count;
+  return GALIC_OK;
+}
+
+int ensure_rep_scratch(galic_ctx *ctx, int count)
+{
+  int st = ensure_orbit_scratch(ctx, 2 * count);
+  if(st) return st;
+  if(count <= ctx->scratch_rep) return GALIC_OK;
+  dfree(ctx->d_idx); dfree(ctx->d_accepted); dfree(ctx->d_vel_try); dfree(ctx->d_F); dfree(ctx->d_inst_v);
+  dfree(ctx->d_inst_cell);
+  CK(dalloc(&ctx->d_idx, count));
+  CK(dalloc(&ctx->d_accepted, count));
+  CK(dalloc(&ctx->d_vel_try, 3 * (size_t) count));
+  CK(dalloc(&ctx->d_F, 2 * (size_t) count));
+  CK(dalloc(&ctx->d_inst_v, 4 * (size_t) count));
+  CK(dalloc(&ctx->d_inst_cell, count));
+  ctx->scratch_rep = count;
+  return GALIC_OK;
+}
+
+FitArgs make_fit_args(galic_ctx *ctx)
+{
+  FitArgs f;
+  const galic_params_t &p = ctx->prm;
+  f.L = ctx->L;
+  f.Ngrid = ctx->G;
+  f.Nstack = ctx->Ns;
+  f.committed = ctx->d_committed;
+  f.stacks = ctx->d_stacks;
+  f.targets = ctx->d_targets;
+  f.dgs_distance = ctx->d_dist;
+  f.fit = ctx->d_fit;
+  f.firstrun = ctx->d_firstrun;
+  for(int t = 0; t < 4; t++) {
+    // main.c:296 / 313: MinParticles * MType / NType, left to right
+    f.thr_d[t] = p.NType[t] ? p.MinParticlesPerBinForDensityMeasurement * p.MType[t] / p.NType[t] : 0;
+    f.thr_e[t] = p.NType[t] ? p.MinParticlesPerBinForDispersionMeasurement * p.MType[t] / p.NType[t] : 0;
+    f.MType[t] = p.MType[t];
+    f.present[t] = (t >= 1 && p.NType[t] > 0) ? 1 : 0;
+    f.tovs[t] = p.TypeOfVelocityStructure[t];
+  }
+  f.R200_20 = p.R200 / 20.0;
+  f.LowerDispLimit = p.LowerDispLimit;
+  return f;
+}
+
+int fixed_point_shift(double bound)
+{
+  if(!(bound > 0) || !std::isfinite(bound)) bound = 1.0;
+  int e = (int) std::ceil(std::log2(bound));
+  return 84 - e;
+}
+
+void set_shifts(galic_ctx *ctx, int *shift)
+{
+  const galic_params_t &p = ctx->prm;
+  // |potential| bound: tabulated part plus the analytic halo and bulge
+  double phi = std::fabs(ctx->pot_min) + p.G * p.M200 / p.Halo_A;
+  if(p.Bulge_Mass > 0 && p.Bulge_A > 0) phi += p.G * p.Bulge_Mass / p.Bulge_A;
+  for(int t = 0; t < 4; t++) {
+    double bm = std::max(p.MType[t], 1e-300);
+    double be = bm * 2.0 * phi * 16.0;  // v^2 <= 2|phi| with a factor 16 headroom
+    for(int g = 0; g < NG_COMMITTED; g++) {
+      bool mass = (g == GALIC_GRID_MASS_S || g == GALIC_GRID_MASS_I);
+      shift[t * NG_COMMITTED + g] = fixed_point_shift(mass ? 2.0 * bm : be);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" const char *galic_status_string(int status)
+{
+  if(status < 0 || status >= (int) (sizeof(kStatusText) / sizeof(kStatusText[0]))) return "unknown status";
+  return kStatusText[status];
+}
+
+extern "C" int galic_last_status(const galic_ctx *ctx) { return ctx ? ctx->status : GALIC_ERR_INVALID_ARGUMENT; }
+
+extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
+{
+  galic_ctx *ctx = nullptr;
+  if(!out) return GALIC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int st = check_params(prm);
+  if(st) return st;
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return GALIC_ERR_NO_DEVICE;
+  }
+  ctx = new galic_ctx();
+  ctx->prm = *prm;
+  cudaGetDevice(&ctx->device);
+  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  for(int k = 0; k < 3; k++) CK(cudaEventCreate(&ctx->ev[k]));
+  CK(prepare_fit_kernels());
+  ctx->L = prm->DG_MaxLevel;
+  ctx->G = 1 << (2 * ctx->L);
+  ctx->Ns = stack_size(ctx->L);
+  const int NF = prm->FG_Nbin * prm->FG_Nbin;
+  CK(dalloc(&ctx->d_fg_acc, NF));
+  CK(dalloc(&ctx->d_fg_pot, NF));
+  for(int t = 1; t <= 3; t++) {
+    CK(dalloc(&ctx->d_vstream[t], NF));
+    CK(cudaMemset(ctx->d_vstream[t], 0, NF * sizeof(double)));
+  }
+  CK(cudaMemset(ctx->d_fg_acc, 0, NF * sizeof(double2)));
+  CK(cudaMemset(ctx->d_fg_pot, 0, NF * sizeof(double)));
+  CK(dalloc(&ctx->d_cellsize, ctx->G));
+  CK(dalloc(&ctx->d_dist, ctx->Ns));
+  CK(dalloc(&ctx->d_targets, (size_t) 4 * NT_TARGET * ctx->Ns));
+  CK(cudaMemset(ctx->d_targets, 0, (size_t) 4 * NT_TARGET * ctx->Ns * sizeof(double)));
+  CK(dalloc(&ctx->d_committed, (size_t) 4 * NG_COMMITTED * ctx->G));
+  CK(cudaMemset(ctx->d_committed, 0, (size_t) 4 * NG_COMMITTED * ctx->G * sizeof(double)));
+  CK(dalloc(&ctx->d_stacks, (size_t) 4 * NG_COMMITTED * ctx->Ns));
+  CK(dalloc(&ctx->d_fx, (size_t) 4 * NG_COMMITTED * ctx->G));
+  CK(dalloc(&ctx->d_shift, 4 * NG_COMMITTED));
+  CK(dalloc(&ctx->d_fit, 4 * 7 + 4 * 5));
+  CK(cudaMemset(ctx->d_fit, 0, (4 * 7 + 4 * 5) * sizeof(double)));
+  CK(dalloc(&ctx->d_firstrun, 4));
+  CK(cudaMemset(ctx->d_firstrun, 0, 4 * sizeof(int)));
+  CK(dalloc(&ctx->d_counters, 9));
+  CK(cudaMemset(ctx->d_counters, 0, 9 * sizeof(unsigned long long)));
+  CK(dalloc(&ctx->d_status, 1));
+  CK(dalloc(&ctx->d_next, 1));
+  CK(dalloc(&ctx->d_maxerr, 1));
+
+  DevModel &M = ctx->dm;
+  M.V200 = prm->V200;
+  M.M200 = prm->M200;
+  M.R200 = prm->R200;
+  M.G = prm->G;
+  M.Halo_Mass = prm->Halo_Mass;
+  M.Halo_A = prm->Halo_A;
+  M.Bulge_Mass = prm->Bulge_Mass;
+  M.Bulge_A = prm->Bulge_A;
+  M.f_orb = prm->TimeStepFactorOrbit;
+  M.f_cc = prm->TimeStepFactorCellCross;
+  M.LowerDispLimit = prm->LowerDispLimit;
+  M.MaxVelInUnitsVesc = prm->MaxVelInUnitsVesc;
+  M.tabulated = (prm->Disk_Mass > 0 || (prm->Halo_Mass > 0 && prm->SampleForceNhalo > 0) ||
+                 (prm->Bulge_Mass > 0 && prm->SampleForceNbulge > 0))
+                    ? 1
+                    : 0;
+  M.analytic_halo = (prm->Halo_Mass > 0 && prm->SampleForceNhalo == 0) ? 1 : 0;
+  M.analytic_bulge = (prm->Bulge_Mass > 0 && prm->SampleForceNbulge == 0) ? 1 : 0;
+  for(int t = 0; t < 4; t++) {
+    M.tovs[t] = prm->TypeOfVelocityStructure[t];
+    M.vstream_zero[t] = 1;
+  }
+  M.FG_Nbin = prm->FG_Nbin;
+  M.DG_Nbin = 1 << ctx->L;
+  M.DG_L = ctx->L;
+  M.EG_L = prm->EG_MaxLevel;
+  M.DG_Ngrid = ctx->G;
+  M.DG_Nstack = ctx->Ns;
+  M.FG_Rmin = prm->FG_Rmin;
+  M.FG_Fac = prm->FG_Fac;
+  M.DG_Rmin = prm->DG_Rmin;
+  M.DG_Fac = prm->DG_Fac;
+  M.EG_Rmin = prm->EG_Rmin;
+  M.EG_Fac = prm->EG_Fac;
+  M.fg_acc = ctx->d_fg_acc;
+  M.fg_pot = ctx->d_fg_pot;
+  for(int t = 0; t < 4; t++) M.vstream[t] = ctx->d_vstream[t];
+  M.cellsize = ctx->d_cellsize;
+  M.step_cap = GALIC_STEP_CAP;
+  *out = ctx;
+  return GALIC_OK;
+}
+
+extern "C" void galic_ctx_destroy(galic_ctx *ctx)
+{
+  if(!ctx) return;
+  cudaStreamSynchronize(ctx->stream);
+  dfree(ctx->d_fg_acc); dfree(ctx->d_fg_pot);
+  for(int t = 0; t < 4; t++) dfree(ctx->d_vstream[t]);
+  dfree(ctx->d_cellsize); dfree(ctx->d_dist); dfree(ctx->d_targets); dfree(ctx->d_committed); dfree(ctx->d_stacks);
+  dfree(ctx->d_fx); dfree(ctx->d_shift); dfree(ctx->d_fit); dfree(ctx->d_firstrun); dfree(ctx->d_counters);
+  dfree(ctx->d_status); dfree(ctx->d_next); dfree(ctx->d_maxerr);
+  dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
+  dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits);
+  dfree(ctx->d_b_pos); dfree(ctx->d_b_vel); dfree(ctx->d_b_mass); dfree(ctx->d_b_time); dfree(ctx->d_grids);
+  dfree(ctx->d_b_tall); dfree(ctx->d_b_err); dfree(ctx->d_b_type); dfree(ctx->d_b_norbit); dfree(ctx->d_b_status);
+  dfree(ctx->d_b_steps);
+  dfree(ctx->d_idx); dfree(ctx->d_accepted); dfree(ctx->d_vel_try); dfree(ctx->d_F); dfree(ctx->d_inst_v);
+  dfree(ctx->d_inst_cell);
+  for(int k = 0; k < 3; k++)
+    if(ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if(ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" int galic_set_force_grid(galic_ctx *ctx, const double *pot, const double *dpotdr, const double *dpotdz)
+{
+  if(!ctx || !pot || !dpotdr || !dpotdz) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  const int NF = ctx->prm.FG_Nbin * ctx->prm.FG_Nbin;
+  std::vector<double2> acc(NF);
+  double pmin = 0;
+  for(int i = 0; i < NF; i++) {
+    acc[i] = make_double2(dpotdr[i], dpotdz[i]);
+    if(pot[i] < pmin) pmin = pot[i];
+  }
+  ctx->pot_min = pmin;
+  CK(cudaMemcpy(ctx->d_fg_acc, acc.data(), NF * sizeof(double2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_fg_pot, pot, NF * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->have_fg = true;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_set_vstream(galic_ctx *ctx, int type, const double *v)
+{
+  if(!ctx || !v || type < 1 || type > 3) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  const int NF = ctx->prm.FG_Nbin * ctx->prm.FG_Nbin;
+  int zero = 1;
+  for(int i = 0; i < NF && zero; i++) {
+    uint64_t b;
+    memcpy(&b, &v[i], 8);
+    if(b != 0) zero = 0;  // only +0.0 everywhere allows skipping the lookup
+  }
+  ctx->dm.vstream_zero[type] = zero;
+  CK(cudaMemcpy(ctx->d_vstream[type], v, NF * sizeof(double), cudaMemcpyHostToDevice));
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_set_density_geometry(galic_ctx *ctx, const double *cellsize, const double *dist)
+{
+  if(!ctx || !cellsize || !dist) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  CK(cudaMemcpy(ctx->d_cellsize, cellsize, ctx->G * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_dist, dist, ctx->Ns * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->have_geom = true;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_set_targets(galic_ctx *ctx, int type, const double *dgs_mass, const double *egs_mass,
+                                 const double *egs_r, const double *egs_t, const double *egs_p, const double *egs_q)
+{
+  if(!ctx || type < 1 || type > 3 || !dgs_mass || !egs_mass || !egs_r || !egs_t || !egs_p || !egs_q)
+    return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  const double *src[NT_TARGET] = {dgs_mass, egs_mass, egs_r, egs_t, egs_p, egs_q};
+  for(int k = 0; k < NT_TARGET; k++)
+    CK(cudaMemcpy(ctx->d_targets + ((size_t) type * NT_TARGET + k) * ctx->Ns, src[k], ctx->Ns * sizeof(double),
+                  cudaMemcpyHostToDevice));
+  ctx->have_targets[type] = true;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, const double *vel, const double *mass,
+                                   const double *tint, const double *vesc, const int *type, const double *targets)
+{
+  if(!ctx || n <= 0 || !pos || !vel || !mass || !tint || !vesc || !type || !targets)
+    return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  for(int i = 0; i < n; i++)
+    if(type[i] < 1 || type[i] > 3 || !(tint[i] > 0)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(n != ctx->n) {
+    dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
+    dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits);
+    CK(dalloc(&ctx->d_pos, 3 * (size_t) n));
+    CK(dalloc(&ctx->d_vel, 3 * (size_t) n));
+    CK(dalloc(&ctx->d_mass, n));
+    CK(dalloc(&ctx->d_tint, n));
+    CK(dalloc(&ctx->d_vesc, n));
+    CK(dalloc(&ctx->d_ptargets, 4 * (size_t) n));
+    CK(dalloc(&ctx->d_vdisp, 4 * (size_t) n));
+    CK(dalloc(&ctx->d_type, n));
+    CK(dalloc(&ctx->d_orbits, n));
+    ctx->n = n;
+  }
+  CK(cudaMemcpy(ctx->d_pos, pos, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_vel, vel, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_mass, mass, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_tint, tint, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_vesc, vesc, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemset(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double)));
+  CK(cudaMemset(ctx->d_orbits, 0, n * sizeof(int)));
+  ctx->have_response = false;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_get_particles(galic_ctx *ctx, double *vel, int *orbits, double *vdisp)
+{
+  if(!ctx || ctx->n == 0) return fail(ctx, GALIC_ERR_STATE);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if(vel) CK(cudaMemcpy(vel, ctx->d_vel, 3 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+  if(orbits) CK(cudaMemcpy(orbits, ctx->d_orbits, ctx->n * sizeof(int), cudaMemcpyDeviceToHost));
+  if(vdisp) CK(cudaMemcpy(vdisp, ctx->d_vdisp, 4 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+  return fail(ctx, GALIC_OK);
+}
+
+namespace {
+
+double one_orbit(galic_ctx *ctx, double *pos, double *vel, double *grids[5], double mass, double timespan,
+                 int *orbitstaken, int type, int with_egy)
+{
+  if(!ctx) return -1.0;
+  if(!pos || !vel || !grids[0] || !orbitstaken || (with_egy && (!grids[1] || !grids[2] || !grids[3] || !grids[4])) ||
+     type < 1 || type > 3 || !ctx->have_geom) {
+    fail(ctx, !ctx->have_geom ? GALIC_ERR_STATE : GALIC_ERR_INVALID_ARGUMENT);
+    return -1.0;
+  }
+  if(ensure_orbit_scratch(ctx, 1)) return -1.0;
+  const int G = ctx->G;
+  OrbitBatch b;
+  b.count = 1;
+  b.pos = ctx->d_b_pos;
+  b.vel = ctx->d_b_vel;
+  b.mass = ctx->d_b_mass;
+  b.timespan = ctx->d_b_time;
+  b.type = ctx->d_b_type;
+  b.grids = ctx->d_grids;
+  b.tall = ctx->d_b_tall;
+  b.norbit = ctx->d_b_norbit;
+  b.steps = ctx->d_b_steps;
+  b.egy_err = ctx->d_b_err;
+  b.status = ctx->d_b_status;
+  b.with_egy = with_egy;
+  cudaStream_t s = ctx->stream;
+  auto ck = [&](cudaError_t e) {
+    if(e != cudaSuccess) {
+      fprintf(stderr, "galic_cuda: %s\n", cudaGetErrorString(e));
+      fail(ctx, GALIC_ERR_CUDA);
+      return false;
+    }
+    return true;
+  };
+  if(!ck(cudaMemcpyAsync(ctx->d_b_pos, pos, 3 * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+     !ck(cudaMemcpyAsync(ctx->d_b_vel, vel, 3 * sizeof(double), cudaMemcpyHostToDevice, s)) ||
+     !ck(cudaMemcpyAsync(ctx->d_b_mass, &mass, sizeof(double), cudaMemcpyHostToDevice, s)) ||
+     !ck(cudaMemcpyAsync(ctx->d_b_time, &timespan, sizeof(double), cudaMemcpyHostToDevice, s)) ||
+     !ck(cudaMemcpyAsync(ctx->d_b_type, &type, sizeof(int), cudaMemcpyHostToDevice, s)) ||
+     !ck(cudaMemsetAsync(ctx->d_grids, 0, (size_t) NF_ORBIT * G * sizeof(double), s)))
+    return -1.0;
+  launch_orbits_dense(ctx->dm, b, s);
+  launch_scale_dense(ctx->dm, b, s);
+  double tall = 0;
+  int norbit = 0, status = 0;
+  if(!ck(cudaMemcpyAsync(&tall, ctx->d_b_tall, sizeof(double), cudaMemcpyDeviceToHost, s)) ||
+     !ck(cudaMemcpyAsync(&norbit, ctx->d_b_norbit, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+     !ck(cudaMemcpyAsync(&status, ctx->d_b_status, sizeof(int), cudaMemcpyDeviceToHost, s)))
+    return -1.0;
+  for(int f = 0; f < (with_egy ? NF_ORBIT : 1); f++)
+    if(!ck(cudaMemcpyAsync(grids[f], ctx->d_grids + (size_t) f * G, G * sizeof(double), cudaMemcpyDeviceToHost, s)))
+      return -1.0;
+  if(!ck(cudaStreamSynchronize(s)) || !ck(cudaGetLastError())) return -1.0;
+  ctx->last_launches = 2;
+  if(status == ORBIT_STEP_CAP) {
+    fail(ctx, GALIC_ERR_STEP_CAP);
+    return -1.0;
+  }
+  if(status == ORBIT_NONFINITE) {
+    fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+    return -1.0;
+  }
+  *orbitstaken = norbit;
+  fail(ctx, GALIC_OK);
+  return tall;
+}
+
+}  // namespace
+
+extern "C" double galic_produce_orbit_response_field_mod(galic_ctx *ctx, double *pos, double *vel, int id,
+                                                         double *mfield, double *egyfield_r, double *egyfield_t,
+                                                         double *egyfield_q, double *egyfield_p, double mass,
+                                                         double timespan, int *orbitstaken, int type)
+{
+  (void) id;
+  double *g[5] = {mfield, egyfield_r, egyfield_t, egyfield_q, egyfield_p};
+  return one_orbit(ctx, pos, vel, g, mass, timespan, orbitstaken, type, 1);
+}
+
+extern "C" double galic_produce_orbit_response_field(galic_ctx *ctx, double *pos, double *vel, int id,
+                                                     double *mfield, double mass, double timespan, int *orbitstaken)
+{
+  (void) id;
+  double *g[5] = {mfield, nullptr, nullptr, nullptr, nullptr};
+  return one_orbit(ctx, pos, vel, g, mass, timespan, orbitstaken, 1, 0);
+}
+
+extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(form == GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_UNSUPPORTED);
+  if(ctx->n == 0 || !ctx->have_geom) return fail(ctx, GALIC_ERR_STATE);
+  const galic_params_t &p = ctx->prm;
+  for(int t = 1; t <= 3; t++)
+    if(p.NType[t] > 0 && !ctx->have_targets[t]) return fail(ctx, GALIC_ERR_STATE);
+  cudaStream_t s = ctx->stream;
+  const int G = ctx->G;
+  int shift[4 * NG_COMMITTED];
+  set_shifts(ctx, shift);
+  CK(cudaMemcpyAsync(ctx->d_shift, shift, sizeof(shift), cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev[0], s));
+  CK(cudaMemsetAsync(ctx->d_fx, 0, (size_t) 4 * NG_COMMITTED * G * sizeof(FxWord), s));
+  CK(cudaMemsetAsync(ctx->d_next, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(ctx->d_maxerr, 0, sizeof(double), s));
+  CK(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), s));
+  CalcAllArgs a;
+  a.n = ctx->n;
+  a.pos = ctx->d_pos;
+  a.vel = ctx->d_vel;
+  a.mass = ctx->d_mass;
+  a.tint = ctx->d_tint;
+  a.type = ctx->d_type;
+  a.order = nullptr;
+  a.next = ctx->d_next;
+  a.fx = ctx->d_fx;
+  a.shift = ctx->d_shift;
+  a.orbits = ctx->d_orbits;
+  a.steps_total = ctx->d_counters + 8;
+  a.max_egy_err = ctx->d_maxerr;
+  a.status = ctx->d_status;
+  int launches = 0;
+  const int block = 128;
+  int per_sm = calc_all_occupancy(block);
+  if(per_sm < 1) per_sm = 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  int grid = per_sm * sms;
+  int need = (ctx->n + block - 1) / block;
+  if(grid > need) grid = need;
+  CK(cudaEventRecord(ctx->ev[1], s));
+  launches += launch_calc_all_fp64(ctx->dm, a, grid, block, s);
+  CK(cudaEventRecord(ctx->ev[2], s));
+  launch_instantaneous(ctx->dm, ctx->n, ctx->d_pos, ctx->d_vel, ctx->d_mass, ctx->d_type, ctx->d_vdisp, ctx->d_fx,
+                       ctx->d_shift, G, s);
+  launch_fx_finalize(ctx->d_fx, ctx->d_shift, ctx->d_committed, 4 * NG_COMMITTED, G, s);
+  launches += 2;
+  FitArgs f = make_fit_args(ctx);
+  launches += launch_global_fit(f, s);
+  int status = 0;
+  unsigned long long steps = 0;
+  CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&steps, ctx->d_counters + 8, sizeof(steps), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&ctx->last_max_egy_err, ctx->d_maxerr, sizeof(double), cudaMemcpyDeviceToHost, s));
+  cudaEvent_t ev_end;
+  CK(cudaEventCreate(&ev_end));
+  CK(cudaEventRecord(ev_end, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  float ms_total = 0, ms_orbit = 0;
+  CK(cudaEventElapsedTime(&ms_total, ctx->ev[0], ev_end));
+  CK(cudaEventElapsedTime(&ms_orbit, ctx->ev[1], ctx->ev[2]));
+  cudaEventDestroy(ev_end);
+  ctx->last_ms_total = ms_total;
+  ctx->last_ms_orbit = ms_orbit;
+  ctx->last_steps = (long long) steps;
+  ctx->last_launches = launches;
+  if(status == ORBIT_STEP_CAP) return fail(ctx, GALIC_ERR_STEP_CAP);
+  if(status == ORBIT_NONFINITE) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->have_response = true;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial,
+                                  int form)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(form == GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_UNSUPPORTED);
+  if(!ctx->have_response) return fail(ctx, GALIC_ERR_STATE);
+  if(count < 0 || (count > 0 && !idx)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  // every particle at most once per repetition: the reference evaluates a
+  // repetition against committed state and P[n] only changes for n itself
+  std::vector<char> seen(ctx->n, 0);
+  for(int k = 0; k < count; k++) {
+    if(idx[k] < 0 || idx[k] >= ctx->n || seen[idx[k]]) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+    seen[idx[k]] = 1;
+  }
+  cudaStream_t s = ctx->stream;
+  FitArgs f = make_fit_args(ctx);
+  if(count == 0) {  // init_updates + commit_updates with no particle: only the fit
+    ctx->last_launches = launch_global_fit(f, s);
+    CK(cudaStreamSynchronize(s));
+    return fail(ctx, GALIC_OK);
+  }
+  int st = ensure_rep_scratch(ctx, count);
+  if(st) return st;
+  CK(cudaMemcpyAsync(ctx->d_idx, idx, count * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(ctx->d_b_status, 0, 2 * (size_t) count * sizeof(int), s));
+  RepArgs R;
+  R.count = count;
+  R.idx = ctx->d_idx;
+  R.seed = seed;
+  R.rep_serial = rep_serial;
+  R.p_pos = ctx->d_pos;
+  R.p_vel = ctx->d_vel;
+  R.p_mass = ctx->d_mass;
+  R.p_tint = ctx->d_tint;
+  R.p_vesc = ctx->d_vesc;
+  R.p_targets = ctx->d_ptargets;
+  R.p_vdisp = ctx->d_vdisp;
+  R.p_type = ctx->d_type;
+  R.p_orbits = ctx->d_orbits;
+  R.b_pos = ctx->d_b_pos;
+  R.b_vel = ctx->d_b_vel;
+  R.b_mass = ctx->d_b_mass;
+  R.b_time = ctx->d_b_time;
+  R.b_type = ctx->d_b_type;
+  R.b_norbit = ctx->d_b_norbit;
+  R.grids = ctx->d_grids;
+  R.vel_try = ctx->d_vel_try;
+  R.F = ctx->d_F;
+  R.accepted = ctx->d_accepted;
+  R.inst_v = ctx->d_inst_v;
+  R.inst_cell = ctx->d_inst_cell;
+  R.tries = ctx->d_counters;
+  R.changes = ctx->d_counters + 4;
+  for(int t = 0; t < 4; t++) {
+    R.fac_rs[t] = ctx->prm.fac_value_rs[t];
+    R.fac_ts[t] = ctx->prm.fac_value_ts[t];
+    R.fac_qs[t] = ctx->prm.fac_value_qs[t];
+    R.fac_ps[t] = ctx->prm.fac_value_ps[t];
+  }
+  R.status = ctx->d_status;
+  OrbitBatch b;
+  b.count = 2 * count;
+  b.pos = ctx->d_b_pos;
+  b.vel = ctx->d_b_vel;
+  b.mass = ctx->d_b_mass;
+  b.timespan = ctx->d_b_time;
+  b.type = ctx->d_b_type;
+  b.grids = ctx->d_grids;
+  b.tall = ctx->d_b_tall;
+  b.norbit = ctx->d_b_norbit;
+  b.steps = ctx->d_b_steps;
+  b.egy_err = ctx->d_b_err;
+  b.status = ctx->d_b_status;
+  b.with_egy = 1;
+  ctx->last_launches = launch_rep(ctx->dm, R, f, b, s);
+  int status = 0;
+  std::vector<int> ost(2 * count);
+  std::vector<long long> steps(2 * count);
+  CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ost.data(), ctx->d_b_status, 2 * (size_t) count * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(steps.data(), ctx->d_b_steps, 2 * (size_t) count * sizeof(long long), cudaMemcpyDeviceToHost,
+                     s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  long long tot = 0;
+  for(int k = 0; k < 2 * count; k++) {
+    tot += steps[k];
+    if(ost[k] == ORBIT_STEP_CAP) status = std::max(status, (int) GALIC_ERR_STEP_CAP);
+  }
+  ctx->last_steps = tot;
+  if(status) return fail(ctx, status);
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_get_fit(galic_ctx *ctx, double *out)
+{
+  if(!ctx || !out) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(out, ctx->d_fit, 4 * 7 * sizeof(double), cudaMemcpyDeviceToHost));
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_get_counters(galic_ctx *ctx, long long *tries, long long *changes)
+{
+  if(!ctx || !tries || !changes) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  unsigned long long c[8];
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  for(int t = 0; t < 4; t++) {
+    tries[t] = (long long) c[t];
+    changes[t] = (long long) c[4 + t];
+  }
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_get_response(galic_ctx *ctx, int type, int which, double *out)
+{
+  if(!ctx || !out || type < 1 || type > 3 || which < 0 || which >= GALIC_GRID_COUNT)
+    return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(out, ctx->d_committed + ((size_t) type * NG_COMMITTED + which) * ctx->G, ctx->G * sizeof(double),
+                cudaMemcpyDeviceToHost));
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_set_step_cap(galic_ctx *ctx, long long cap)
+{
+  if(!ctx || cap < 1) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->dm.step_cap = cap;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_last_timing(const galic_ctx *ctx, double *ms_total, double *ms_orbit_kernel)
+{
+  if(!ctx || !ms_total || !ms_orbit_kernel) return GALIC_ERR_INVALID_ARGUMENT;
+  *ms_total = ctx->last_ms_total;
+  *ms_orbit_kernel = ctx->last_ms_orbit;
+  return GALIC_OK;
+}
+
+extern "C" double galic_last_max_energy_error(const galic_ctx *ctx) { return ctx ? ctx->last_max_egy_err : 0; }
+
+extern "C" long long galic_last_orbit_steps(const galic_ctx *ctx) { return ctx ? ctx->last_steps : 0; }
+extern "C" int galic_last_kernel_launches(const galic_ctx *ctx) { return ctx ? ctx->last_launches : 0; }

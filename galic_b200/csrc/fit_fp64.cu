@@ -1,0 +1,364 @@
+// Merit function and optimisation repetition (built with --fmad=false).
+//
+//  k_fit_smooth / k_fit_diff / k_fit_final   calc_global_fit (main.c:251-362)
+//  k_propose      the proposal part of optimize (main.c:365-441)
+//  k_eval_fit     eval_fit_mod (main.c:1021-1217), one CTA per evaluation
+//  k_accept       the accept branch of optimize (main.c:468-507)
+//  k_delta_cols   the _delta accumulation (main.c:477-486) and commit_updates
+//                 (main.c:818-827): per bin, the accepted particles'
+//                 new - old values are summed in particle order, as the
+//                 reference's sequential loop does, then added to the
+//                 committed grid.
+//  k_inst_delta   add_to_energy_grid of the accepted particles
+//                 (main.c:488-498) and its commit (main.c:830-835).
+#include <cuda_runtime.h>
+
+#include "galic_gpu.h"
+#include "grng.h"
+#include "kernels.cuh"
+#include "rep.cuh"
+#include "stack.cuh"
+
+namespace {
+
+__global__ void k_fit_smooth(FitArgs f)
+{
+  extern __shared__ double sm[];
+  const int type = blockIdx.x / NG_COMMITTED, g = blockIdx.x % NG_COMMITTED;
+  if(type < 1 || !f.present[type]) return;
+  const int off = ((1 << (2 * f.L)) - 1) / 3;
+  const double *src = f.committed + ((size_t) type * NG_COMMITTED + g) * f.Ngrid;
+  for(int i = threadIdx.x; i < f.Ngrid; i += blockDim.x) sm[off + i] = src[i];
+  __syncthreads();
+  stack_smooth_cta(sm, f.L);
+  double *dst = f.stacks + ((size_t) type * NG_COMMITTED + g) * f.Nstack;
+  for(int i = threadIdx.x; i < f.Nstack; i += blockDim.x) dst[i] = sm[i];
+}
+
+// raw[type][w]: w = 0 S, 1 Sdisp_r, 2 Sdisp_t, 3 Sdisp_p, 4 Sdisp_q
+__global__ void k_fit_diff(FitArgs f, double *raw)
+{
+  extern __shared__ double sm[];
+  const int type = blockIdx.x / 5, w = blockIdx.x % 5;
+  if(type < 1 || !f.present[type]) return;
+  const double *stk = f.stacks + (size_t) type * NG_COMMITTED * f.Nstack;
+  const double *tg = f.targets + (size_t) type * NT_TARGET * f.Nstack;
+  const double *d1, *d2, *r1, *r2, *dist;
+  double thr;
+  int flag;
+  if(w == 0) {
+    d1 = stk + (size_t) GALIC_GRID_MASS_S * f.Nstack;
+    d2 = tg + (size_t) T_DGM * f.Nstack;
+    r1 = d2;
+    r2 = nullptr;
+    dist = f.dgs_distance;
+    thr = f.thr_d[type];
+    flag = 0;
+  } else {
+    const int gi[5] = {0, GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
+    const int ti[5] = {0, T_R, T_T, T_P, T_Q};
+    d1 = stk + (size_t) gi[w] * f.Nstack;
+    d2 = tg + (size_t) ti[w] * f.Nstack;
+    r1 = stk + (size_t) GALIC_GRID_MASS_I * f.Nstack;
+    r2 = tg + (size_t) T_EGM * f.Nstack;
+    dist = nullptr;
+    thr = f.thr_e[type];
+    flag = 1;
+  }
+  for(int i = threadIdx.x; i < f.Nstack; i += blockDim.x) sm[i] = d1[i];
+  __syncthreads();
+  double v = stack_diff_cta(sm, d2, r1, r2, dist, thr, flag, 0, f.L, f.R200_20, f.LowerDispLimit);
+  if(threadIdx.x == 0) raw[type * 5 + w] = v;
+}
+
+__global__ void k_fit_final(FitArgs f, const double *raw)
+{
+  const int type = threadIdx.x;
+  if(type < 1 || type > 3 || !f.present[type]) return;
+  const double *tg = f.targets + (size_t) type * NT_TARGET * f.Nstack;
+  double S = raw[type * 5 + 0];
+  S *= 1.0 / tg[T_DGM * f.Nstack + 0];
+  double sr = raw[type * 5 + 1], st = raw[type * 5 + 2], sp = raw[type * 5 + 3], sq = raw[type * 5 + 4];
+  double count;
+  if(f.tovs[type] == 0 || f.tovs[type] == 1) {
+    count = 3.0;
+    sq = 0;
+  } else
+    count = 4.0;
+  double *o = f.fit + type * 7;
+  double srel = o[5];
+  if(f.firstrun[type] == 0) {
+    srel = S / ((sr + st + sp + sq) / count);
+    f.firstrun[type] = 1;
+  }
+  o[0] = S;
+  o[1] = sr * srel;
+  o[2] = st * srel;
+  o[3] = sp * srel;
+  o[4] = sq * srel;
+  o[5] = srel;
+  o[6] = count;
+}
+
+// ---------------------------------------------------------------- optimize
+
+__global__ void k_propose(DevModel M, RepArgs R)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= R.count) return;
+  LogConsts L = make_log_consts(M);
+  const int n = R.idx[k];
+  const int type = R.p_type[n];
+  const int tovs = M.tovs[type];
+  const double *pos = &R.p_pos[3 * n];
+  grng_t g;
+  grng_init(&g, R.seed, (uint32_t) n, R.rep_serial);
+  (void) grng_uniform(&g);  // dir_rnd (main.c:370)
+  double phi = gm_atan2(pos[1], pos[0]);
+  double Rv[3], Tv[3], Qv[3];
+  if(tovs == 2) {
+    double c = gm_cos(phi), s = gm_sin(phi);
+    Rv[0] = c; Rv[1] = s; Rv[2] = 0;
+    Tv[0] = -s; Tv[1] = c; Tv[2] = 0;
+    Qv[0] = 0; Qv[1] = 0; Qv[2] = 1;
+  } else {
+    double theta = gm_acos(pos[2] / sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]));
+    double st = gm_sin(theta), ct = gm_cos(theta), sp = gm_sin(phi), cp = gm_cos(phi);
+    Rv[0] = st * cp; Rv[1] = st * sp; Rv[2] = ct;
+    Tv[0] = -ct * cp; Tv[1] = -ct * sp; Tv[2] = st;
+    Qv[0] = -sp; Qv[1] = cp; Qv[2] = 0;
+  }
+  const double *tg = &R.p_targets[4 * n];
+  double sigma_r = sqrt(tg[0]), sigma_t = sqrt(tg[1]), sigma_p = sqrt(tg[2]);
+  double vstr = vstream_at(M, fg_coord(M, L, pos), type);
+  double v_new[3], v2_new;
+  int iter = 0, st_code = 0;
+  do {
+    double vr_new = grng_gaussian(&g, sigma_r);
+    double vt_new = grng_gaussian(&g, sigma_t);
+    double vq_new = vstr + grng_gaussian(&g, sigma_p);
+    for(int j = 0; j < 3; j++) v_new[j] = vr_new * Rv[j] + vt_new * Tv[j] + vq_new * Qv[j];
+    v2_new = v_new[0] * v_new[0] + v_new[1] * v_new[1] + v_new[2] * v_new[2];
+    iter++;
+    if(iter > 100000) {  // main.c:432-433
+      st_code = GALIC_ERR_REJECTION_CAP;
+      break;
+    }
+  } while(sqrt(v2_new) >= M.MaxVelInUnitsVesc * R.p_vesc[n]);
+  if(st_code) atomicMax(R.status, st_code);
+  for(int j = 0; j < 3; j++) {
+    R.vel_try[3 * k + j] = v_new[j];
+    R.b_pos[3 * (2 * k) + j] = pos[j];
+    R.b_pos[3 * (2 * k + 1) + j] = pos[j];
+    R.b_vel[3 * (2 * k) + j] = R.p_vel[3 * n + j];
+    R.b_vel[3 * (2 * k + 1) + j] = v_new[j];
+  }
+  R.b_mass[2 * k] = R.b_mass[2 * k + 1] = R.p_mass[n];
+  R.b_time[2 * k] = R.b_time[2 * k + 1] = R.p_tint[n];
+  R.b_type[2 * k] = R.b_type[2 * k + 1] = type;
+}
+
+// one CTA per (particle k, which): which 0 = F_base, 1 = F_try
+__global__ void k_eval_fit(DevModel M, RepArgs R, FitArgs f)
+{
+  extern __shared__ double sm[];
+  __shared__ double sh_d[4];
+  __shared__ Cell sh_c;
+  const int k = blockIdx.x >> 1, which = blockIdx.x & 1;
+  const int n = R.idx[k];
+  const int type = R.p_type[n];
+  const int L = f.L, G = f.Ngrid, Ns = f.Nstack;
+  const int off = ((1 << (2 * L)) - 1) / 3;
+  const double *gold = R.grids + (size_t) (2 * k) * NF_ORBIT * G;
+  const double *gnew = R.grids + (size_t) (2 * k + which) * NF_ORBIT * G;
+  const double *stk = f.stacks + (size_t) type * NG_COMMITTED * Ns;
+  const double *tg = f.targets + (size_t) type * NT_TARGET * Ns;
+  const double MT = f.MType[type];
+
+  // density term (main.c:1033-1047)
+  for(int i = threadIdx.x; i < G; i += blockDim.x)
+    sm[off + i] = stk[(size_t) GALIC_GRID_MASS_S * Ns + off + i] + gnew[F_M * G + i] - gold[F_M * G + i];
+  __syncthreads();
+  stack_smooth_cta(sm, L);
+  double value = stack_diff_cta(sm, tg + T_DGM * Ns, tg + T_DGM * Ns, nullptr, f.dgs_distance, f.thr_d[type], 0, 0, L,
+                                f.R200_20, f.LowerDispLimit);
+  value *= 1.0 / MT;
+
+  // time-averaged dispersion terms (main.c:1052-1120): r, t, q, p
+  const int fs[4] = {F_R, F_T, F_Q, F_P};
+  const int gs[4] = {GALIC_GRID_R_S, GALIC_GRID_T_S, GALIC_GRID_Q_S, GALIC_GRID_P_S};
+  const int ts[4] = {T_R, T_T, T_Q, T_P};
+  double vs[4];
+  for(int a = 0; a < 4; a++) {
+    for(int i = threadIdx.x; i < G; i += blockDim.x)
+      sm[off + i] = stk[(size_t) gs[a] * Ns + off + i] + gnew[fs[a] * G + i] - gold[fs[a] * G + i];
+    __syncthreads();
+    stack_smooth_cta(sm, L);
+    vs[a] = stack_diff_cta(sm, tg + ts[a] * Ns, tg + T_DGM * Ns, tg + ts[a] * Ns, f.dgs_distance, f.thr_d[type], 2, 1,
+                           L, f.R200_20, f.LowerDispLimit) /
+            MT;
+  }
+  const double value_rs = vs[0], value_ts = vs[1], value_qs = vs[2], value_ps = vs[3];
+
+  // instantaneous terms (main.c:1125-1176)
+  if(threadIdx.x == 0) {
+    LogConsts Lc = make_log_consts(M);
+    const double *vel = which ? &R.vel_try[3 * k] : &R.p_vel[3 * n];
+    disp_components(M, Lc, type, &R.p_pos[3 * n], vel, sh_d);
+    sh_c = energy_cell(M, Lc, &R.p_pos[3 * n]);
+  }
+  __syncthreads();
+  const double mass = R.p_mass[n];
+  const double *vd = &R.p_vdisp[4 * n];
+  // add_to_energy_grid: vr2 *= mass etc. (main.c:885-888); order r, t, p, q
+  const double dv[4] = {(sh_d[0] - vd[0]) * mass, (sh_d[1] - vd[1]) * mass, (sh_d[2] - vd[2]) * mass,
+                        (sh_d[3] - vd[3]) * mass};
+  const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
+  const int ti[4] = {T_R, T_T, T_P, T_Q};
+  const Cell c = sh_c;
+  const int Nb = 1 << L;
+  const int cells[4] = {c.iz * Nb + c.iR, c.iz * Nb + c.iR + 1, (c.iz + 1) * Nb + c.iR, (c.iz + 1) * Nb + c.iR + 1};
+  const double w[4] = {(1 - c.fR) * (1 - c.fz), (c.fR) * (1 - c.fz), (1 - c.fR) * (c.fz), (c.fR) * (c.fz)};
+  double vi[4];
+  for(int a = 0; a < 4; a++) {
+    for(int i = threadIdx.x; i < G; i += blockDim.x) sm[off + i] = stk[(size_t) gi[a] * Ns + off + i];
+    __syncthreads();
+    if(threadIdx.x == 0)
+      for(int j = 0; j < 4; j++) sm[off + cells[j]] += w[j] * dv[a];
+    __syncthreads();
+    stack_smooth_cta(sm, L);
+    vi[a] = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns, nullptr,
+                           f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
+  }
+  double value_r = vi[0], value_t = vi[1], value_p = vi[2], value_q = vi[3];
+  if(M.tovs[type] == 0 || type == 2) value_q = 0;  // main.c:1195
+  if(threadIdx.x == 0) {
+    const double *fit = f.fit + type * 7;
+    double F = value + fit[5] / fit[6] * (value_r + value_t + value_p + value_q) +
+               (R.fac_rs[type] * value_rs + R.fac_ts[type] * value_ts + R.fac_ps[type] * value_ps +
+                R.fac_qs[type] * value_qs) /
+                   4;
+    R.F[blockIdx.x] = F;
+  }
+}
+
+__global__ void k_accept(DevModel M, RepArgs R)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= R.count) return;
+  const int n = R.idx[k];
+  const int type = R.p_type[n];
+  R.p_orbits[n] = R.b_norbit[2 * k];  // main.c:460 writes the old orbit's count
+  atomicAdd(&R.tries[type], 1ULL);
+  const bool acc = R.F[2 * k + 1] < R.F[2 * k];
+  R.accepted[k] = acc ? 1 : 0;
+  if(!acc) return;
+  for(int j = 0; j < 3; j++) R.p_vel[3 * n + j] = R.vel_try[3 * k + j];
+  R.p_orbits[n] = R.b_norbit[2 * k + 1];
+  atomicAdd(&R.changes[type], 1ULL);
+  LogConsts L = make_log_consts(M);
+  double d[4];
+  disp_components(M, L, type, &R.p_pos[3 * n], &R.vel_try[3 * k], d);
+  double *vd = &R.p_vdisp[4 * n];
+  const double mass = R.p_mass[n];
+  for(int j = 0; j < 4; j++) {
+    R.inst_v[4 * k + j] = (d[j] - vd[j]) * mass;
+    vd[j] = d[j];
+  }
+  R.inst_cell[k] = energy_cell(M, L, &R.p_pos[3 * n]);
+}
+
+// per (type, field, bin): delta = sum over accepted particles, in order, of
+// new - old; committed += delta
+__global__ void k_delta_cols(RepArgs R, FitArgs f)
+{
+  const int G = f.Ngrid;
+  const size_t total = (size_t) 4 * NF_ORBIT * G;
+  for(size_t t = blockIdx.x * (size_t) blockDim.x + threadIdx.x; t < total; t += (size_t) gridDim.x * blockDim.x) {
+    const int type = (int) (t / ((size_t) NF_ORBIT * G));
+    const int fld = (int) ((t / G) % NF_ORBIT);
+    const int i = (int) (t % G);
+    if(type < 1 || !f.present[type]) continue;
+    double delta = 0;
+    for(int k = 0; k < R.count; k++) {
+      if(!R.accepted[k] || R.b_type[2 * k] != type) continue;
+      const double *gold = R.grids + (size_t) (2 * k) * NF_ORBIT * G;
+      const double *gnew = gold + (size_t) NF_ORBIT * G;
+      delta += gnew[fld * G + i] - gold[fld * G + i];
+    }
+    // orbit fields m,r,t,q,p map to committed MASS_S, R_S, T_S, Q_S, P_S
+    double *dst = (double *) f.committed + ((size_t) type * NG_COMMITTED + fld) * G + i;
+    *dst += delta;
+  }
+}
+
+__global__ void k_inst_delta(RepArgs R, FitArgs f)
+{
+  const int G = f.Ngrid, Nb = 1 << f.L;
+  const size_t total = (size_t) 4 * 4 * G;
+  const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
+  for(size_t t = blockIdx.x * (size_t) blockDim.x + threadIdx.x; t < total; t += (size_t) gridDim.x * blockDim.x) {
+    const int type = (int) (t / ((size_t) 4 * G));
+    const int a = (int) ((t / G) % 4);
+    const int cidx = (int) (t % G);
+    if(type < 1 || !f.present[type]) continue;
+    double delta = 0;
+    for(int k = 0; k < R.count; k++) {
+      if(!R.accepted[k] || R.b_type[2 * k] != type) continue;
+      const Cell c = R.inst_cell[k];
+      const int base = c.iz * Nb + c.iR;
+      double w;
+      if(cidx == base) w = (1 - c.fR) * (1 - c.fz);
+      else if(cidx == base + 1) w = (c.fR) * (1 - c.fz);
+      else if(cidx == base + Nb) w = (1 - c.fR) * (c.fz);
+      else if(cidx == base + Nb + 1) w = (c.fR) * (c.fz);
+      else continue;
+      // inst_v holds (vr2, vt2, vp2, vq2) differences times mass
+      delta += w * R.inst_v[4 * k + a];
+    }
+    double *dst = (double *) f.committed + ((size_t) type * NG_COMMITTED + gi[a]) * G + cidx;
+    *dst += delta;
+  }
+}
+
+}  // namespace
+
+// the stack kernels keep a whole level-7 stack (171 KiB) in shared memory;
+// called once per context, on the context's device
+cudaError_t prepare_fit_kernels()
+{
+  cudaError_t e;
+  if((e = cudaFuncSetAttribute(k_fit_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  if((e = cudaFuncSetAttribute(k_fit_diff, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  return cudaFuncSetAttribute(k_eval_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+int launch_global_fit(const FitArgs &f, cudaStream_t s)
+{
+  size_t smem = (size_t) f.Nstack * sizeof(double);
+  double *raw = f.fit + 4 * 7;  // scratch after the 4x7 fit block
+  k_fit_smooth<<<4 * NG_COMMITTED, 1024, smem, s>>>(f);
+  k_fit_diff<<<4 * 5, 1024, smem, s>>>(f, raw);
+  k_fit_final<<<1, 4, 0, s>>>(f, raw);
+  return 3;
+}
+
+int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s)
+{
+  int launches = 0;
+  const int count = R.count;
+  k_propose<<<(count + 63) / 64, 64, 0, s>>>(M, R);
+  launches++;
+  cudaMemsetAsync(b.grids, 0, (size_t) b.count * NF_ORBIT * M.DG_Ngrid * sizeof(double), s);
+  launch_orbits_dense(M, b, s);
+  launch_scale_dense(M, b, s);
+  launches += 2;
+  size_t smem = (size_t) f.Nstack * sizeof(double);
+  k_eval_fit<<<2 * count, 1024, smem, s>>>(M, R, f);
+  k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R);
+  k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
+  k_inst_delta<<<148 * 8, 256, 0, s>>>(R, f);
+  launches += 4;
+  launches += launch_global_fit(f, s);
+  return launches;
+}

@@ -1,0 +1,72 @@
+// Launch wrappers shared by the C-ABI layer (api.cu) and the kernel files.
+#ifndef GALIC_KERNELS_CUH
+#define GALIC_KERNELS_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fixedpoint.cuh"
+#include "galic_gpu.h"
+#include "model.cuh"
+
+// field order of the per-orbit grids: the argument order of
+// produce_orbit_response_field_mod (orbit_response.c:155-157): m, r, t, q, p
+enum { F_M = 0, F_R = 1, F_T = 2, F_Q = 3, F_P = 4, NF_ORBIT = 5 };
+// committed per-type grids, in galic_grid_id order
+enum { NG_COMMITTED = 10 };
+// target stacks per type: DGs_MassTarget, EGs_MassTarget, EGs_EgyTarget_{r,t,p,q}
+enum { T_DGM = 0, T_EGM = 1, T_R = 2, T_T = 3, T_P = 4, T_Q = 5, NT_TARGET = 6 };
+
+struct OrbitBatch {
+  int count;
+  const double *pos, *vel;    // count x 3
+  const double *mass, *timespan;
+  const int *type;
+  double *grids;              // count x NF_ORBIT x DG_Ngrid (zeroed by the caller)
+  double *tall;               // count
+  int *norbit;                // count
+  long long *steps;           // count
+  double *egy_err;            // count
+  int *status;                // count
+  int with_egy;               // produce_orbit_response_field_mod (1) or _field (0)
+};
+
+struct CalcAllArgs {
+  int n;
+  const double *pos, *vel, *mass, *tint;
+  const int *type;
+  const int *order;           // processing order (longest first)
+  int *next;                  // work counter, zeroed by the caller
+  FxWord *fx;                 // [4][NG_COMMITTED][Ngrid]
+  const int *shift;           // [4][NG_COMMITTED]
+  int *orbits;                // per particle
+  unsigned long long *steps_total;
+  double *max_egy_err;        // max relative energy error (as ordered bits)
+  int *status;                // worst OrbitStatus seen
+};
+
+struct FitArgs {
+  int L;                      // DG_MaxLevel == EG_MaxLevel
+  int Ngrid, Nstack;
+  const double *committed;    // [4][10][Ngrid]
+  double *stacks;             // [4][10][Nstack]
+  const double *targets;      // [4][6][Nstack]
+  const double *dgs_distance; // [Nstack]
+  double *fit;                // [4][7]
+  int *firstrun;              // [4]
+  double thr_d[4], thr_e[4], MType[4];
+  int present[4], tovs[4];
+  double R200_20, LowerDispLimit;
+};
+
+void launch_orbits_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s);
+void launch_scale_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s);
+int launch_calc_all_fp64(const DevModel &M, const CalcAllArgs &a, int grid, int block, cudaStream_t s);
+void launch_instantaneous(const DevModel &M, int n, const double *pos, const double *vel, const double *mass,
+                          const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid, cudaStream_t s);
+void launch_fx_finalize(const FxWord *fx, const int *shift, double *committed, int count, int Ngrid, cudaStream_t s);
+int launch_global_fit(const FitArgs &f, cudaStream_t s);
+cudaError_t prepare_fit_kernels();
+int calc_all_occupancy(int block);
+
+#endif

@@ -1,0 +1,37 @@
+// Arguments of one optimisation repetition on the device.
+#ifndef GALIC_REP_CUH
+#define GALIC_REP_CUH
+
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+struct RepArgs {
+  int count;
+  const int *idx;  // particles optimised in this repetition
+  uint64_t seed;
+  uint32_t rep_serial;
+  // particle state P[] (device)
+  const double *p_pos;
+  double *p_vel;
+  const double *p_mass, *p_tint, *p_vesc, *p_targets;
+  double *p_vdisp;
+  const int *p_type;
+  int *p_orbits;
+  // 2*count orbits: [2k] old velocity, [2k+1] trial velocity
+  double *b_pos, *b_vel, *b_mass, *b_time;
+  int *b_type, *b_norbit;
+  double *grids;  // 2*count x NF_ORBIT x Ngrid
+  double *vel_try;  // count x 3
+  double *F;        // 2*count: F_base, F_try
+  int *accepted;    // count
+  double *inst_v;   // count x 4
+  Cell *inst_cell;  // count
+  unsigned long long *tries, *changes;  // [4]
+  double fac_rs[4], fac_ts[4], fac_qs[4], fac_ps[4];
+  int *status;
+};
+
+int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s);
+
+#endif

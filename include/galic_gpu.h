@@ -1,0 +1,200 @@
+/*
+ * galic_gpu.h - C ABI of the B200 (sm_100a) implementation of GALIC's
+ * orbit-response hot path (libgalic_cuda.so).
+ *
+ * The reference (denisyurin/GALIC, C99 + MPI) keeps every input of the hot
+ * path in globals: the run parameters in `All` (allvars.h:639-836), the
+ * tabulated force grid FG_* (grid.c:204-230), the density/energy response
+ * grids DG_* / EG_* and their stacks (grid.c:233-325) and the particle array
+ * `P` (allvars.h:844-868).  This ABI replaces the globals by a context
+ * handle: the caller uploads the same arrays once, in the reference's own
+ * layouts, then calls entry points that replace the reference functions named
+ * beside each declaration.  All pointers passed in or out are HOST pointers
+ * unless a name says otherwise; every array uses the reference's index
+ * convention:
+ *   force grid  FG[iz * FG_Nbin + iR]                       (grid.c:78-80)
+ *   response    grid[iz * DG_Nbin + iR]                     (orbit_response.c:283-286)
+ *   stacks      stack[STACKOFFSET(l,i,j)], STACKOFFSET(l,i,j) =
+ *               ((1<<2l)-1)/3 + i*2^l + j                   (allvars.h:160)
+ *
+ * Errors: every entry point returns a galic_status (0 = success) except the
+ * per-orbit drop-ins, which return the reference's value (tall) and report a
+ * failure as a negative return value plus galic_last_status().  Nothing
+ * aborts and no kernel traps: the reference's terminate()/exit(1) paths
+ * (orbit_response.c:450-456, main.c:432-433) become status codes.
+ *
+ * Threading: one context per host thread; a context is not reentrant, as the
+ * reference's globals are not.
+ */
+#ifndef GALIC_GPU_H
+#define GALIC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GALIC_OK = 0,
+  GALIC_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size or parameter */
+  GALIC_ERR_STEP_CAP = 2,         /* an orbit exceeded the step cap (reference: >1e8 steps, exit(1)) */
+  GALIC_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+  GALIC_ERR_NO_DEVICE = 4,        /* no CUDA device visible */
+  GALIC_ERR_BUDGET = 5,           /* the request does not fit the HBM budget */
+  GALIC_ERR_UNSUPPORTED = 6,      /* configuration the reference rejects with terminate() */
+  GALIC_ERR_REJECTION_CAP = 7,    /* velocity proposal loop exceeded 100000 tries (main.c:432) */
+  GALIC_ERR_OVERFLOW = 8,         /* a fixed-point response bin left its representable range */
+  GALIC_ERR_STATE = 9             /* call out of order (e.g. fit requested before any response) */
+} galic_status;
+
+/* Compute forms of the orbit-response path. */
+typedef enum {
+  GALIC_FORM_FP64 = 0, /* plain FP64, bit-exact per orbit to the CPU restatement (the drop-in) */
+  GALIC_FORM_FP32 = 1  /* FP32 integrate / FP64 merit: the batched throughput form */
+} galic_form;
+
+/*
+ * Parameters of one galaxy model: the subset of the reference's `All`
+ * (allvars.h:639-836) and grid globals (allvars.h:300-420) that the hot path
+ * reads.  Arrays indexed by particle type use index 1 (halo), 2 (disk),
+ * 3 (bulge); index 0 is unused, as in the reference's [6]-sized arrays.
+ */
+typedef struct galic_params {
+  /* structure (structure.c:54-143, init.c:46-54) */
+  double V200, M200, R200, G;
+  double Halo_Mass, Halo_A, HaloStretch;
+  double Disk_Mass;
+  double Bulge_Mass, Bulge_A, BulgeStretch;
+  /* orbit integration (orbit_response.c:16-26) */
+  double TimeStepFactorOrbit, TimeStepFactorCellCross;
+  /* optimisation (main.c:365-527, grid.c:1086-1151) */
+  double LowerDispLimit, MaxVelInUnitsVesc;
+  int SampleForceNhalo, SampleForceNdisk, SampleForceNbulge;
+  int TypeOfVelocityStructure[4];
+  int MinParticlesPerBinForDispersionMeasurement;
+  int MinParticlesPerBinForDensityMeasurement;
+  double MType[4];
+  int NType[4];
+  double fac_value_rs[4], fac_value_ts[4], fac_value_qs[4], fac_value_ps[4];
+  /* grid geometry (grid.c:329-487) */
+  int FG_Nbin, DG_MaxLevel, EG_MaxLevel;
+  double FG_Rmin, FG_Fac, DG_Rmin, DG_Fac, EG_Rmin, EG_Fac;
+} galic_params_t;
+
+typedef struct galic_ctx galic_ctx;
+
+/* ---------------------------------------------------------- context */
+
+/* Creates a context on the current CUDA device and validates `prm`.
+ * Replaces the reference's global set-up (forcegrid_allocate,
+ * densitygrid_allocate, energygrid_allocate: grid.c:204-325). */
+int galic_ctx_create(const galic_params_t *prm, galic_ctx **out);
+void galic_ctx_destroy(galic_ctx *ctx);
+int galic_last_status(const galic_ctx *ctx);
+/* human-readable text of a status code */
+const char *galic_status_string(int status);
+
+/* Force grid: FG_Pot, FG_DPotDR, FG_DPotDz, each FG_Nbin^2 doubles
+ * (grid.c:59-197, filled by forcedensitygrid_calculate grid.c:621-763). */
+int galic_set_force_grid(galic_ctx *ctx, const double *pot, const double *dpotdr, const double *dpotdz);
+/* FG_Vstream[type], FG_Nbin^2 doubles (disp_fields.c:118-132). */
+int galic_set_vstream(galic_ctx *ctx, int type, const double *vstream);
+/* DG_CellSize (DG_Ngrid doubles, grid.c:849) and DGs_Distance
+ * (DG_Nstack doubles, grid.c:381-416). */
+int galic_set_density_geometry(galic_ctx *ctx, const double *cellsize, const double *dgs_distance);
+/* Target stacks of one type, each a full stack (DG_Nstack / EG_Nstack
+ * doubles, already smoothed): DGs_MassTarget, EGs_MassTarget,
+ * EGs_EgyTarget_{r,t,p,q} (grid.c:830-857, 941-1076). */
+int galic_set_targets(galic_ctx *ctx, int type, const double *dgs_mass, const double *egs_mass,
+                      const double *egs_r, const double *egs_t, const double *egs_p, const double *egs_q);
+/* Particle state P[] (allvars.h:844-868): pos/vel are n x 3 doubles,
+ * targets are n x 4 doubles (vr2_target, vt2_target, vp2_target,
+ * vq2_target), type in {1,2,3}. */
+int galic_set_particles(galic_ctx *ctx, int n, const double *pos, const double *vel, const double *mass,
+                        const double *tint, const double *vesc, const int *type, const double *targets);
+int galic_get_particles(galic_ctx *ctx, double *vel, int *orbits, double *vdisp /* n x 4: vr2,vt2,vp2,vq2 */);
+
+/* ---------------------------------------------------------- per-orbit drop-ins */
+
+/* Replaces produce_orbit_response_field_mod (orbit_response.c:155-491,
+ * proto.h:142-145); same arguments after the context, q before p.  Output
+ * grids are caller-owned host arrays of DG_Ngrid (= EG_Ngrid) doubles,
+ * zeroed, filled and scaled by mass/tall by the callee.  Returns tall, or a
+ * negative value on error (see galic_last_status). */
+double galic_produce_orbit_response_field_mod(galic_ctx *ctx, double *pos, double *vel, int id, double *mfield,
+                                              double *egyfield_r, double *egyfield_t, double *egyfield_q,
+                                              double *egyfield_p, double mass, double timespan,
+                                              int *orbitstaken, int type);
+/* Replaces produce_orbit_response_field (orbit_response.c:33-151). */
+double galic_produce_orbit_response_field(galic_ctx *ctx, double *pos, double *vel, int id, double *mfield,
+                                          double mass, double timespan, int *orbitstaken);
+
+/* ---------------------------------------------------------- batched hot path */
+
+/* Replaces calc_all_response_fields (main.c:151-246) including its final
+ * calc_global_fit (main.c:251-362): integrates every particle's orbit,
+ * bins the time-averaged responses per type with exact fixed-point
+ * accumulation, adds the instantaneous energy grid, and evaluates the fit. */
+int galic_calc_all_response_fields(galic_ctx *ctx, int form);
+
+/* One optimisation repetition: init_updates (main.c:844-874), optimize(n)
+ * for n = idx[0..count-1] (main.c:365-527) and commit_updates
+ * (main.c:808-841), which ends in calc_global_fit.  Proposals for idx[k] are
+ * drawn from Philox stream (seed, idx[k], rep_serial).  All count
+ * particles are evaluated against the committed state, as in the reference
+ * (accepted changes only reach `_delta` grids until the commit). */
+int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial, int form);
+
+/* Merit values of the last calc_global_fit: per type (index 1..3)
+ * S, Sdisp_r, Sdisp_t, Sdisp_p, Sdisp_q, Srelfac, Srelfac_count
+ * (main.c:294-358): out is 4 x 7 doubles, row = type. */
+int galic_get_fit(galic_ctx *ctx, double *out);
+/* Counters of optimize (main.c:468, 505): tries[4], changes[4]. */
+int galic_get_counters(galic_ctx *ctx, long long *tries, long long *changes);
+
+/* Committed response grids of one type (DG_Ngrid doubles each), the
+ * reference's DG_MassLoc, EG_EgyResponse{R,T,Q,P}LocS, EG_MassLoc,
+ * EG_EgyResponse{R,T,P,Q}Loc; `which` selects one of them (galic_grid_id). */
+typedef enum {
+  GALIC_GRID_MASS_S = 0, GALIC_GRID_R_S, GALIC_GRID_T_S, GALIC_GRID_Q_S, GALIC_GRID_P_S,
+  GALIC_GRID_MASS_I, GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I,
+  GALIC_GRID_COUNT
+} galic_grid_id;
+int galic_get_response(galic_ctx *ctx, int type, int which, double *out);
+
+/* Per-orbit step cap (reference: 1e8 steps, orbit_response.c:450, then
+ * exit(1)); an orbit that exceeds it ends with GALIC_ERR_STEP_CAP. */
+int galic_set_step_cap(galic_ctx *ctx, long long cap);
+
+/* Total orbit steps taken by the last batched call (for throughput). */
+long long galic_last_orbit_steps(const galic_ctx *ctx);
+/* Device time of the last galic_calc_all_response_fields, measured with CUDA
+ * events on the library's stream: the whole call and its orbit kernel (ms). */
+int galic_last_timing(const galic_ctx *ctx, double *ms_total, double *ms_orbit_kernel);
+/* Largest relative orbit energy error of the last batched call
+ * (orbit_response.c:460-462; the reference only prints it above 0.5). */
+double galic_last_max_energy_error(const galic_ctx *ctx);
+/* Number of kernels launched by the last batched call. */
+int galic_last_kernel_launches(const galic_ctx *ctx);
+
+/* ---------------------------------------------------------- host helpers */
+
+/* Grid geometry of forcedensitygrid_create (grid.c:329-480): from Halo_A,
+ * the enclosed-mass fractions and the bin counts computes Rmax, DG_Rin,
+ * the spacing factors and Rmin of the DG, FG and EG grids.
+ * out: Rmax, DG_Rin, DG_Fac, DG_Rmin, FG_Fac, FG_Rmin, EG_Fac, EG_Rmin. */
+int galic_grid_geometry(double halo_a, double outer_frac, double inner_frac, int fg_nbin, int dg_maxlevel,
+                        int eg_maxlevel, double *out);
+/* DGs_Distance stack (grid.c:381-416) and DG_CellSize/DG_CellVol
+ * (grid.c:830-850) for DG_MaxLevel with spacing (dg_rmin, dg_fac). */
+int galic_density_geometry(int dg_maxlevel, double dg_rmin, double dg_fac, double *dgs_distance,
+                           double *cellsize, double *cellvol);
+/* smooth_stack (grid.c:1247-1265) on a host stack, in place. */
+void galic_smooth_stack(double *data, int maxlevel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,305 @@
+"""ctypes access to the CPU oracle (test infrastructure only).
+
+* `Oracle` drives oracle/liboracle.so, the C restatement of GALIC's hot path
+  (oracle/galic_oracle.c), with either glibc's or the project's
+  transcendental functions.
+* `Reference` drives oracle/_ref/libgalic_ref.so, GALIC's own C compiled with
+  the single-rank MPI / GSL stand-ins.  The reference keeps process-wide
+  globals (and calls exit() on fatal errors), so `run_reference` executes each
+  scenario in a fresh spawned process.
+"""
+import ctypes as C
+import multiprocessing as mp
+import os
+import subprocess
+
+import numpy as np
+
+from galic_b200 import _ffi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref.so")
+REF_SRC = "/root/reference/src"
+
+dptr, iptr = _ffi.dptr, _ffi.iptr
+PD, PI, VP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+PP = C.POINTER(_ffi.GalicParams)
+
+
+def build_oracle():
+    """Compiles oracle/liboracle.so (and oracle/_ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "restatement"], check=True)
+    if os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF_SRC={REF_SRC}"],
+                       check=True)
+
+
+def reference_available():
+    return os.path.exists(REF_SO)
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        L = C.CDLL(ORACLE_SO)
+        sig = {
+            "orc_create": (VP, [PP, C.c_int]),
+            "orc_destroy": (None, [VP]),
+            "orc_set_step_cap": (None, [VP, C.c_longlong]),
+            "orc_set_force_grid": (None, [VP, PD, PD, PD]),
+            "orc_set_vstream": (None, [VP, C.c_int, PD]),
+            "orc_set_density_geometry": (None, [VP, PD, PD]),
+            "orc_set_targets": (None, [VP, C.c_int, PD, PD, PD, PD, PD, PD]),
+            "orc_set_particles": (None, [VP, C.c_int, PD, PD, PD, PD, PD, PI, PD]),
+            "orc_get_particles": (None, [VP, PD, PI, PD]),
+            "orc_forcegrid_acc": (None, [VP, PD, PD]),
+            "orc_forcegrid_pot": (C.c_double, [VP, PD]),
+            "orc_densitygrid_cell": (None, [VP, PD, PI, PI, PD, PD]),
+            "orc_vstream": (C.c_double, [VP, PD, C.c_int]),
+            "orc_orbit_mod": (C.c_double, [VP, PD, PD, PD, PD, PD, PD, PD, C.c_double, C.c_double, PI, C.c_int, PD]),
+            "orc_orbit": (C.c_double, [VP, PD, PD, PD, C.c_double, C.c_double, PI, PD]),
+            "orc_smooth_stack": (None, [PD, C.c_int]),
+            "orc_stack_difference": (C.c_double, [VP, PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
+            "orc_stack_difference_mod": (C.c_double, [VP, PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
+            "orc_calc_all": (C.c_int, [VP]),
+            "orc_optimize_rep": (C.c_int, [VP, PI, C.c_int, C.c_uint64, C.c_uint32]),
+            "orc_get_fit": (None, [VP, PD]),
+            "orc_get_counters": (None, [VP, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+            "orc_get_response": (None, [VP, C.c_int, C.c_int, PD]),
+            "orc_steps_total": (C.c_longlong, [VP]),
+            "orc_grid_geometry": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
+            "orc_density_geometry": (C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _olib = L
+    return _olib
+
+
+class Oracle:
+    """The C restatement; use_libm=True pins it to the reference, False matches the CUDA kernels."""
+
+    def __init__(self, params, use_libm=False):
+        self.L = oracle_lib()
+        self.params = params.copy()
+        self.h = self.L.orc_create(C.byref(self.params), 1 if use_libm else 0)
+        Lv = params.DG_MaxLevel
+        self.ngrid = 1 << (2 * Lv)
+        self.nstack = ((1 << (2 + 2 * Lv)) - 1) // 3
+        self.n = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def load_model(self, m, particles=True):
+        self.L.orc_set_force_grid(self.h, dptr(m.pot), dptr(m.dpotdr), dptr(m.dpotdz))
+        for t in (1, 2, 3):
+            self.L.orc_set_vstream(self.h, t, dptr(np.ascontiguousarray(m.vstream[t], dtype=np.float64)))
+        self.L.orc_set_density_geometry(self.h, dptr(m.cellsize), dptr(m.dgs_distance))
+        for t, tg in m.targets.items():
+            self.L.orc_set_targets(self.h, t, *[dptr(np.ascontiguousarray(a)) for a in tg])
+        if particles:
+            self.set_particles(m.pos, m.vel, m.mass, m.tint, m.vesc, m.ptype, m.ptargets)
+
+    def set_particles(self, pos, vel, mass, tint, vesc, ptype, ptargets):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (pos, vel, mass, tint, vesc)]
+        self.L.orc_set_particles(self.h, len(mass), *[dptr(a) for a in arrs],
+                                 iptr(np.ascontiguousarray(ptype, dtype=np.int32)),
+                                 dptr(np.ascontiguousarray(ptargets, dtype=np.float64)))
+        self.n = len(mass)
+
+    def orbit_mod(self, pos, vel, mass, timespan, ptype):
+        g = [np.zeros(self.ngrid) for _ in range(5)]
+        orbits = C.c_int(0)
+        info = np.zeros(2)
+        tall = self.L.orc_orbit_mod(self.h, dptr(np.ascontiguousarray(pos, dtype=np.float64)),
+                                    dptr(np.ascontiguousarray(vel, dtype=np.float64)), *[dptr(a) for a in g],
+                                    float(mass), float(timespan), C.byref(orbits), int(ptype), dptr(info))
+        return tall, orbits.value, g[0], g[1], g[2], g[3], g[4], info
+
+    def orbit(self, pos, vel, mass, timespan):
+        m = np.zeros(self.ngrid)
+        orbits = C.c_int(0)
+        info = np.zeros(2)
+        tall = self.L.orc_orbit(self.h, dptr(np.ascontiguousarray(pos, dtype=np.float64)),
+                                dptr(np.ascontiguousarray(vel, dtype=np.float64)), dptr(m), float(mass),
+                                float(timespan), C.byref(orbits), dptr(info))
+        return tall, orbits.value, m, info
+
+    def calc_all(self):
+        return self.L.orc_calc_all(self.h)
+
+    def optimize_rep(self, idx, seed, rep_serial):
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        return self.L.orc_optimize_rep(self.h, iptr(idx), len(idx), int(seed), int(rep_serial))
+
+    def fit(self):
+        out = np.zeros(28)
+        self.L.orc_get_fit(self.h, dptr(out))
+        return out.reshape(4, 7)
+
+    def counters(self):
+        tr = np.zeros(4, dtype=np.int64)
+        ch = np.zeros(4, dtype=np.int64)
+        self.L.orc_get_counters(self.h, _ffi.llptr(tr), _ffi.llptr(ch))
+        return tr, ch
+
+    def response(self, ptype, which):
+        out = np.zeros(self.ngrid)
+        self.L.orc_get_response(self.h, int(ptype), int(which), dptr(out))
+        return out
+
+    def particles(self):
+        vel = np.zeros((self.n, 3))
+        orbits = np.zeros(self.n, dtype=np.int32)
+        vdisp = np.zeros((self.n, 4))
+        self.L.orc_get_particles(self.h, dptr(vel), iptr(orbits), dptr(vdisp))
+        return vel, orbits, vdisp
+
+    def steps_total(self):
+        return self.L.orc_steps_total(self.h)
+
+
+# --------------------------------------------------------------- the reference
+
+
+def _ref_lib():
+    L = C.CDLL(REF_SO)
+    sig = {
+        "ref_setup": (C.c_int, [PP]),
+        "ref_set_force_grid": (None, [PD, PD, PD]),
+        "ref_set_vstream": (None, [C.c_int, PD]),
+        "ref_set_density_geometry": (None, [PD, PD]),
+        "ref_set_targets": (None, [C.c_int, PD, PD, PD, PD, PD, PD]),
+        "ref_set_particles": (None, [C.c_int, PD, PD, PD, PD, PD, PI, PD]),
+        "ref_get_particles": (None, [PD, PI, PD]),
+        "ref_orbit_mod": (C.c_double, [PD, PD, PD, PD, PD, PD, PD, C.c_double, C.c_double, PI, C.c_int]),
+        "ref_orbit": (C.c_double, [PD, PD, PD, C.c_double, C.c_double, PI]),
+        "ref_forcegrid_acc": (None, [PD, PD]),
+        "ref_forcegrid_pot": (C.c_double, [PD]),
+        "ref_densitygrid_cell": (None, [PD, PI, PI, PD, PD]),
+        "ref_vstream": (C.c_double, [PD, C.c_int]),
+        "ref_calc_all": (None, []),
+        "ref_optimize_rep": (None, [PI, C.c_int, C.c_ulonglong, C.c_uint]),
+        "ref_get_fit": (None, [PD]),
+        "ref_get_counters": (None, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+        "ref_get_response": (None, [C.c_int, C.c_int, PD]),
+        "ref_smooth_stack": (None, [PD, C.c_int]),
+        "ref_stack_difference": (C.c_double, [PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
+        "ref_stack_difference_mod": (C.c_double, [PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
+        "ref_geometry": (C.c_int, [C.c_char_p, C.c_double, C.c_double, PD, PD, PD, PD]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+class Reference:
+    """GALIC's own C (one model per process: the reference keeps globals)."""
+
+    def __init__(self, params):
+        self.L = _ref_lib()
+        self.params = params.copy()
+        self.L.ref_setup(C.byref(self.params))
+        Lv = params.DG_MaxLevel
+        self.ngrid = 1 << (2 * Lv)
+        self.nstack = ((1 << (2 + 2 * Lv)) - 1) // 3
+        self.n = 0
+
+    def load_model(self, m, particles=True):
+        self.L.ref_set_force_grid(dptr(m.pot), dptr(m.dpotdr), dptr(m.dpotdz))
+        for t in (1, 2, 3):
+            self.L.ref_set_vstream(t, dptr(np.ascontiguousarray(m.vstream[t], dtype=np.float64)))
+        self.L.ref_set_density_geometry(dptr(m.cellsize), dptr(m.dgs_distance))
+        for t, tg in m.targets.items():
+            self.L.ref_set_targets(t, *[dptr(np.ascontiguousarray(a)) for a in tg])
+        if not particles:
+            return
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (m.pos, m.vel, m.mass, m.tint, m.vesc)]
+        self.L.ref_set_particles(len(m.mass), *[dptr(a) for a in arrs],
+                                 iptr(np.ascontiguousarray(m.ptype, dtype=np.int32)),
+                                 dptr(np.ascontiguousarray(m.ptargets, dtype=np.float64)))
+        self.n = len(m.mass)
+
+    def orbit_mod(self, pos, vel, mass, timespan, ptype):
+        g = [np.zeros(self.ngrid) for _ in range(5)]
+        orbits = C.c_int(0)
+        p = np.array(pos, dtype=np.float64)
+        v = np.array(vel, dtype=np.float64)
+        tall = self.L.ref_orbit_mod(dptr(p), dptr(v), *[dptr(a) for a in g], float(mass), float(timespan),
+                                    C.byref(orbits), int(ptype))
+        return tall, orbits.value, g[0], g[1], g[2], g[3], g[4]
+
+    def orbit(self, pos, vel, mass, timespan):
+        m = np.zeros(self.ngrid)
+        orbits = C.c_int(0)
+        p = np.array(pos, dtype=np.float64)
+        v = np.array(vel, dtype=np.float64)
+        tall = self.L.ref_orbit(dptr(p), dptr(v), dptr(m), float(mass), float(timespan), C.byref(orbits))
+        return tall, orbits.value, m
+
+    def calc_all(self):
+        self.L.ref_calc_all()
+
+    def optimize_rep(self, idx, seed, rep_serial):
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        self.L.ref_optimize_rep(iptr(idx), len(idx), int(seed), int(rep_serial))
+
+    def fit(self):
+        out = np.zeros(28)
+        self.L.ref_get_fit(dptr(out))
+        return out.reshape(4, 7)
+
+    def counters(self):
+        tr = np.zeros(4, dtype=np.int64)
+        ch = np.zeros(4, dtype=np.int64)
+        self.L.ref_get_counters(_ffi.llptr(tr), _ffi.llptr(ch))
+        return tr, ch
+
+    def response(self, ptype, which):
+        out = np.zeros(self.ngrid)
+        self.L.ref_get_response(int(ptype), int(which), dptr(out))
+        return out
+
+    def particles(self):
+        vel = np.zeros((self.n, 3))
+        orbits = np.zeros(self.n, dtype=np.int32)
+        vdisp = np.zeros((self.n, 4))
+        self.L.ref_get_particles(dptr(vel), iptr(orbits), dptr(vdisp))
+        return vel, orbits, vdisp
+
+
+def _child(fn, args, q):
+    try:
+        q.put(("ok", fn(*args)))
+    except BaseException as e:  # noqa: BLE001
+        q.put(("err", repr(e)))
+
+
+def run_reference(fn, *args, timeout=600):
+    """Runs fn(*args) in a fresh spawned process (fn must be importable)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_child, args=(fn, args, q))
+    p.start()
+    try:
+        kind, val = q.get(timeout=timeout)
+    finally:
+        p.join(timeout=30)
+        if p.is_alive():
+            p.kill()
+    if kind != "ok":
+        raise RuntimeError(f"reference scenario failed: {val}")
+    return val

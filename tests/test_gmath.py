@@ -1,0 +1,80 @@
+"""The project's elementary functions (galic_b200/csrc/gmath.h) against glibc.
+
+gmath.h replaces log/atan2/sin/cos/acos on the orbit path so that the CUDA
+kernels and the CPU restatement agree bit for bit; these tests bound its
+error against glibc over the argument ranges the path uses."""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+SRC = r'''
+#include "gmath.h"
+double t_log(double x) { return gm_log(x); }
+double t_atan2(double y, double x) { return gm_atan2(y, x); }
+double t_sin(double x) { return gm_sin(x); }
+double t_cos(double x) { return gm_cos(x); }
+double t_acos(double x) { return gm_acos(x); }
+'''
+
+
+@pytest.fixture(scope="module")
+def gm(tmp_path_factory):
+    d = tmp_path_factory.mktemp("gm")
+    src = d / "t.c"
+    src.write_text(SRC)
+    so = d / "libt.so"
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I",
+                    os.path.join(ROOT, "galic_b200", "csrc"), str(src), "-o", str(so)], check=True)
+    L = C.CDLL(str(so))
+    for n, k in (("t_log", 1), ("t_atan2", 2), ("t_sin", 1), ("t_cos", 1), ("t_acos", 1)):
+        f = getattr(L, n)
+        f.restype = C.c_double
+        f.argtypes = [C.c_double] * k
+    return L
+
+
+def ulps(a, b):
+    if a == b:
+        return 0.0
+    return abs(a - b) / abs(math.nextafter(b, math.inf) - b)
+
+
+def test_log_within_one_ulp(gm):
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([np.exp(rng.uniform(-700, 700, 20000)), 1 + rng.random(20000) * 1e4,
+                         [1.0, 2.0, 0.5, 1e-310, 5e-324, 1.7976931348623157e308]])
+    assert max(ulps(gm.t_log(x), math.log(x)) for x in xs) <= 1.0
+    assert gm.t_log(1.0) == 0.0
+    assert math.isinf(gm.t_log(0.0)) and gm.t_log(0.0) < 0
+    assert math.isnan(gm.t_log(-1.0))
+
+
+def test_atan2_within_two_ulp_and_signed_zeros(gm):
+    rng = np.random.default_rng(2)
+    a = rng.uniform(-1, 1, 20000) * 10 ** rng.uniform(-5, 5, 20000)
+    b = rng.uniform(-1, 1, 20000) * 10 ** rng.uniform(-5, 5, 20000)
+    assert max(ulps(gm.t_atan2(y, x), math.atan2(y, x)) for y, x in zip(a, b)) <= 2.0
+    for y, x in ((0.0, 0.0), (-0.0, 0.0), (0.0, -0.0), (-0.0, -0.0), (0.0, -1.0), (-0.0, -1.0), (1.0, 0.0),
+                 (-1.0, 0.0), (math.inf, math.inf), (1.0, -math.inf)):
+        assert gm.t_atan2(y, x) == math.atan2(y, x)
+        assert math.copysign(1, gm.t_atan2(y, x)) == math.copysign(1, math.atan2(y, x))
+
+
+def test_sin_cos_within_one_ulp(gm):
+    rng = np.random.default_rng(3)
+    xs = np.concatenate([rng.uniform(-math.pi, math.pi, 20000), rng.uniform(-300, 300, 5000), [0.0, -0.0, 1e-30]])
+    assert max(ulps(gm.t_sin(x), math.sin(x)) for x in xs) <= 1.0
+    assert max(ulps(gm.t_cos(x), math.cos(x)) for x in xs) <= 1.0
+
+
+def test_acos_within_two_ulp(gm):
+    rng = np.random.default_rng(4)
+    xs = np.concatenate([rng.uniform(-1, 1, 20000), [1.0, -1.0, 0.0, 1 - 2 ** -52, -1 + 2 ** -53]])
+    assert max(ulps(gm.t_acos(x), math.acos(x)) for x in xs) <= 2.0
+    assert math.isnan(gm.t_acos(1.5))

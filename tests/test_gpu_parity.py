@@ -1,0 +1,148 @@
+"""CUDA path (through the C ABI) against the oracle and the golden fixtures.
+
+* Per orbit, the FP64 kernels reproduce the restatement with the project's
+  math functions bit for bit (same IEEE operations, same order, no
+  contraction), and GALIC's own output within BIN_TOL.
+* The batched response (exact fixed-point sums instead of the reference's
+  sequential FP64 sums) matches the restatement within 1e-12 of each grid's
+  peak bin, and the fit within 1e-10.
+* An optimisation repetition makes the same accept decisions and leaves the
+  same velocities.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import golden_lib
+from galic_b200 import Context, GalicError, synth
+from oracle_lib import Oracle
+
+pytestmark = pytest.mark.gpu
+
+BIN_TOL = 1e-9        # against GALIC's own C (math library differences)
+BATCH_TOL = 1e-12     # batched fixed-point sums vs sequential FP64 sums, per grid peak
+FIT_TOL = 1e-10
+FIT_ATOL = 1e-14
+
+
+def peak_rel(a, b):
+    den = np.max(np.abs(b), axis=-1, keepdims=True)
+    den = np.where(den == 0, 1, den)
+    return float(np.max(np.abs(a - b) / den))
+
+
+@pytest.fixture(params=golden_lib.GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def golden(request):
+    return golden_lib.load(request.param)
+
+
+def test_orbits_bit_exact_vs_oracle_and_close_to_reference(golden):
+    ins, outs = golden
+    m = golden_lib.model(ins)
+    o = Oracle(m.params, use_libm=False)
+    o.load_model(m)
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        for i in range(m.n):
+            a = ctx.produce_orbit_response_field_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])
+            b = o.orbit_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])
+            assert a[0] == b[0] and a[1] == b[1], i
+            for k in range(2, 7):
+                assert np.array_equal(a[k], b[k]), (i, k)
+        for key in golden_lib.orbit_keys(outs):
+            i = int(outs[f"{key}_idx"])
+            a = ctx.produce_orbit_response_field_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])
+            assert abs(a[0] - outs[f"{key}_tall"]) <= 1e-12 * a[0]
+            assert peak_rel(np.stack(a[2:]), outs[f"{key}_grids"]) < BIN_TOL
+        for j in range(3):
+            i = int(outs[f"orbit{j}_idx"])
+            tall, norbit, mm = ctx.produce_orbit_response_field(m.pos[i], m.vel[i], m.mass[i], m.tint[i])
+            tb, nb, mb, _ = o.orbit(m.pos[i], m.vel[i], m.mass[i], m.tint[i])
+            assert tall == tb and norbit == nb and np.array_equal(mm, mb)
+
+
+def test_calc_all_and_rep_vs_oracle(golden):
+    ins, outs = golden
+    m = golden_lib.model(ins)
+    o = Oracle(m.params, use_libm=False)
+    o.load_model(m)
+    assert o.calc_all() == 0
+    present = [t for t in (1, 2, 3) if m.params.NType[t]]
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.calc_all_response_fields()
+        for t in present:
+            got = np.stack([ctx.response(t, w) for w in range(10)])
+            want = np.stack([o.response(t, w) for w in range(10)])
+            assert peak_rel(got, want) < BATCH_TOL, t
+            assert peak_rel(got, outs[f"calc_resp{t}"]) < BIN_TOL, t
+        f, g = ctx.fit()[present, :5], o.fit()[present, :5]
+        assert np.all(np.abs(f - g) <= FIT_TOL * np.abs(g) + FIT_ATOL)
+        vel, orbits, vdisp = ctx.particles()
+        ov, oo, od = o.particles()
+        assert np.array_equal(orbits, oo)
+        assert np.array_equal(vdisp, od)
+        idx = outs["rep_idx"]
+        ctx.optimize_rep(idx, 987654321, 7)
+        assert o.optimize_rep(idx, 987654321, 7) == 0
+        tr, ch = ctx.counters()
+        otr, och = o.counters()
+        assert np.array_equal(tr, otr) and np.array_equal(ch, och)
+        vel, orbits, vdisp = ctx.particles()
+        ov, oo, od = o.particles()
+        assert np.array_equal(vel, ov)
+        assert np.array_equal(orbits, oo)
+        f, g = ctx.fit()[present, :5], o.fit()[present, :5]
+        assert np.all(np.abs(f - g) <= FIT_TOL * np.abs(g) + FIT_ATOL)
+
+
+def test_batched_deterministic_and_matches_oracle_larger_model():
+    m = synth.config_halo_disk(n_halo=1500, n_disk=500, level=6, seed=5)
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.calc_all_response_fields()
+        r1 = np.stack([ctx.response(t, w) for t in (1, 2) for w in range(10)])
+        f1 = ctx.fit()
+        steps = ctx.last_orbit_steps()
+        ctx.calc_all_response_fields()
+        r2 = np.stack([ctx.response(t, w) for t in (1, 2) for w in range(10)])
+        assert np.array_equal(r1, r2)  # order-independent fixed-point sums
+        assert np.array_equal(f1, ctx.fit())
+    o = Oracle(m.params, use_libm=False)
+    o.load_model(m)
+    assert o.calc_all() == 0
+    want = np.stack([o.response(t, w) for t in (1, 2) for w in range(10)])
+    assert peak_rel(r1, want) < BATCH_TOL
+    assert steps == o.steps_total()
+
+
+def test_step_cap_reports_status_and_context_survives():
+    m = synth.config_halo(n=64, level=5, seed=9)
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.set_step_cap(10)
+        with pytest.raises(GalicError) as e:
+            ctx.calc_all_response_fields()
+        assert e.value.status == 2
+        with pytest.raises(GalicError) as e:
+            ctx.produce_orbit_response_field_mod(m.pos[0], m.vel[0], m.mass[0], m.tint[0], 1)
+        assert e.value.status == 2
+        ctx.set_step_cap(100000000)
+        ctx.calc_all_response_fields()
+        assert np.isfinite(ctx.fit()[1, 0])
+
+
+def test_invalid_repetition_lists_rejected():
+    m = synth.config_halo(n=64, level=5, seed=10)
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        with pytest.raises(GalicError) as e:
+            ctx.optimize_rep([1, 2], 1, 0)  # before any response: out of order
+        assert e.value.status == 9
+        ctx.calc_all_response_fields()
+        for bad in ([1, 1], [-1], [64]):
+            with pytest.raises(GalicError) as e:
+                ctx.optimize_rep(bad, 1, 0)
+            assert e.value.status == 1
+        ctx.optimize_rep([], 1, 0)
