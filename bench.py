@@ -298,7 +298,7 @@ def ours_arm(args, rank, world, local_rank):
         kern_avg = sum(kern_ms) / len(kern_ms)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
-        if world == 1:
+        if world == 1 and args.cpu_seconds > 0:
             v, kind, cores, orbits, st = cpu_orbit_steps_per_s(model, args.cpu_seconds)
             cpu = {"value": v, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
                    "sample": f"{orbits} orbits ({st} orbit-steps) of this workload, {cores} processes, "

@@ -40,8 +40,9 @@ def build(verbose=False):
         objs.append(obj)
         if not _needs(obj, [src] + headers + [__file__]):
             continue
-        fmad = "--fmad=true" if f.endswith("_fp32.cu") else "--fmad=false"
-        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", fmad, "-Xcompiler", "-fPIC,-ffp-contract=off",
+        fp32 = f.endswith("_fp32.cu")
+        fmad = ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"] if fp32 else ["--fmad=false"]
+        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", *fmad, "-Xcompiler", "-fPIC,-ffp-contract=off",
                "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-c", src, "-o", obj]
         if f.endswith(".cu"):
             cmd += ["-Xptxas", "-warn-spills"]

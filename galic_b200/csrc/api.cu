@@ -60,6 +60,12 @@ struct galic_ctx {
   int last_launches = 0;
   double last_max_egy_err = 0;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  // FP32 form: one float4 table {DPotDR, DPotDz, Vstream[type], 0} per type
+  std::vector<double> h_dpotdr, h_dpotdz, h_vstream[4];
+  float4 *d_tab32[4] = {nullptr, nullptr, nullptr, nullptr};
+  float *d_cellsize32 = nullptr;
+  bool tab32_dirty = true;
+  std::vector<double> h_cellsize;
   double last_ms_total = 0, last_ms_orbit = 0;
 };
 
@@ -213,6 +219,32 @@ void set_shifts(galic_ctx *ctx, int *shift)
   }
 }
 
+// float4 tables of the FP32 form, rebuilt after any table upload
+int ensure_tab32(galic_ctx *ctx)
+{
+  if(!ctx->tab32_dirty) return GALIC_OK;
+  const int NF = ctx->prm.FG_Nbin * ctx->prm.FG_Nbin;
+  if(ctx->h_dpotdr.size() != (size_t) NF) {
+    ctx->h_dpotdr.assign(NF, 0.0);
+    ctx->h_dpotdz.assign(NF, 0.0);
+  }
+  std::vector<float4> tab(NF);
+  for(int t = 1; t <= 3; t++) {
+    if(!ctx->d_tab32[t]) CK(dalloc(&ctx->d_tab32[t], NF));
+    for(int i = 0; i < NF; i++) {
+      double vs = ctx->h_vstream[t].size() == (size_t) NF ? ctx->h_vstream[t][i] : 0.0;
+      tab[i] = make_float4((float) ctx->h_dpotdr[i], (float) ctx->h_dpotdz[i], (float) vs, 0.f);
+    }
+    CK(cudaMemcpy(ctx->d_tab32[t], tab.data(), NF * sizeof(float4), cudaMemcpyHostToDevice));
+  }
+  if(!ctx->d_cellsize32) CK(dalloc(&ctx->d_cellsize32, ctx->G));
+  std::vector<float> cs(ctx->G);
+  for(int i = 0; i < ctx->G; i++) cs[i] = (float) ctx->h_cellsize[i];
+  CK(cudaMemcpy(ctx->d_cellsize32, cs.data(), ctx->G * sizeof(float), cudaMemcpyHostToDevice));
+  ctx->tab32_dirty = false;
+  return GALIC_OK;
+}
+
 }  // namespace
 
 extern "C" const char *galic_status_string(int status)
@@ -332,6 +364,8 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx->d_b_steps);
   dfree(ctx->d_idx); dfree(ctx->d_accepted); dfree(ctx->d_vel_try); dfree(ctx->d_F); dfree(ctx->d_inst_v);
   dfree(ctx->d_inst_cell);
+  for(int t = 0; t < 4; t++) dfree(ctx->d_tab32[t]);
+  dfree(ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
     if(ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
   if(ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -349,6 +383,9 @@ extern "C" int galic_set_force_grid(galic_ctx *ctx, const double *pot, const dou
     if(pot[i] < pmin) pmin = pot[i];
   }
   ctx->pot_min = pmin;
+  ctx->h_dpotdr.assign(dpotdr, dpotdr + NF);
+  ctx->h_dpotdz.assign(dpotdz, dpotdz + NF);
+  ctx->tab32_dirty = true;
   CK(cudaMemcpy(ctx->d_fg_acc, acc.data(), NF * sizeof(double2), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_fg_pot, pot, NF * sizeof(double), cudaMemcpyHostToDevice));
   ctx->have_fg = true;
@@ -366,6 +403,8 @@ extern "C" int galic_set_vstream(galic_ctx *ctx, int type, const double *v)
     if(b != 0) zero = 0;  // only +0.0 everywhere allows skipping the lookup
   }
   ctx->dm.vstream_zero[type] = zero;
+  ctx->h_vstream[type].assign(v, v + NF);
+  ctx->tab32_dirty = true;
   CK(cudaMemcpy(ctx->d_vstream[type], v, NF * sizeof(double), cudaMemcpyHostToDevice));
   return fail(ctx, GALIC_OK);
 }
@@ -374,6 +413,8 @@ extern "C" int galic_set_density_geometry(galic_ctx *ctx, const double *cellsize
 {
   if(!ctx || !cellsize || !dist) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   CK(cudaMemcpy(ctx->d_cellsize, cellsize, ctx->G * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->h_cellsize.assign(cellsize, cellsize + ctx->G);
+  ctx->tab32_dirty = true;
   CK(cudaMemcpy(ctx->d_dist, dist, ctx->Ns * sizeof(double), cudaMemcpyHostToDevice));
   ctx->have_geom = true;
   return fail(ctx, GALIC_OK);
@@ -529,8 +570,11 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
 {
   if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
   if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
-  if(form == GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_UNSUPPORTED);
   if(ctx->n == 0 || !ctx->have_geom) return fail(ctx, GALIC_ERR_STATE);
+  if(form == GALIC_FORM_FP32) {
+    int st = ensure_tab32(ctx);
+    if(st) return st;
+  }
   const galic_params_t &p = ctx->prm;
   for(int t = 1; t <= 3; t++)
     if(p.NType[t] > 0 && !ctx->have_targets[t]) return fail(ctx, GALIC_ERR_STATE);
@@ -561,8 +605,8 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   a.max_egy_err = ctx->d_maxerr;
   a.status = ctx->d_status;
   int launches = 0;
-  const int block = 128;
-  int per_sm = calc_all_occupancy(block);
+  const int block = form == GALIC_FORM_FP32 ? 256 : 128;
+  int per_sm = form == GALIC_FORM_FP32 ? calc_all_fp32_occupancy(block) : calc_all_occupancy(block);
   if(per_sm < 1) per_sm = 1;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -570,7 +614,10 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   int need = (ctx->n + block - 1) / block;
   if(grid > need) grid = need;
   CK(cudaEventRecord(ctx->ev[1], s));
-  launches += launch_calc_all_fp64(ctx->dm, a, grid, block, s);
+  if(form == GALIC_FORM_FP32)
+    launches += launch_calc_all_fp32(ctx->dm, ctx->d_tab32, ctx->d_cellsize32, a, grid, block, s);
+  else
+    launches += launch_calc_all_fp64(ctx->dm, a, grid, block, s);
   CK(cudaEventRecord(ctx->ev[2], s));
   launch_instantaneous(ctx->dm, ctx->n, ctx->d_pos, ctx->d_vel, ctx->d_mass, ctx->d_type, ctx->d_vdisp, ctx->d_fx,
                        ctx->d_shift, G, s);

@@ -21,7 +21,7 @@
 
 namespace {
 
-__global__ void k_fit_smooth(FitArgs f)
+__global__ void __launch_bounds__(1024) k_fit_smooth(FitArgs f)
 {
   extern __shared__ double sm[];
   const int type = blockIdx.x / NG_COMMITTED, g = blockIdx.x % NG_COMMITTED;
@@ -36,7 +36,7 @@ __global__ void k_fit_smooth(FitArgs f)
 }
 
 // raw[type][w]: w = 0 S, 1 Sdisp_r, 2 Sdisp_t, 3 Sdisp_p, 4 Sdisp_q
-__global__ void k_fit_diff(FitArgs f, double *raw)
+__global__ void __launch_bounds__(1024) k_fit_diff(FitArgs f, double *raw)
 {
   extern __shared__ double sm[];
   const int type = blockIdx.x / 5, w = blockIdx.x % 5;
@@ -159,7 +159,7 @@ __global__ void k_propose(DevModel M, RepArgs R)
 }
 
 // one CTA per (particle k, which): which 0 = F_base, 1 = F_try
-__global__ void k_eval_fit(DevModel M, RepArgs R, FitArgs f)
+__global__ void __launch_bounds__(256) k_eval_fit(DevModel M, RepArgs R, FitArgs f)
 {
   extern __shared__ double sm[];
   __shared__ double sh_d[4];
@@ -354,7 +354,7 @@ int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const Orbi
   launch_scale_dense(M, b, s);
   launches += 2;
   size_t smem = (size_t) f.Nstack * sizeof(double);
-  k_eval_fit<<<2 * count, 1024, smem, s>>>(M, R, f);
+  k_eval_fit<<<2 * count, 256, smem, s>>>(M, R, f);
   k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R);
   k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
   k_inst_delta<<<148 * 8, 256, 0, s>>>(R, f);

@@ -1,0 +1,42 @@
+// Warp-cooperative flush of merged deposits into the fixed-point grids.
+//
+// Each lane of the batched orbit kernels merges the deposits of consecutive
+// steps that fall into the same DG cell in registers (20 values: 4 corners x
+// {m, m vr2, m vt2, m vq2, m vp2}).  When its cell changes, the lane only
+// parks the 20 values (already scaled by mass/Tint) in its slot of a per-warp
+// shared-memory queue.  At one fixed point of every loop iteration the whole
+// warp drains all parked slots together: item k of slot s is handled by lane
+// k mod 32, so the fixed-point conversion and the two integer atomics of every
+// value run on full warps instead of on the one lane whose cell changed.
+#ifndef GALIC_FLUSH_CUH
+#define GALIC_FLUSH_CUH
+
+#include "fixedpoint.cuh"
+#include "kernels.cuh"
+
+struct WarpQueue {
+  double val[32][20];  // [slot][corner * 5 + field]
+  int cell[32];        // base cell iz*Nb+iR of the slot
+  int type[32];
+  int list[32];        // compacted occupied slots of one drain
+};
+
+// all 32 lanes call this with the same `full` mask (slots to drain)
+__device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *fx, const int *shift, int G, int Nb)
+{
+  const int lane = threadIdx.x & 31;
+  if(full & (1u << lane)) q.list[__popc(full & ((1u << lane) - 1))] = lane;
+  __syncwarp();
+  const int items = __popc(full) * 20;
+  for(int it = lane; it < items; it += 32) {
+    const int s = q.list[it / 20];
+    const int k = it - (it / 20) * 20;
+    const int corner = k / 5, f = k - corner * 5;
+    const int off = (corner & 1) + ((corner >> 1) ? Nb : 0);
+    const int t = q.type[s];
+    fx_add(&fx[((size_t) t * NG_COMMITTED + f) * G + q.cell[s] + off], q.val[s][k], shift[t * NG_COMMITTED + f]);
+  }
+  __syncwarp();
+}
+
+#endif

@@ -14,6 +14,9 @@
 enum { F_M = 0, F_R = 1, F_T = 2, F_Q = 3, F_P = 4, NF_ORBIT = 5 };
 // committed per-type grids, in galic_grid_id order
 enum { NG_COMMITTED = 10 };
+// threads per CTA of the persistent orbit kernels
+#define CALC_ALL_BLOCK_FP64 128
+#define CALC_ALL_BLOCK_FP32 256
 // target stacks per type: DGs_MassTarget, EGs_MassTarget, EGs_EgyTarget_{r,t,p,q}
 enum { T_DGM = 0, T_EGM = 1, T_R = 2, T_T = 3, T_P = 4, T_Q = 5, NT_TARGET = 6 };
 
@@ -68,5 +71,8 @@ void launch_fx_finalize(const FxWord *fx, const int *shift, double *committed, i
 int launch_global_fit(const FitArgs &f, cudaStream_t s);
 cudaError_t prepare_fit_kernels();
 int calc_all_occupancy(int block);
+int calc_all_fp32_occupancy(int block);
+int launch_calc_all_fp32(const DevModel &M64, const float4 *const tab[4], const float *cellsize32,
+                         const CalcAllArgs &a, int grid, int block, cudaStream_t s);
 
 #endif

@@ -1,0 +1,388 @@
+// FP32-integrate / FP64-accumulate form of calc_all_response_fields
+// (main.c:151-231, orbit_response.c:155-491).
+//
+// Same algorithm as the FP64 form (orbit_fp64.cu) with these changes, all of
+// which only move results within the stated tolerance of the FP64 oracle:
+//  * positions, velocities, accelerations and the interpolation run in FP32;
+//    the force grid is read from one float4 table per particle type
+//    {DPotDR, DPotDz, Vstream[type], 0} (one 16-byte load per corner);
+//  * log(x)/log(Fac) becomes log2(x) * (1/log2 Fac) (MUFU.LG2), divisions
+//    become reciprocal multiplies, and accR (cos phi, sin phi) is evaluated as
+//    accR (x/R, y/R), which is the same vector without atan2/sin/cos;
+//  * the orbit time tall, the mass/timespan normalisation and every deposit
+//    into the response grids stay FP64 (merged per cell in FP32 registers,
+//    then rounded once into the exact fixed-point accumulators);
+//  * the relative energy drift check uses FP64 potentials.
+// Built with --fmad=true (this file keeps contraction on).
+#include <cuda_runtime.h>
+
+#include "flush.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+struct Model32 {
+  float V200, f_orb, f_cc;
+  float invFG, ilgFG;       // 1/FG_Rmin, 1/log2(FG_Fac)
+  float invDG, ilgDG;       // 1/DG_Rmin, 1/log2(DG_Fac)
+  float GMh, Ah, eps_h, haloscale;   // G*Halo_Mass, Halo_A, 1e-6 Halo_A, M200/Halo_Mass
+  float GMb, Ab, eps_b;
+  int tabulated, analytic_halo, analytic_bulge;
+  int tovs[4];
+  int FG_Nbin, DG_Nbin;
+  float fgmax;             // FG_Nbin - 1
+  float dgmax;             // DG_Nbin - 1
+  const float4 *tab[4];    // per type: {DPotDR, DPotDz, Vstream[type], 0}
+  const float *cellsize;
+};
+
+__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
+
+struct Cell32 {
+  int iR, iz;
+  float fR, fz;
+};
+
+__device__ __forceinline__ Cell32 cell32(float br, float bz, int nbin, float bmax)
+{
+  Cell32 c;
+  br = fmaxf(br, 0.f);
+  bz = fmaxf(bz, 0.f);
+  int binr = (br < bmax) ? (int) br : nbin - 1;
+  int binz = (bz < bmax) ? (int) bz : nbin - 1;
+  c.fR = br - (float) binr;
+  c.fz = bz - (float) binz;
+  if(binr >= nbin - 1) {
+    binr = nbin - 2;
+    c.fR = 1.f;
+  }
+  if(binz >= nbin - 1) {
+    binz = nbin - 2;
+    c.fz = 1.f;
+  }
+  c.iR = binr;
+  c.iz = binz;
+  return c;
+}
+
+// acceleration (grid.c:122-197) and streaming velocity (disp_fields.c:118-132)
+// at x; both read the same float4 table corners
+__device__ __forceinline__ void accel32(const Model32 &M, int type, const float *x, float *a, float *vstr)
+{
+  const float R2 = x[0] * x[0] + x[1] * x[1];
+  const float R = sqrtf(R2);
+  const float az_abs = fabsf(x[2]);
+  const float jd = __log2f(fmaf(R, M.invFG, 1.f)) * M.ilgFG;
+  const float id = __log2f(fmaf(az_abs, M.invFG, 1.f)) * M.ilgFG;
+  const int N = M.FG_Nbin;
+  Cell32 c = cell32(jd, id, N, M.fgmax);
+  const float4 *T = M.tab[type];
+  const float4 t00 = __ldg(&T[c.iz * N + c.iR]);
+  const float4 t01 = __ldg(&T[c.iz * N + c.iR + 1]);
+  const float4 t10 = __ldg(&T[(c.iz + 1) * N + c.iR]);
+  const float4 t11 = __ldg(&T[(c.iz + 1) * N + c.iR + 1]);
+  const float w00 = (1.f - c.fR) * (1.f - c.fz), w01 = c.fR * (1.f - c.fz);
+  const float w10 = (1.f - c.fR) * c.fz, w11 = c.fR * c.fz;
+  *vstr = t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11;
+  a[0] = a[1] = a[2] = 0.f;
+  if(M.tabulated) {
+    if(jd < M.fgmax && id < M.fgmax) {
+      float accR = t00.x * w00 + t01.x * w01 + t10.x * w10 + t11.x * w11;
+      float accz = t00.y * w00 + t01.y * w01 + t10.y * w10 + t11.y * w11;
+      if(x[2] < 0) accz = -accz;
+      const float inv = R > 0.f ? frcp(R) : 0.f;
+      a[0] = accR * x[0] * inv;
+      a[1] = accR * x[1] * inv;
+      a[2] = accz;
+    } else {
+      const float r = sqrtf(R2 + x[2] * x[2]);
+      const float rp = r + M.Ah;
+      const float fac = M.haloscale * M.GMh * frcp((r + M.eps_h) * rp * rp);
+      a[0] = -fac * x[0];
+      a[1] = -fac * x[1];
+      a[2] = -fac * x[2];
+    }
+  }
+  if(M.analytic_halo | M.analytic_bulge) {
+    const float r = sqrtf(R2 + x[2] * x[2]);
+    float fac = 0.f;
+    if(M.analytic_halo) {
+      const float rp = r + M.Ah;
+      fac += M.GMh * frcp((r + M.eps_h) * rp * rp);
+    }
+    if(M.analytic_bulge) {
+      const float rp = r + M.Ab;
+      fac += M.GMb * frcp((r + M.eps_b) * rp * rp);
+    }
+    a[0] -= fac * x[0];
+    a[1] -= fac * x[1];
+    a[2] -= fac * x[2];
+  }
+}
+
+struct Proj32 {
+  float vr2, vt2, vq2, vp2;
+};
+
+// orbit_response.c:222-273 in FP32; vstr is the streaming velocity at x
+__device__ __forceinline__ Proj32 project32(int tovs, const float *x, const float *v, float vstr)
+{
+  Proj32 o;
+  if(tovs == 2) {
+    const float r2 = x[0] * x[0] + x[1] * x[1];
+    const float vdx = v[0] * x[0] + v[1] * x[1];
+    const float ir2 = frcp(r2);
+    o.vr2 = vdx * vdx * ir2;
+    const float vq = (v[1] * x[0] - v[0] * x[1]) * rsqrtf(r2);
+    o.vq2 = vq * vq;
+    o.vp2 = (vq - vstr) * (vq - vstr);
+    o.vt2 = v[2] * v[2];
+  } else {
+    // Q = x cross (0,0,-1) = (-y, x, 0); T = x cross Q
+    const float r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+    const float vdx = v[0] * x[0] + v[1] * x[1] + v[2] * x[2];
+    o.vr2 = vdx * vdx * frcp(r2);
+    const float q2 = x[0] * x[0] + x[1] * x[1];
+    const float vq = (v[1] * x[0] - v[0] * x[1]) * rsqrtf(q2);
+    o.vq2 = vq * vq;
+    o.vp2 = (vq - vstr) * (vq - vstr);
+    const float T0 = x[0] * x[2], T1 = x[1] * x[2], T2 = -q2;
+    const float t2 = T0 * T0 + T1 * T1 + T2 * T2;
+    const float vdT = v[0] * T0 + v[1] * T1 + v[2] * T2;
+    o.vt2 = vdT * vdT * frcp(t2);
+  }
+  return o;
+}
+
+__device__ __forceinline__ Cell32 density_cell32(const Model32 &M, const float *x)
+{
+  const float r = sqrtf(x[0] * x[0] + x[1] * x[1]);
+  const float br = __log2f(fmaf(r, M.invDG, 1.f)) * M.ilgDG - 0.5f;
+  const float bz = __log2f(fmaf(fabsf(x[2]), M.invDG, 1.f)) * M.ilgDG - 0.5f;
+  return cell32(br, bz, M.DG_Nbin, M.dgmax);
+}
+
+// register-merged FP32 sums, parked as FP64 (x mass/Tint) in the warp queue
+struct Sink32 {
+  WarpQueue *q;
+  int lane, type, Nb;
+  double fac;
+  int cur;
+  bool parked;
+  float a[4][5];
+  __device__ __forceinline__ void park()
+  {
+    if(cur < 0) return;
+#pragma unroll
+    for(int c = 0; c < 4; c++)
+#pragma unroll
+      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = (double) a[c][f] * fac;
+    q->cell[lane] = cur;
+    q->type[lane] = type;
+    parked = true;
+    cur = -1;
+  }
+  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
+  {
+    const int c = iz * Nb + iR;
+    if(c != cur) {
+      park();
+#pragma unroll
+      for(int k = 0; k < 4; k++)
+#pragma unroll
+        for(int f = 0; f < 5; f++) a[k][f] = 0.f;
+      cur = c;
+    }
+    const float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
+#pragma unroll
+    for(int k = 0; k < 4; k++) {
+      a[k][0] += w[k];
+      a[k][1] = fmaf(w[k], p.vr2, a[k][1]);
+      a[k][2] = fmaf(w[k], p.vt2, a[k][2]);
+      a[k][3] = fmaf(w[k], p.vq2, a[k][3]);
+      a[k][4] = fmaf(w[k], p.vp2, a[k][4]);
+    }
+  }
+};
+
+struct State32 {
+  float x[3], v[3], a[3];
+  double tall, timespan, E0;
+  int iR, iz;
+  float fR, fz, radsign_prev;
+  Proj32 proj;
+  int norbit, flag, type, tovs, steps, status;
+};
+
+enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
+
+__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32) k_calc_all_fp32(DevModel M64, Model32 M, CalcAllArgs A,
+                                                                     long long step_cap)
+{
+  __shared__ WarpQueue queues[CALC_ALL_BLOCK_FP32 / 32];
+  LogConsts L64 = make_log_consts(M64);
+  const int G = M64.DG_Ngrid;
+  State32 s;
+  Sink32 sink;
+  sink.q = &queues[threadIdx.x >> 5];
+  sink.lane = threadIdx.x & 31;
+  sink.Nb = M.DG_Nbin;
+  sink.cur = -1;
+  sink.parked = false;
+  int p = -1;
+  unsigned long long my_steps = 0;
+  double my_err = 0;
+  int my_status = 0;
+
+  auto begin = [&]() -> bool {
+    int k = atomicAdd(A.next, 1);
+    if(k >= A.n) {
+      p = -1;
+      return false;
+    }
+    p = A.order ? A.order[k] : k;
+    const int type = A.type[p];
+    sink.type = type;
+    sink.fac = A.mass[p] / A.tint[p];
+    sink.cur = -1;
+    double xd[3], vd[3];
+    for(int i = 0; i < 3; i++) {
+      xd[i] = A.pos[3 * p + i];
+      vd[i] = A.vel[3 * p + i];
+      s.x[i] = (float) xd[i];
+      s.v[i] = (float) vd[i];
+    }
+    s.type = type;
+    s.tovs = M.tovs[type];
+    s.tall = 0;
+    s.timespan = A.tint[p];
+    s.radsign_prev = 0.f;
+    s.norbit = 0;
+    s.flag = 0;
+    s.steps = 0;
+    s.status = ORBIT_OK;
+    float vstr;
+    accel32(M, type, s.x, s.a, &vstr);
+    Cell32 c = density_cell32(M, s.x);
+    s.iR = c.iR;
+    s.iz = c.iz;
+    s.fR = c.fR;
+    s.fz = c.fz;
+    s.proj = project32(s.tovs, s.x, s.v, vstr);
+    s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, L64, xd);
+    return true;
+  };
+
+  int state = begin() ? LANE_ACTIVE : LANE_DONE;
+  for(;;) {
+    const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
+    if(full) {
+      warp_drain(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
+      sink.parked = false;
+    }
+    if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
+    if(state == LANE_ACTIVE) {
+      // get_timestep (orbit_response.c:16-26)
+      const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
+      const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
+      const float t1 = M.f_orb * M.V200 * frcp(aa);
+      const float t2 = M.f_cc * __ldg(&M.cellsize[s.iz * M.DG_Nbin + s.iR]) * frcp(vv);
+      double dt = (double) fminf(t1, t2);
+      if(s.timespan < dt + s.tall) {
+        dt = s.timespan - s.tall;
+        s.flag = 1;
+      }
+      const float hdt = 0.5f * (float) dt;
+      const float fdt = (float) dt;
+      sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+#pragma unroll
+      for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+#pragma unroll
+      for(int i = 0; i < 3; i++) s.x[i] = fmaf(fdt, s.v[i], s.x[i]);
+      float vstr;
+      accel32(M, s.type, s.x, s.a, &vstr);
+#pragma unroll
+      for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+      Cell32 c = density_cell32(M, s.x);
+      s.iR = c.iR;
+      s.iz = c.iz;
+      s.fR = c.fR;
+      s.fz = c.fz;
+      s.proj = project32(s.tovs, s.x, s.v, vstr);
+      sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+      s.tall += dt;
+      const float radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];
+      if(radsign > 0.f && s.radsign_prev < 0.f) s.norbit++;
+      s.radsign_prev = radsign;
+      s.steps++;
+      if(!(s.tall == s.tall)) {
+        s.status = ORBIT_NONFINITE;
+        state = LANE_FINISH;
+      } else if(s.steps > step_cap) {
+        s.status = ORBIT_STEP_CAP;
+        state = LANE_FINISH;
+      } else if(s.flag)
+        state = LANE_FINISH;
+    } else if(state == LANE_FINISH) {
+      sink.park();
+      A.orbits[p] = s.norbit;
+      my_steps += (unsigned long long) s.steps;
+      if(s.status != ORBIT_OK)
+        my_status = max(my_status, s.status);
+      else {
+        double xd[3] = {s.x[0], s.x[1], s.x[2]};
+        double vd0 = s.v[0], vd1 = s.v[1], vd2 = s.v[2];
+        double E1 = 0.5 * (vd0 * vd0 + vd1 * vd1 + vd2 * vd2) + forcegrid_pot(M64, L64, xd);
+        double e = fabs((E1 - s.E0) / s.E0);
+        if(e > my_err) my_err = e;
+      }
+      state = begin() ? LANE_ACTIVE : LANE_DONE;
+    }
+  }
+  if(my_steps) atomicAdd(A.steps_total, my_steps);
+  if(my_err >= 0) atomicMax((unsigned long long *) A.max_egy_err, (unsigned long long) __double_as_longlong(my_err));
+  if(my_status) atomicMax(A.status, my_status);
+}
+
+}  // namespace
+
+int calc_all_fp32_occupancy(int block)
+{
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_calc_all_fp32, block, 0);
+  return blocks;
+}
+
+int launch_calc_all_fp32(const DevModel &M64, const float4 *const tab[4], const float *cellsize32,
+                         const CalcAllArgs &a, int grid, int block, cudaStream_t s)
+{
+  Model32 M;
+  M.V200 = (float) M64.V200;
+  M.f_orb = (float) M64.f_orb;
+  M.f_cc = (float) M64.f_cc;
+  M.invFG = (float) (1.0 / M64.FG_Rmin);
+  M.ilgFG = (float) (1.0 / std::log2(M64.FG_Fac));
+  M.invDG = (float) (1.0 / M64.DG_Rmin);
+  M.ilgDG = (float) (1.0 / std::log2(M64.DG_Fac));
+  M.GMh = (float) (M64.G * M64.Halo_Mass);
+  M.Ah = (float) M64.Halo_A;
+  M.eps_h = (float) (1.0e-6 * M64.Halo_A);
+  M.haloscale = (float) (M64.M200 / M64.Halo_Mass);
+  M.GMb = (float) (M64.G * M64.Bulge_Mass);
+  M.Ab = (float) M64.Bulge_A;
+  M.eps_b = (float) (1.0e-6 * M64.Bulge_A);
+  M.tabulated = M64.tabulated;
+  M.analytic_halo = M64.analytic_halo;
+  M.analytic_bulge = M64.analytic_bulge;
+  for(int t = 0; t < 4; t++) {
+    M.tovs[t] = M64.tovs[t];
+    M.tab[t] = tab[t];
+  }
+  M.FG_Nbin = M64.FG_Nbin;
+  M.DG_Nbin = M64.DG_Nbin;
+  M.fgmax = (float) (M64.FG_Nbin - 1);
+  M.dgmax = (float) (M64.DG_Nbin - 1);
+  M.cellsize = cellsize32;
+  k_calc_all_fp32<<<grid, block, 0, s>>>(M64, M, a, M64.step_cap);
+  return 1;
+}

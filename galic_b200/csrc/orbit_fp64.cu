@@ -14,6 +14,7 @@
 //  k_fx_finalize    fixed-point words -> FP64 committed grids.
 #include <cuda_runtime.h>
 
+#include "flush.cuh"
 #include "kernels.cuh"
 
 namespace {
@@ -85,37 +86,38 @@ __global__ void k_scale_dense(OrbitBatch b, int G)
   }
 }
 
-// Register-merged fixed-point sink of the batched path.
-struct MergeSink {
-  FxWord *grid;  // [NG_COMMITTED][Ngrid] of this particle's type; fields 0..4 used
-  const int *shift;
-  int Ngrid, Nb;
-  double fac;    // mass / timespan
-  int cur;       // merged cell iz*Nb+iR, -1 if none
+// Register-merged sink of the batched path: deposits of consecutive steps in
+// the same cell are summed in registers; on a cell change the 20 sums are
+// scaled by mass/Tint and parked in the lane's slot of the warp queue, which
+// the whole warp drains into the fixed-point grids (flush.cuh).
+struct QueueSink {
+  WarpQueue *q;
+  int lane, type, Nb;
+  double fac;  // mass / timespan
+  int cur;     // merged cell iz*Nb+iR, -1 if none
+  bool parked;
   double a[4][5];
-  __device__ __forceinline__ void reset()
-  {
-#pragma unroll
-    for(int c = 0; c < 4; c++)
-#pragma unroll
-      for(int f = 0; f < 5; f++) a[c][f] = 0;
-  }
-  __device__ __forceinline__ void flush()
+  __device__ __forceinline__ void park()
   {
     if(cur < 0) return;
-    const int cells[4] = {cur, cur + 1, cur + Nb, cur + Nb + 1};
 #pragma unroll
     for(int c = 0; c < 4; c++)
 #pragma unroll
-      for(int f = 0; f < 5; f++) fx_add(&grid[(size_t) f * Ngrid + cells[c]], a[c][f] * fac, shift[f]);
+      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = a[c][f] * fac;
+    q->cell[lane] = cur;
+    q->type[lane] = type;
+    parked = true;
     cur = -1;
   }
   __device__ __forceinline__ void operator()(const Deposit &d)
   {
     int c = d.iz * Nb + d.iR;
     if(c != cur) {
-      flush();
-      reset();
+      park();
+#pragma unroll
+      for(int k = 0; k < 4; k++)
+#pragma unroll
+        for(int f = 0; f < 5; f++) a[k][f] = 0;
       cur = c;
     }
     const double w[4] = {d.m00, d.m10, d.m01, d.m11};
@@ -137,15 +139,20 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
   atomicMax((unsigned long long *) addr, (unsigned long long) __double_as_longlong(v));
 }
 
-__global__ void __launch_bounds__(128) k_calc_all_fp64(DevModel M, CalcAllArgs A)
+enum LaneState { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
+
+__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevModel M, CalcAllArgs A)
 {
+  __shared__ WarpQueue queues[CALC_ALL_BLOCK_FP64 / 32];
   LogConsts L = make_log_consts(M);
   const int G = M.DG_Ngrid;
   OrbitState s;
-  MergeSink sink;
-  sink.Ngrid = G;
+  QueueSink sink;
+  sink.q = &queues[threadIdx.x >> 5];
+  sink.lane = threadIdx.x & 31;
   sink.Nb = M.DG_Nbin;
   sink.cur = -1;
+  sink.parked = false;
   int p = -1;
   unsigned long long my_steps = 0;
   double my_err = 0;
@@ -160,29 +167,34 @@ __global__ void __launch_bounds__(128) k_calc_all_fp64(DevModel M, CalcAllArgs A
     }
     p = A.order ? A.order[k] : k;
     int type = A.type[p];
-    sink.grid = A.fx + (size_t) type * NG_COMMITTED * G;
-    sink.shift = A.shift + type * NG_COMMITTED;
+    sink.type = type;
     sink.fac = A.mass[p] / A.tint[p];
     sink.cur = -1;
     orbit_begin(M, L, s, &A.pos[3 * p], &A.vel[3 * p], A.tint[p], type, true);
     return true;
   };
 
-  bool active = fetch();
-  while(__any_sync(0xffffffffu, active)) {
-    if(active) {
-      bool more = orbit_step(M, L, s, true, sink);
-      if(!more) {
-        sink.flush();
-        A.orbits[p] = s.norbit;
-        my_steps += (unsigned long long) s.steps;
-        if(s.status != ORBIT_OK) my_status = max(my_status, s.status);
-        else {
-          double e = orbit_energy_error(M, L, s);
-          if(e > my_err) my_err = e;
-        }
-        active = fetch();
+  int state = fetch() ? LANE_ACTIVE : LANE_DONE;
+  for(;;) {
+    const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
+    if(full) {
+      warp_drain(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
+      sink.parked = false;
+    }
+    if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
+    if(state == LANE_ACTIVE) {
+      if(!orbit_step(M, L, s, true, sink)) state = LANE_FINISH;
+    } else if(state == LANE_FINISH) {
+      sink.park();
+      A.orbits[p] = s.norbit;
+      my_steps += (unsigned long long) s.steps;
+      if(s.status != ORBIT_OK)
+        my_status = max(my_status, s.status);
+      else {
+        double e = orbit_energy_error(M, L, s);
+        if(e > my_err) my_err = e;
       }
+      state = fetch() ? LANE_ACTIVE : LANE_DONE;
     }
   }
   if(my_steps) atomicAdd(A.steps_total, my_steps);

@@ -146,3 +146,33 @@ def test_invalid_repetition_lists_rejected():
                 ctx.optimize_rep(bad, 1, 0)
             assert e.value.status == 1
         ctx.optimize_rep([], 1, 0)
+
+
+def test_fp32_form_close_to_fp64():
+    """FP32-integrate / FP64-accumulate form against the FP64 form on the same
+    model: aggregate response grids (relative to each grid's peak) and the
+    merit values."""
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64
+
+    m = synth.config_halo_disk(n_halo=20000, n_disk=5000, level=6, seed=6)
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.calc_all_response_fields(GALIC_FORM_FP64)
+        r64 = np.stack([ctx.response(t, w) for t in (1, 2) for w in range(5)])
+        f64 = ctx.fit()
+        s64 = ctx.last_orbit_steps()
+        ctx.calc_all_response_fields(GALIC_FORM_FP32)
+        r32 = np.stack([ctx.response(t, w) for t in (1, 2) for w in range(5)])
+        f32 = ctx.fit()
+        s32 = ctx.last_orbit_steps()
+        ctx.calc_all_response_fields(GALIC_FORM_FP32)
+        assert np.array_equal(r32, np.stack([ctx.response(t, w) for t in (1, 2) for w in range(5)]))
+    err = peak_rel(r32, r64)
+    a, b = f32[1:3, :5], f64[1:3, :5]
+    nz = b != 0  # Sdisp_q is zero for velocity structures 0 and 1 (main.c:344-348)
+    assert np.all(a[~nz] == 0)
+    ferr = np.max(np.abs(a[nz] - b[nz]) / np.abs(b[nz]))
+    print(f"fp32 vs fp64: bins {err:.3e} of peak, fit {ferr:.3e}, steps {s32} vs {s64}")
+    assert abs(s32 - s64) <= 1e-3 * s64
+    assert err < 1e-3
+    assert ferr < 1e-3
