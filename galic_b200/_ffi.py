@@ -106,6 +106,8 @@ SIGNATURES = [
     ("galic_last_timing", C.c_int, [VP, PD, PD]),
     ("galic_last_max_energy_error", C.c_double, [VP]),
     ("galic_last_kernel_launches", C.c_int, [VP]),
+    ("galic_orbit_responses_noalloc", C.c_int,
+     [C.POINTER(GalicParams), VP, VP, VP, VP, C.c_double, C.c_int, VP, VP, VP, VP, VP, VP, VP, VP]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
     ("galic_density_geometry", C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
     ("galic_smooth_stack", None, [PD, C.c_int]),
