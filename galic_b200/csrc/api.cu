@@ -45,6 +45,7 @@ struct galic_ctx {
   double *d_pos = nullptr, *d_vel = nullptr, *d_mass = nullptr, *d_tint = nullptr, *d_vesc = nullptr;
   double *d_ptargets = nullptr, *d_vdisp = nullptr;
   int *d_type = nullptr, *d_orbits = nullptr;
+  int *d_order = nullptr;  // orbit processing order of the batched kernels (by initial radius)
   // scratch of the per-orbit drop-ins and the repetition
   int scratch_orbits = 0;
   double *d_b_pos = nullptr, *d_b_vel = nullptr, *d_b_mass = nullptr, *d_b_time = nullptr, *d_grids = nullptr;
@@ -60,7 +61,9 @@ struct galic_ctx {
   int last_launches = 0;
   double last_max_egy_err = 0;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  // FP32 form: one float4 table {DPotDR, DPotDz, Vstream[type], 0} per type
+  // FP32 form: per type a quad table, 4 float4 per force-grid cell (iz, iR):
+  // DPotDR, DPotDz and Vstream[type] of the corners (iz,iR), (iz,iR+1),
+  // (iz+1,iR), (iz+1,iR+1), then padding
   std::vector<double> h_dpotdr, h_dpotdz, h_vstream[4];
   float4 *d_tab32[4] = {nullptr, nullptr, nullptr, nullptr};
   float *d_cellsize32 = nullptr;
@@ -203,7 +206,9 @@ int fixed_point_shift(double bound)
   return 84 - e;
 }
 
-void set_shifts(galic_ctx *ctx, int *shift)
+// form: two-word exact words (FP64 form) or one signed word (FP32 form,
+// flush.cuh:warp_drain32); both keep every bin total inside the word's range
+void set_shifts(galic_ctx *ctx, int *shift, int form)
 {
   const galic_params_t &p = ctx->prm;
   // |potential| bound: tabulated part plus the analytic halo and bulge
@@ -214,7 +219,7 @@ void set_shifts(galic_ctx *ctx, int *shift)
     double be = bm * 2.0 * phi * 16.0;  // v^2 <= 2|phi| with a factor 16 headroom
     for(int g = 0; g < NG_COMMITTED; g++) {
       bool mass = (g == GALIC_GRID_MASS_S || g == GALIC_GRID_MASS_I);
-      shift[t * NG_COMMITTED + g] = fixed_point_shift(mass ? 2.0 * bm : be);
+      shift[t * NG_COMMITTED + g] = fixed_point_shift(mass ? 2.0 * bm : be) + (form == GALIC_FORM_FP32 ? 2 : 0);
     }
   }
 }
@@ -228,14 +233,26 @@ int ensure_tab32(galic_ctx *ctx)
     ctx->h_dpotdr.assign(NF, 0.0);
     ctx->h_dpotdz.assign(NF, 0.0);
   }
-  std::vector<float4> tab(NF);
+  const int N = ctx->prm.FG_Nbin;
+  std::vector<float4> tab(4 * (size_t) NF, make_float4(0.f, 0.f, 0.f, 0.f));
   for(int t = 1; t <= 3; t++) {
-    if(!ctx->d_tab32[t]) CK(dalloc(&ctx->d_tab32[t], NF));
-    for(int i = 0; i < NF; i++) {
-      double vs = ctx->h_vstream[t].size() == (size_t) NF ? ctx->h_vstream[t][i] : 0.0;
-      tab[i] = make_float4((float) ctx->h_dpotdr[i], (float) ctx->h_dpotdz[i], (float) vs, 0.f);
-    }
-    CK(cudaMemcpy(ctx->d_tab32[t], tab.data(), NF * sizeof(float4), cudaMemcpyHostToDevice));
+    if(!ctx->d_tab32[t]) CK(dalloc(&ctx->d_tab32[t], 4 * (size_t) NF));
+    const bool hv = ctx->h_vstream[t].size() == (size_t) NF;
+    for(int iz = 0; iz + 1 < N; iz++)
+      for(int iR = 0; iR + 1 < N; iR++) {
+        const int c[4] = {iz * N + iR, iz * N + iR + 1, (iz + 1) * N + iR, (iz + 1) * N + iR + 1};
+        float r[4], z[4], v[4];
+        for(int k = 0; k < 4; k++) {
+          r[k] = (float) ctx->h_dpotdr[c[k]];
+          z[k] = (float) ctx->h_dpotdz[c[k]];
+          v[k] = hv ? (float) ctx->h_vstream[t][c[k]] : 0.f;
+        }
+        float4 *e = &tab[4 * (size_t) (iz * N + iR)];
+        e[0] = make_float4(r[0], r[1], r[2], r[3]);
+        e[1] = make_float4(z[0], z[1], z[2], z[3]);
+        e[2] = make_float4(v[0], v[1], v[2], v[3]);
+      }
+    CK(cudaMemcpy(ctx->d_tab32[t], tab.data(), 4 * (size_t) NF * sizeof(float4), cudaMemcpyHostToDevice));
   }
   if(!ctx->d_cellsize32) CK(dalloc(&ctx->d_cellsize32, ctx->G));
   std::vector<float> cs(ctx->G);
@@ -358,7 +375,7 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx->d_fx); dfree(ctx->d_shift); dfree(ctx->d_fit); dfree(ctx->d_firstrun); dfree(ctx->d_counters);
   dfree(ctx->d_status); dfree(ctx->d_next); dfree(ctx->d_maxerr);
   dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
-  dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits);
+  dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits); dfree(ctx->d_order);
   dfree(ctx->d_b_pos); dfree(ctx->d_b_vel); dfree(ctx->d_b_mass); dfree(ctx->d_b_time); dfree(ctx->d_grids);
   dfree(ctx->d_b_tall); dfree(ctx->d_b_err); dfree(ctx->d_b_type); dfree(ctx->d_b_norbit); dfree(ctx->d_b_status);
   dfree(ctx->d_b_steps);
@@ -442,7 +459,8 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
     if(type[i] < 1 || type[i] > 3 || !(tint[i] > 0)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   if(n != ctx->n) {
     dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
-    dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits);
+    dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits); dfree(ctx->d_order);
+    CK(dalloc(&ctx->d_order, n));
     CK(dalloc(&ctx->d_pos, 3 * (size_t) n));
     CK(dalloc(&ctx->d_vel, 3 * (size_t) n));
     CK(dalloc(&ctx->d_mass, n));
@@ -462,6 +480,18 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
   CK(cudaMemcpy(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemset(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double)));
+  {
+    // neighbouring lanes then integrate orbits that start at similar radii and
+    // read nearby force-grid cells; results do not depend on the order
+    std::vector<double> r2(n);
+    std::vector<int> order(n);
+    for(int i = 0; i < n; i++) {
+      r2[i] = pos[3 * i] * pos[3 * i] + pos[3 * i + 1] * pos[3 * i + 1] + pos[3 * i + 2] * pos[3 * i + 2];
+      order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return r2[a] < r2[b]; });
+    CK(cudaMemcpy(ctx->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  }
   CK(cudaMemset(ctx->d_orbits, 0, n * sizeof(int)));
   ctx->have_response = false;
   return fail(ctx, GALIC_OK);
@@ -581,7 +611,7 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   cudaStream_t s = ctx->stream;
   const int G = ctx->G;
   int shift[4 * NG_COMMITTED];
-  set_shifts(ctx, shift);
+  set_shifts(ctx, shift, form);
   CK(cudaMemcpyAsync(ctx->d_shift, shift, sizeof(shift), cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev[0], s));
   CK(cudaMemsetAsync(ctx->d_fx, 0, (size_t) 4 * NG_COMMITTED * G * sizeof(FxWord), s));
@@ -596,7 +626,7 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   a.mass = ctx->d_mass;
   a.tint = ctx->d_tint;
   a.type = ctx->d_type;
-  a.order = nullptr;
+  a.order = ctx->d_order;
   a.next = ctx->d_next;
   a.fx = ctx->d_fx;
   a.shift = ctx->d_shift;

@@ -39,4 +39,41 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
   __syncwarp();
 }
 
+// FP32 variant: the lane parks its FP32 sums and the orbit's FP64 scale; the
+// drain forms the FP64 product and adds it as ONE signed 64-bit fixed-point
+// word, X = round(v * 2^(shift-24)), to the high word of the bin (the low
+// word stays zero, so fx_value reads it unchanged).  shift - 24 is chosen so
+// that no bin can overflow 2^62; the resolution (~2^-62 of the bound) is far
+// inside the FP32 form's tolerance, and one atomic per value instead of two
+// halves the L2 atomic traffic.
+struct WarpQueue32 {
+  float val[32][20];
+  double fac[32];
+  int cell[32];
+  int type[32];
+  int list[32];
+};
+
+__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, unsigned full, FxWord *fx, const int *shift, int G,
+                                             int Nb)
+{
+  const int lane = threadIdx.x & 31;
+  if(full & (1u << lane)) q.list[__popc(full & ((1u << lane) - 1))] = lane;
+  __syncwarp();
+  const int items = __popc(full) * 20;
+  for(int it = lane; it < items; it += 32) {
+    const int s = q.list[it / 20];
+    const int k = it - (it / 20) * 20;
+    const int corner = k / 5, f = k - corner * 5;
+    const int off = (corner & 1) + ((corner >> 1) ? Nb : 0);
+    const int t = q.type[s];
+    const float vf = q.val[s][k];
+    if(vf == 0.f) continue;
+    const double v = (double) vf * q.fac[s];
+    const long long X = __double2ll_rn(ldexp(v, shift[t * NG_COMMITTED + f] - 24));
+    if(X) atomicAdd(&fx[((size_t) t * NG_COMMITTED + f) * G + q.cell[s] + off].hi, (unsigned long long) X);
+  }
+  __syncwarp();
+}
+
 #endif

@@ -17,6 +17,7 @@
  * Methods (all published; coefficients are exact Taylor coefficients, rounded
  * once to double, and the constants were computed to 60 digits with Python's
  * decimal module):
+ * Polynomials are evaluated by Horner's rule with fused multiply-adds.
  *  - log:   Cody & Waite style reduction x = 2^k * m, m in [sqrt(1/2), sqrt(2)),
  *           log(m) = 2 atanh(s), s = (m-1)/(m+1), atanh by its Taylor series;
  *           the algebraic rewrite log(1+f) = f - (f^2/2 - s (f^2/2 + R)) keeps
@@ -30,8 +31,8 @@
  *           significant bits), Taylor polynomials on |r| <= pi/4.  Accurate
  *           for |x| < 2^20; the orbit path only uses |x| <= pi.
  *  - acos:  acos(x) = atan2(sqrt((1-x)(1+x)), x).
- * Measured against glibc over random arguments the error is within 1 ulp
- * (tests/test_gmath.py).
+ * Measured against glibc over random arguments the error is within 1 ulp for
+ * log, sin and cos and within 2 ulp for atan2 and acos (tests/test_gmath.py).
  */
 #ifndef GALIC_GMATH_H
 #define GALIC_GMATH_H
@@ -65,6 +66,15 @@ GM_HD double gm_round(double x)
   return gm_copysign(t, x);
 }
 
+/* fused multiply-add, correctly rounded on both sides (DFMA on the GPU,
+ * the C library's fma on the host): Horner steps use it explicitly, so the
+ * result does not depend on the compilers' contraction settings */
+#ifdef __CUDA_ARCH__
+#define gm_fma(a, b, c) __fma_rn((a), (b), (c))
+#else
+#define gm_fma(a, b, c) __builtin_fma((a), (b), (c))
+#endif
+
 #define GM_INF gm_from_bits(0x7ff0000000000000ULL)
 #define GM_NAN gm_from_bits(0x7ff8000000000000ULL)
 
@@ -96,15 +106,15 @@ GM_HD double gm_log(double x)
   double z = s * s;
   /* R(z) = sum_{j>=1} 2 z^j / (2j+1) */
   double p = 0x1.8618618618618p-4;
-  p = 0x1.af286bca1af28p-4 + z * p;
-  p = 0x1.e1e1e1e1e1e1ep-4 + z * p;
-  p = 0x1.1111111111111p-3 + z * p;
-  p = 0x1.3b13b13b13b14p-3 + z * p;
-  p = 0x1.745d1745d1746p-3 + z * p;
-  p = 0x1.c71c71c71c71cp-3 + z * p;
-  p = 0x1.2492492492492p-2 + z * p;
-  p = 0x1.999999999999ap-2 + z * p;
-  p = 0x1.5555555555555p-1 + z * p;
+  p = gm_fma(z, p, 0x1.af286bca1af28p-4);
+  p = gm_fma(z, p, 0x1.e1e1e1e1e1e1ep-4);
+  p = gm_fma(z, p, 0x1.1111111111111p-3);
+  p = gm_fma(z, p, 0x1.3b13b13b13b14p-3);
+  p = gm_fma(z, p, 0x1.745d1745d1746p-3);
+  p = gm_fma(z, p, 0x1.c71c71c71c71cp-3);
+  p = gm_fma(z, p, 0x1.2492492492492p-2);
+  p = gm_fma(z, p, 0x1.999999999999ap-2);
+  p = gm_fma(z, p, 0x1.5555555555555p-1);
   double R = z * p;
   double hfsq = 0.5 * f * f;
   double dk = (double) k;
@@ -142,12 +152,12 @@ GM_HD double gm_atan_unit(double t)
   double u = (t - c) / (1.0 + t * c);
   double z = u * u;
   double p = -0x1.1111111111111p-4;
-  p = 0x1.3b13b13b13b14p-4 + z * p;
-  p = -0x1.745d1745d1746p-4 + z * p;
-  p = 0x1.c71c71c71c71cp-4 + z * p;
-  p = -0x1.2492492492492p-3 + z * p;
-  p = 0x1.999999999999ap-3 + z * p;
-  p = -0x1.5555555555555p-2 + z * p;
+  p = gm_fma(z, p, 0x1.3b13b13b13b14p-4);
+  p = gm_fma(z, p, -0x1.745d1745d1746p-4);
+  p = gm_fma(z, p, 0x1.c71c71c71c71cp-4);
+  p = gm_fma(z, p, -0x1.2492492492492p-3);
+  p = gm_fma(z, p, 0x1.999999999999ap-3);
+  p = gm_fma(z, p, -0x1.5555555555555p-2);
   double atu = u + u * (z * p);
   return ah[k] + (al[k] + atu);
 }
@@ -188,13 +198,13 @@ GM_HD double gm_sin_poly(double r)
 {
   double z = r * r;
   double p = 0x1.952c77030ad4ap-49;
-  p = -0x1.ae7f3e733b81fp-41 + z * p;
-  p = 0x1.6124613a86d09p-33 + z * p;
-  p = -0x1.ae64567f544e4p-26 + z * p;
-  p = 0x1.71de3a556c734p-19 + z * p;
-  p = -0x1.a01a01a01a01ap-13 + z * p;
-  p = 0x1.1111111111111p-7 + z * p;
-  p = -0x1.5555555555555p-3 + z * p;
+  p = gm_fma(z, p, -0x1.ae7f3e733b81fp-41);
+  p = gm_fma(z, p, 0x1.6124613a86d09p-33);
+  p = gm_fma(z, p, -0x1.ae64567f544e4p-26);
+  p = gm_fma(z, p, 0x1.71de3a556c734p-19);
+  p = gm_fma(z, p, -0x1.a01a01a01a01ap-13);
+  p = gm_fma(z, p, 0x1.1111111111111p-7);
+  p = gm_fma(z, p, -0x1.5555555555555p-3);
   return r + r * (z * p);
 }
 
@@ -202,13 +212,13 @@ GM_HD double gm_cos_poly(double r)
 {
   double z = r * r;
   double p = -0x1.6827863b97d97p-53;
-  p = 0x1.ae7f3e733b81fp-45 + z * p;
-  p = -0x1.93974a8c07c9dp-37 + z * p;
-  p = 0x1.1eed8eff8d898p-29 + z * p;
-  p = -0x1.27e4fb7789f5cp-22 + z * p;
-  p = 0x1.a01a01a01a01ap-16 + z * p;
-  p = -0x1.6c16c16c16c17p-10 + z * p;
-  p = 0x1.5555555555555p-5 + z * p;
+  p = gm_fma(z, p, 0x1.ae7f3e733b81fp-45);
+  p = gm_fma(z, p, -0x1.93974a8c07c9dp-37);
+  p = gm_fma(z, p, 0x1.1eed8eff8d898p-29);
+  p = gm_fma(z, p, -0x1.27e4fb7789f5cp-22);
+  p = gm_fma(z, p, 0x1.a01a01a01a01ap-16);
+  p = gm_fma(z, p, -0x1.6c16c16c16c17p-10);
+  p = gm_fma(z, p, 0x1.5555555555555p-5);
   double hz = 0.5 * z;
   double w = 1.0 - hz;
   return w + (((1.0 - w) - hz) + z * (z * p));

@@ -17,6 +17,12 @@ enum { NG_COMMITTED = 10 };
 // threads per CTA of the persistent orbit kernels
 #define CALC_ALL_BLOCK_FP64 128
 #define CALC_ALL_BLOCK_FP32 256
+#ifndef GALIC_FP64_MIN_BLOCKS
+#define GALIC_FP64_MIN_BLOCKS 3
+#endif
+#ifndef GALIC_FP32_MIN_BLOCKS
+#define GALIC_FP32_MIN_BLOCKS 2
+#endif
 // target stacks per type: DGs_MassTarget, EGs_MassTarget, EGs_EgyTarget_{r,t,p,q}
 enum { T_DGM = 0, T_EGM = 1, T_R = 2, T_T = 3, T_P = 4, T_Q = 5, NT_TARGET = 6 };
 
@@ -72,7 +78,7 @@ int launch_global_fit(const FitArgs &f, cudaStream_t s);
 cudaError_t prepare_fit_kernels();
 int calc_all_occupancy(int block);
 int calc_all_fp32_occupancy(int block);
-int launch_calc_all_fp32(const DevModel &M64, const float4 *const tab[4], const float *cellsize32,
+int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
                          const CalcAllArgs &a, int grid, int block, cudaStream_t s);
 
 #endif

@@ -4,8 +4,9 @@
 // Same algorithm as the FP64 form (orbit_fp64.cu) with these changes, all of
 // which only move results within the stated tolerance of the FP64 oracle:
 //  * positions, velocities, accelerations and the interpolation run in FP32;
-//    the force grid is read from one float4 table per particle type
-//    {DPotDR, DPotDz, Vstream[type], 0} (one 16-byte load per corner);
+//    the force grid is read from one "quad" table per particle type: for
+//    every cell the four corners' DPotDR, DPotDz and Vstream[type] (three
+//    float4, one 64-byte line), so a bilinear lookup is one cache line;
 //  * log(x)/log(Fac) becomes log2(x) * (1/log2 Fac) (MUFU.LG2), divisions
 //    become reciprocal multiplies, and accR (cos phi, sin phi) is evaluated as
 //    accR (x/R, y/R), which is the same vector without atan2/sin/cos;
@@ -32,7 +33,7 @@ struct Model32 {
   int FG_Nbin, DG_Nbin;
   float fgmax;             // FG_Nbin - 1
   float dgmax;             // DG_Nbin - 1
-  const float4 *tab[4];    // per type: {DPotDR, DPotDz, Vstream[type], 0}
+  const float4 *quad[4];   // per type, per cell iz*N+iR: {DPotDR x4}, {DPotDz x4}, {Vstream x4}, pad
   const float *cellsize;
 };
 
@@ -76,19 +77,17 @@ __device__ __forceinline__ void accel32(const Model32 &M, int type, const float 
   const float id = __log2f(fmaf(az_abs, M.invFG, 1.f)) * M.ilgFG;
   const int N = M.FG_Nbin;
   Cell32 c = cell32(jd, id, N, M.fgmax);
-  const float4 *T = M.tab[type];
-  const float4 t00 = __ldg(&T[c.iz * N + c.iR]);
-  const float4 t01 = __ldg(&T[c.iz * N + c.iR + 1]);
-  const float4 t10 = __ldg(&T[(c.iz + 1) * N + c.iR]);
-  const float4 t11 = __ldg(&T[(c.iz + 1) * N + c.iR + 1]);
+  // corners in the quad: (iz,iR), (iz,iR+1), (iz+1,iR), (iz+1,iR+1)
+  const float4 *Q = M.quad[type] + 4 * (c.iz * N + c.iR);
+  const float4 qR = __ldg(&Q[0]), qZ = __ldg(&Q[1]), qV = __ldg(&Q[2]);
   const float w00 = (1.f - c.fR) * (1.f - c.fz), w01 = c.fR * (1.f - c.fz);
   const float w10 = (1.f - c.fR) * c.fz, w11 = c.fR * c.fz;
-  *vstr = t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11;
+  *vstr = qV.x * w00 + qV.z * w10 + qV.y * w01 + qV.w * w11;
   a[0] = a[1] = a[2] = 0.f;
   if(M.tabulated) {
     if(jd < M.fgmax && id < M.fgmax) {
-      float accR = t00.x * w00 + t01.x * w01 + t10.x * w10 + t11.x * w11;
-      float accz = t00.y * w00 + t01.y * w01 + t10.y * w10 + t11.y * w11;
+      float accR = qR.x * w00 + qR.y * w01 + qR.z * w10 + qR.w * w11;
+      float accz = qZ.x * w00 + qZ.y * w01 + qZ.z * w10 + qZ.w * w11;
       if(x[2] < 0) accz = -accz;
       const float inv = R > 0.f ? frcp(R) : 0.f;
       a[0] = accR * x[0] * inv;
@@ -162,37 +161,74 @@ __device__ __forceinline__ Cell32 density_cell32(const Model32 &M, const float *
   return cell32(br, bz, M.DG_Nbin, M.dgmax);
 }
 
-// register-merged FP32 sums, parked as FP64 (x mass/Tint) in the warp queue
+// Register-merged FP32 sums per corner of the current DG cell.  When the
+// orbit moves to a neighbouring cell, the corners the two cells share keep
+// their sums (moved to their slot in the new cell) and only the corners left
+// behind are parked in the warp queue (the drain skips the zero entries);
+// any other move parks all four.
 struct Sink32 {
-  WarpQueue *q;
+  WarpQueue32 *q;
   int lane, type, Nb;
   double fac;
-  int cur;
+  int cur, cur_iR, cur_iz;
   bool parked;
   float a[4][5];
-  __device__ __forceinline__ void park()
+  __device__ __forceinline__ void park_masked(const bool keep[4])
   {
-    if(cur < 0) return;
 #pragma unroll
     for(int c = 0; c < 4; c++)
 #pragma unroll
-      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = (double) a[c][f] * fac;
+      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = keep[c] ? 0.f : a[c][f];
+    q->fac[lane] = fac;
     q->cell[lane] = cur;
     q->type[lane] = type;
     parked = true;
+  }
+  __device__ __forceinline__ void park()
+  {
+    if(cur < 0) return;
+    const bool none[4] = {false, false, false, false};
+    park_masked(none);
     cur = -1;
   }
-  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
+  __device__ __forceinline__ void move_to(int iR, int iz)
   {
-    const int c = iz * Nb + iR;
-    if(c != cur) {
+    const int dz = iz - cur_iz, dR = iR - cur_iR;
+    if(cur >= 0 && dz >= -1 && dz <= 1 && dR >= -1 && dR <= 1) {
+      bool keep[4] = {false, false, false, false};
+      float na[4][5];
+#pragma unroll
+      for(int j = 0; j < 4; j++) {
+#pragma unroll
+        for(int f = 0; f < 5; f++) na[j][f] = 0.f;
+#pragma unroll
+        for(int k = 0; k < 4; k++) {
+          // new corner j = (iz + (j>>1), iR + (j&1)) is old corner k = (cur_iz + (k>>1), cur_iR + (k&1))
+          const bool same = ((k >> 1) == (j >> 1) + dz) && ((k & 1) == (j & 1) + dR);
+          keep[k] = keep[k] || same;
+#pragma unroll
+          for(int f = 0; f < 5; f++) na[j][f] = same ? a[k][f] : na[j][f];
+        }
+      }
+      park_masked(keep);
+#pragma unroll
+      for(int j = 0; j < 4; j++)
+#pragma unroll
+        for(int f = 0; f < 5; f++) a[j][f] = na[j][f];
+    } else {
       park();
 #pragma unroll
       for(int k = 0; k < 4; k++)
 #pragma unroll
         for(int f = 0; f < 5; f++) a[k][f] = 0.f;
-      cur = c;
     }
+    cur = iz * Nb + iR;
+    cur_iR = iR;
+    cur_iz = iz;
+  }
+  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
+  {
+    if(iz * Nb + iR != cur) move_to(iR, iz);
     const float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
 #pragma unroll
     for(int k = 0; k < 4; k++) {
@@ -210,16 +246,18 @@ struct State32 {
   double tall, timespan, E0;
   int iR, iz;
   float fR, fz, radsign_prev;
+  int cs_cell;   // DG cell whose size is cached in cs_val
+  float cs_val;
   Proj32 proj;
   int norbit, flag, type, tovs, steps, status;
 };
 
 enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
 
-__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32) k_calc_all_fp32(DevModel M64, Model32 M, CalcAllArgs A,
+__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS) k_calc_all_fp32(DevModel M64, Model32 M, CalcAllArgs A,
                                                                      long long step_cap)
 {
-  __shared__ WarpQueue queues[CALC_ALL_BLOCK_FP32 / 32];
+  __shared__ WarpQueue32 queues[CALC_ALL_BLOCK_FP32 / 32];
   LogConsts L64 = make_log_consts(M64);
   const int G = M64.DG_Ngrid;
   State32 s;
@@ -269,6 +307,7 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32) k_calc_all_fp32(DevModel 
     s.fR = c.fR;
     s.fz = c.fz;
     s.proj = project32(s.tovs, s.x, s.v, vstr);
+    s.cs_cell = -1;
     s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, L64, xd);
     return true;
   };
@@ -277,7 +316,7 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32) k_calc_all_fp32(DevModel 
   for(;;) {
     const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
     if(full) {
-      warp_drain(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
+      warp_drain32(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
       sink.parked = false;
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
@@ -286,7 +325,12 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32) k_calc_all_fp32(DevModel 
       const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
       const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
       const float t1 = M.f_orb * M.V200 * frcp(aa);
-      const float t2 = M.f_cc * __ldg(&M.cellsize[s.iz * M.DG_Nbin + s.iR]) * frcp(vv);
+      const int dgc = s.iz * M.DG_Nbin + s.iR;
+      if(dgc != s.cs_cell) {
+        s.cs_cell = dgc;
+        s.cs_val = __ldg(&M.cellsize[dgc]);
+      }
+      const float t2 = M.f_cc * s.cs_val * frcp(vv);
       double dt = (double) fminf(t1, t2);
       if(s.timespan < dt + s.tall) {
         dt = s.timespan - s.tall;
@@ -353,7 +397,7 @@ int calc_all_fp32_occupancy(int block)
   return blocks;
 }
 
-int launch_calc_all_fp32(const DevModel &M64, const float4 *const tab[4], const float *cellsize32,
+int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
                          const CalcAllArgs &a, int grid, int block, cudaStream_t s)
 {
   Model32 M;
@@ -376,7 +420,7 @@ int launch_calc_all_fp32(const DevModel &M64, const float4 *const tab[4], const 
   M.analytic_bulge = M64.analytic_bulge;
   for(int t = 0; t < 4; t++) {
     M.tovs[t] = M64.tovs[t];
-    M.tab[t] = tab[t];
+    M.quad[t] = quad[t];
   }
   M.FG_Nbin = M64.FG_Nbin;
   M.DG_Nbin = M64.DG_Nbin;
