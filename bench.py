@@ -40,7 +40,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"],
+                    help="form of the headline value; the other form is measured beside it")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's particle count")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
@@ -172,6 +173,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def measured_fp32_peak(torch):
+    """FP32 (SIMT, no TF32) GEMM TFLOP/s, burst best of 5: the FP32 denominator."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return best
+
+
 def measured_fp64_peak(torch):
     """FP64 GEMM TFLOP/s (burst, best of 5) on this GPU: the FP64 denominator."""
     n = 4096
@@ -242,6 +265,7 @@ def ours_arm(args, rank, world, local_rank):
     ctx.load_model(model)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
 
+    other = GALIC_FORM_FP32 if form == GALIC_FORM_FP64 else GALIC_FORM_FP64
     for _ in range(args.warmup):
         ctx.calc_all_response_fields(form)
     torch.cuda.synchronize()
@@ -264,6 +288,18 @@ def ours_arm(args, rank, world, local_rank):
         wall = time.perf_counter() - t0
     if dist:
         dist.barrier()
+    # the other form on the same model (one warm-up, then K steps), for the
+    # FP32-vs-FP64 comparison the metric names
+    ctx.calc_all_response_fields(other)
+    other_ms, other_kern, other_steps = [], [], []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        ctx.calc_all_response_fields(other)
+        tot, kern = ctx.last_timing()
+        other_ms.append(tot)
+        other_kern.append(kern)
+        other_steps.append(ctx.last_orbit_steps())
     total_ms = sum(dev_ms)
     total_steps = sum(steps)
     # whole job: steps of all ranks over the slowest rank's device time
@@ -293,8 +329,9 @@ def ours_arm(args, rank, world, local_rank):
         e2e_s.append(time.perf_counter() - t1)
     e2e_value = steps[-1] * (world if dist else 1) / statistics.mean(e2e_s)
 
+    other_value = sum(other_steps) / (sum(other_ms) * 1e-3)
     if rank == 0:
-        peak = measured_fp64_peak(torch)
+        peak = measured_fp64_peak(torch) if form == GALIC_FORM_FP64 else measured_fp32_peak(torch)
         kern_avg = sum(kern_ms) / len(kern_ms)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
@@ -310,12 +347,18 @@ def ours_arm(args, rank, world, local_rank):
                 "config": {"workload": WORKLOAD, "form": args.form, "particles_per_gpu": model.n,
                            "orbit_steps_per_step": steps[-1], "l2": "flushed (256 MiB write) between steps",
                            "parallelism": f"{world} independent models (one per GPU)"},
-                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak, "traffic": None,
-                             "peak_source": "measured FP64 GEMM (torch.matmul float64 4096^3, burst); "
-                                            "MEASURED_PEAKS.json has no FP64 figure",
-                             "flop_per_orbit_step": FLOP_PER_STEP, "kernel": "k_calc_all_fp64",
+                "roofline": {"bound": "fp64" if form == GALIC_FORM_FP64 else "fp32", "achieved": achieved,
+                             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                             "peak_source": ("measured FP64 GEMM (torch.matmul float64 4096^3, burst)"
+                                             if form == GALIC_FORM_FP64 else
+                                             "measured FP32 SIMT GEMM (torch.matmul float32 8192^3, TF32 off, "
+                                             "burst)") + "; MEASURED_PEAKS.json has no FP32/FP64 figure",
+                             "flop_per_orbit_step": FLOP_PER_STEP,
+                             "kernel": "k_calc_all_fp64" if form == GALIC_FORM_FP64 else "k_calc_all_fp32",
                              "kernel_ms": kern_avg},
+                "forms": {args.form: value, ("fp64" if args.form == "fp32" else "fp32"): other_value,
+                          "fp32_over_fp64": (value / other_value) if args.form == "fp32" else (other_value / value),
+                          "unit": "orbit-steps/s"},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
