@@ -56,6 +56,15 @@ class GalicParams(C.Structure):
         return other
 
 
+class GalicFillParams(C.Structure):
+    """galic_fill_params_t: parameters of the tree force-grid fill."""
+    _fields_ = [
+        ("FG_Nbin", C.c_int), ("MultipleDomains", C.c_int),
+        ("FG_Rmin", C.c_double), ("FG_Fac", C.c_double), ("G", C.c_double),
+        ("ForceSoftening", C.c_double), ("ErrTolTheta", C.c_double), ("TopNodeFactor", C.c_double),
+    ]
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
@@ -108,6 +117,8 @@ SIGNATURES = [
     ("galic_last_kernel_launches", C.c_int, [VP]),
     ("galic_orbit_responses_noalloc", C.c_int,
      [C.POINTER(GalicParams), VP, VP, VP, VP, C.c_double, C.c_int, VP, VP, VP, VP, VP, VP, VP, VP]),
+    ("galic_force_grid_fill", C.c_int, [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, PD]),
+    ("galic_peano_hilbert_key", C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
     ("galic_density_geometry", C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
     ("galic_smooth_stack", None, [PD, C.c_int]),

@@ -208,6 +208,36 @@ int galic_orbit_responses_noalloc(const galic_params_t *prm, const double *d_fg_
                                   const double *d_tint, const int *d_type, double *d_out, int *d_orbits,
                                   void *stream);
 
+/* ------------------------------------------------------- force-grid fill */
+
+/* Parameters of the tree force-grid fill, from `All` and the grid globals. */
+typedef struct {
+  int FG_Nbin;            /* FG_Nbin (grid.c:204) */
+  int MultipleDomains;    /* All.MultipleDomains (domain_toplevel.c:79) */
+  double FG_Rmin, FG_Fac; /* FG_Rmin, FG_Fac (grid.c:466-470) */
+  double G;               /* All.G (gravtree.c:456-463) */
+  double ForceSoftening;  /* All.ForceSoftening = 2.8 * All.Softening (init.c:83) */
+  double ErrTolTheta;     /* All.ErrTolTheta (forcetree_walk.c:109) */
+  double TopNodeFactor;   /* All.TopNodeFactor (domain_toplevel.c:79) */
+} galic_fill_params_t;
+
+/* Replaces the tree part of forcedensitygrid_calculate (grid.c:621-750):
+ * places the FG_Nbin^2 x 8 massless probe points of grid.c:680-704 beside
+ * the n sampled mass particles (pos[3n], mass[n], in the reference's P order:
+ * halo, disk, bulge, as drawn by grid.c:662-678), runs gravity()
+ * (gravtree.c:35-50) with one MPI rank, and writes the section-averaged
+ * FG_DPotDR, FG_DPotDz, FG_Pot (FG_Nbin^2 each, [iz * FG_Nbin + iR]).  The
+ * results are bit-identical to the single-rank reference.  ms_walk (may be
+ * NULL) receives the device time of the tree walk.  Mass particles closer
+ * than DomainLen / 2^30 to one another (the MAX_TREE_LEVEL case of
+ * forcetree.c:400-416) give GALIC_ERR_UNSUPPORTED. */
+int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const double *pos, const double *mass,
+                          double *fg_dpotdr, double *fg_dpotdz, double *fg_pot, double *ms_walk);
+
+/* peano_hilbert_key (peano.c:331-347) of the integer cell (x, y, z) with
+ * `bits` bits per dimension (bits <= 21). */
+uint64_t galic_peano_hilbert_key(int x, int y, int z, int bits);
+
 /* ---------------------------------------------------------- host helpers */
 
 /* Grid geometry of forcedensitygrid_create (grid.c:329-480): from Halo_A,

@@ -100,4 +100,10 @@ int orc_grid_geometry(double halo_a, double outer_frac, double inner_frac, int f
 int orc_density_geometry(int dg_maxlevel, double dg_rmin, double dg_fac, double *dgs_distance, double *cellsize,
                          double *cellvol);
 
+/* tree force-grid fill of forcedensitygrid_calculate (grid.c:621-750),
+ * single rank; oracle_forcegrid.c */
+uint64_t orc_peano_key(int x, int y, int z, int bits);
+int orc_force_grid_fill(const galic_fill_params_t *fp, int n, const double *pos, const double *mass,
+                        double *dpotdr, double *dpotdz, double *pot);
+
 #endif

@@ -310,3 +310,69 @@ int ref_geometry(const char *outdir, double outer_frac, double inner_frac, doubl
   memcpy(cellvol, DG_CellVol, DG_Ngrid * sizeof(double));
   return 0;
 }
+
+/* ------------------------------------------------------------ force-grid fill */
+
+/* extra parameters of the force-grid fill (All.* members, grid.c:621-757,
+ * init.c:31-32, 78-84) */
+typedef struct {
+  double Softening, ErrTolTheta, TopNodeFactor, Disk_H, Disk_Z0, Rmax;
+  int MultipleDomains, SampleForceNhalo, SampleForceNdisk, SampleForceNbulge;
+  unsigned long long seed;
+} ref_fill_params;
+
+static void ref_fill_setup(const ref_fill_params *f)
+{
+  All.Softening = f->Softening;
+  All.ForceSoftening = 2.8 * f->Softening; /* set_softenings, init.c:78-84 */
+  All.ErrTolTheta = f->ErrTolTheta;
+  All.TopNodeFactor = f->TopNodeFactor;
+  All.MultipleDomains = f->MultipleDomains;
+  All.TopNodeAllocFactor = 0.1; /* init.c:31-32 */
+  All.BufferSize = 100;         /* MB, as in Model_*.param */
+  All.BufferSizeGravity = 100;
+  All.TreeAllocFactor = 0.8;
+  All.Disk_H = f->Disk_H;
+  All.Disk_Z0 = f->Disk_Z0;
+  All.Rmax = f->Rmax;
+  All.HaloStretch = 1.0;
+  All.BulgeStretch = 1.0;
+  All.SampleForceNhalo = f->SampleForceNhalo;
+  All.SampleForceNdisk = f->SampleForceNdisk;
+  All.SampleForceNbulge = f->SampleForceNbulge;
+}
+
+/* the mass-particle positions forcedensitygrid_calculate draws (grid.c:659-678)
+ * for the same generator seed: halo, then disk, then bulge */
+void ref_fill_positions(const ref_fill_params *f, double *pos)
+{
+  int i, n = 0;
+  ref_fill_setup(f);
+  gsl_rng_set(random_generator, f->seed);
+  for(i = 0; i < f->SampleForceNhalo; i++, n++) halo_get_fresh_coordinate(&pos[3 * n]);
+  for(i = 0; i < f->SampleForceNdisk; i++, n++) disk_get_fresh_coordinate(&pos[3 * n]);
+  for(i = 0; i < f->SampleForceNbulge; i++, n++) bulge_get_fresh_coordinate(&pos[3 * n]);
+}
+
+/* forcedensitygrid_calculate (grid.c:621-891) with its tree force (gravity(),
+ * gravtree.c:35-50); run inside outdir, which receives forcefield.dat,
+ * forcetest.dat and target_*.dat */
+int ref_force_fill(const char *outdir, const ref_fill_params *f, double *dpotdr, double *dpotdz, double *pot)
+{
+  char cwd[4096];
+  if(!getcwd(cwd, sizeof(cwd))) return 1;
+  if(chdir(outdir) != 0) return 2;
+  strcpy(All.OutputDir, ".");
+  ref_fill_setup(f);
+  All.SampleDensityFieldForTargetResponse = 0;
+  gsl_rng_set(random_generator, f->seed);
+  forcedensitygrid_calculate();
+  if(chdir(cwd) != 0) return 3;
+  memcpy(dpotdr, FG_DPotDR, FG_Ngrid * sizeof(double));
+  memcpy(dpotdz, FG_DPotDz, FG_Ngrid * sizeof(double));
+  memcpy(pot, FG_Pot, FG_Ngrid * sizeof(double));
+  return 0;
+}
+
+/* peano_hilbert_key (peano.c:331-347) */
+unsigned long long ref_peano_key(int x, int y, int z, int bits) { return peano_hilbert_key(x, y, z, bits); }

@@ -75,6 +75,8 @@ def oracle_lib():
             "orc_steps_total": (C.c_longlong, [VP]),
             "orc_grid_geometry": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
             "orc_density_geometry": (C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
+            "orc_peano_key": (C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
+            "orc_force_grid_fill": (C.c_int, [C.POINTER(_ffi.GalicFillParams), C.c_int, PD, PD, PD, PD, PD]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -173,6 +175,63 @@ class Oracle:
 # --------------------------------------------------------------- the reference
 
 
+class RefFillParams(C.Structure):
+    """ref_fill_params of oracle/ref_driver.c: the All.* members of the fill."""
+    _fields_ = [("Softening", C.c_double), ("ErrTolTheta", C.c_double), ("TopNodeFactor", C.c_double),
+                ("Disk_H", C.c_double), ("Disk_Z0", C.c_double), ("Rmax", C.c_double),
+                ("MultipleDomains", C.c_int), ("SampleForceNhalo", C.c_int), ("SampleForceNdisk", C.c_int),
+                ("SampleForceNbulge", C.c_int), ("seed", C.c_ulonglong)]
+
+
+def oracle_force_grid_fill(fp, pos, mass):
+    """orc_force_grid_fill: (status, FG_DPotDR, FG_DPotDz, FG_Pot) as [N, N] arrays."""
+    L = oracle_lib()
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    N = fp.FG_Nbin
+    out = [np.zeros((N, N)) for _ in range(3)]
+    st = L.orc_force_grid_fill(C.byref(fp), len(mass), dptr(pos), dptr(mass), *[dptr(a) for a in out])
+    return st, out[0], out[1], out[2]
+
+
+def fill_masses(params, nh, nd, nb):
+    """P[].Mass of the sampled particles (grid.c:662-678)."""
+    m = []
+    if nh:
+        m += [params.Halo_Mass / nh] * nh
+    if nd:
+        m += [params.Disk_Mass / nd] * nd
+    if nb:
+        m += [params.Bulge_Mass / nb] * nb
+    return np.array(m, dtype=np.float64)
+
+
+def reference_force_fill(params, rf, with_grid=True):
+    """GALIC's own forcedensitygrid_calculate (one rank) for the model `params`
+    and fill settings `rf` (RefFillParams); returns (pos[n,3], mass[n],
+    FG_DPotDR, FG_DPotDz, FG_Pot).  Run it through run_reference()."""
+    import tempfile
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    n = rf.SampleForceNhalo + rf.SampleForceNdisk + rf.SampleForceNbulge
+    pos = np.zeros((n, 3))
+    L.ref_fill_positions(C.byref(rf), dptr(pos))
+    mass = fill_masses(params, rf.SampleForceNhalo, rf.SampleForceNdisk, rf.SampleForceNbulge)
+    N = params.FG_Nbin
+    out = [np.zeros((N, N)) for _ in range(3)]
+    if with_grid:
+        with tempfile.TemporaryDirectory() as d:
+            st = L.ref_force_fill(d.encode(), C.byref(rf), *[dptr(a) for a in out])
+        if st != 0:
+            raise RuntimeError(f"ref_force_fill status {st}")
+    return pos, mass, out[0], out[1], out[2]
+
+
+def reference_peano_keys(xyz, bits):
+    L = _ref_lib()
+    return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
+
+
 def _ref_lib():
     L = C.CDLL(REF_SO)
     sig = {
@@ -198,6 +257,9 @@ def _ref_lib():
         "ref_stack_difference": (C.c_double, [PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
         "ref_stack_difference_mod": (C.c_double, [PD, PD, C.c_int, PD, PD, C.c_double, PD, C.c_int]),
         "ref_geometry": (C.c_int, [C.c_char_p, C.c_double, C.c_double, PD, PD, PD, PD]),
+        "ref_fill_positions": (None, [C.POINTER(RefFillParams), PD]),
+        "ref_force_fill": (C.c_int, [C.c_char_p, C.POINTER(RefFillParams), PD, PD, PD]),
+        "ref_peano_key": (C.c_ulonglong, [C.c_int, C.c_int, C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
