@@ -108,6 +108,61 @@ def cpu_orbit_steps_per_s(model, seconds, cores=None):
     return steps / wall, kind, cores, orbits, steps
 
 
+FILL_FLOP_PER_INTERACTION = 19  # forcetree_walk.c:156-196: 3 sub, r2 (5), sqrt, 2 div, r2*r, 4 mul-add pairs
+FILL_FLOP_PER_TEST = 11         # forcetree_walk.c:96-109: 3 sub, r2 (5), 2 mul by theta, float len*len
+
+
+def fill_workload(model):
+    """Mass particles of the tree force-grid fill for the workload (one per
+    model particle, drawn from the same components) and the fill parameters:
+    softening 0.01 a, opening angle 0.4, TopNodeFactor 4, MultipleDomains 4."""
+    from galic_b200 import forcegrid, synth
+
+    comps = [synth.Component(**c) for c in model.meta["components"]]
+    pos, mass = synth.fill_sample(comps, [c.n for c in comps], model.meta["rmax"], seed=7)
+    p = model.params
+    halo_a = [c for c in comps if c.kind == "halo"][0].scale
+    fp = forcegrid.fill_params(p.FG_Nbin, p.FG_Rmin, p.FG_Fac, p.G, 0.01 * halo_a, 0.4, 4.0, 4)
+    return fp, pos, mass
+
+
+def measure_fill(model, steps, cpu, fp64_peak):
+    """galic_force_grid_fill through the C ABI with host buffers: per call the
+    host->device copies, key sort, tree build, walk and read-back."""
+    from galic_b200 import forcegrid
+
+    fp, pos, mass = fill_workload(model)
+    forcegrid.force_grid_fill(fp, pos, mass)
+    walls, walks, stats = [], [], None
+    for _ in range(max(steps, 1)):
+        t = time.perf_counter()
+        out = forcegrid.force_grid_fill(fp, pos, mass)
+        walls.append(time.perf_counter() - t)
+        stats = out[3]
+        walks.append(stats["ms_walk"])
+    walk_ms = statistics.mean(walks)
+    flop = stats["interactions"] * FILL_FLOP_PER_INTERACTION + stats["node_tests"] * FILL_FLOP_PER_TEST
+    achieved = flop / (walk_ms * 1e-3) / 1e12
+    res = {"probes": 8 * fp.FG_Nbin ** 2, "mass_particles": len(mass), "tree_items": stats["tree_items"],
+           "interactions": stats["interactions"], "node_tests": stats["node_tests"],
+           "ms_per_fill_e2e": statistics.mean(walls) * 1e3, "ms_walk": walk_ms,
+           "roofline_walk": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                             "frac": achieved / fp64_peak,
+                             "flop": f"{FILL_FLOP_PER_INTERACTION}/interaction + {FILL_FLOP_PER_TEST}/opening test"}}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+
+        t = time.perf_counter()
+        oracle_lib.oracle_force_grid_fill(fp, pos, mass)
+        cpu_s = time.perf_counter() - t
+        res["cpu_baseline"] = {"ms_per_fill": cpu_s * 1e3, "cores": 1, "kind": "port",
+                               "sample": "the whole fill, single rank (the restatement is bit-identical to the "
+                                         "reference's forcedensitygrid_calculate)"}
+        res["speedup_e2e_vs_cpu"] = cpu_s / statistics.mean(walls)
+    return res
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -333,6 +388,8 @@ def ours_arm(args, rank, world, local_rank):
     if rank == 0:
         peak = measured_fp64_peak(torch) if form == GALIC_FORM_FP64 else measured_fp32_peak(torch)
         kern_avg = sum(kern_ms) / len(kern_ms)
+        fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
+                            peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
         if world == 1 and args.cpu_seconds > 0:
@@ -360,6 +417,7 @@ def ours_arm(args, rank, world, local_rank):
                           "fp32_over_fp64": (value / other_value) if args.form == "fp32" else (other_value / value),
                           "unit": "orbit-steps/s"},
                 "cpu_baseline": cpu,
+                "force_grid_fill": fill,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,

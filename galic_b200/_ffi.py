@@ -65,6 +65,12 @@ class GalicFillParams(C.Structure):
     ]
 
 
+class GalicFillStats(C.Structure):
+    """galic_fill_stats_t: diagnostics of one fill."""
+    _fields_ = [("ms_walk", C.c_double), ("ms_total", C.c_double), ("tree_items", C.c_longlong),
+                ("tree_nodes", C.c_longlong), ("interactions", C.c_longlong), ("node_tests", C.c_longlong)]
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
@@ -117,7 +123,8 @@ SIGNATURES = [
     ("galic_last_kernel_launches", C.c_int, [VP]),
     ("galic_orbit_responses_noalloc", C.c_int,
      [C.POINTER(GalicParams), VP, VP, VP, VP, C.c_double, C.c_int, VP, VP, VP, VP, VP, VP, VP, VP]),
-    ("galic_force_grid_fill", C.c_int, [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, PD]),
+    ("galic_force_grid_fill", C.c_int,
+     [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, C.POINTER(GalicFillStats)]),
     ("galic_peano_hilbert_key", C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
     ("galic_density_geometry", C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),

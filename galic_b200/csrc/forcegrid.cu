@@ -37,6 +37,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -156,7 +157,8 @@ __global__ void k_keys(int n, const double *__restrict__ pos, double cx, double 
 // probes: SoA [3][np] in key order; res: SoA [4][np] (acc x, y, z, pot) * G.
 __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict__ items, int nitems, int np,
                                                     const double *__restrict__ probes, double hmax,
-                                                    double theta, double G, double *__restrict__ res)
+                                                    double theta, double G, double *__restrict__ res,
+                                                    unsigned long long *__restrict__ counts)
 {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = t < np;
@@ -170,6 +172,7 @@ __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict_
   unsigned next = live ? 0u : 0xFFFFFFFFu;  // 0xFFFFFFFF: walk finished
   const double h_inv = 1.0 / hmax;
   const double h3_inv = h_inv * h_inv * h_inv;
+  unsigned n_int = 0, n_test = 0;
   for(;;) {
     const unsigned cur = __reduce_min_sync(0xFFFFFFFFu, next);
     if(cur == 0xFFFFFFFFu) break;
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict_
     const double dz = it.z - pz;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if(it.len >= 0.f) {
+      n_test++;
       const float len2 = it.len * it.len;
       if((double) len2 > r2 * theta * theta) {
         // open: the first daughter follows; a node without daughters is
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict_
     next = it.skip < 0 ? 0xFFFFFFFFu : (unsigned) it.skip;
     const double mass = it.mass;
     if(mass != 0.0) {
+      n_int++;
       const double r = sqrt(r2);
       double fac, wp;
       if(r >= hmax) {
@@ -213,6 +218,16 @@ __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict_
       acc_z += dz * fac;
       pot += wp;
     }
+  }
+  // diagnostics: one atomic pair per warp
+  unsigned long long a = n_int, b = n_test;
+  for(int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+    b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+  }
+  if((threadIdx.x & 31) == 0) {
+    atomicAdd(&counts[0], a);
+    atomicAdd(&counts[1], b);
   }
   if(live) {  // gravtree.c:456-463
     res[t] = acc_x * G;
@@ -401,8 +416,9 @@ extern "C" uint64_t galic_peano_hilbert_key(int x, int y, int z, int bits)
   } while(0)
 
 extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const double *pos, const double *mass,
-                                     double *fg_dpotdr, double *fg_dpotdz, double *fg_pot, double *ms_walk)
+                                     double *fg_dpotdr, double *fg_dpotdz, double *fg_pot, galic_fill_stats_t *stats)
 {
+  const auto t_start = std::chrono::steady_clock::now();
   if(!fp || n < 1 || !pos || !mass || !fg_dpotdr || !fg_dpotdz || !fg_pot || fp->FG_Nbin < 2 ||
      fp->FG_Nbin > 4096 || !(fp->FG_Fac > 1) || !(fp->FG_Rmin > 0) || !(fp->ErrTolTheta > 0) ||
      !(fp->ForceSoftening > 0) || fp->MultipleDomains < 1 || !(fp->TopNodeFactor > 0) ||
@@ -520,13 +536,15 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     for(int j = 0; j < 3; j++) probes[(size_t) j * np + t] = P[3 * ((size_t) n + id) + j];
     t++;
   }
-  DevBuf d_items, d_probes, d_res, d_rank, d_trig, d_out;
+  DevBuf d_items, d_probes, d_res, d_rank, d_trig, d_out, d_counts;
   FCK(cudaMalloc(&d_items.p, (size_t) nitems * sizeof(FillItem)));
   FCK(cudaMalloc(&d_probes.p, 3 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_res.p, 4 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_rank.p, (size_t) np * sizeof(int)));
   FCK(cudaMalloc(&d_trig.p, sizeof(trig)));
   FCK(cudaMalloc(&d_out.p, 3 * (size_t) NN * sizeof(double)));
+  FCK(cudaMalloc(&d_counts.p, 2 * sizeof(unsigned long long)));
+  FCK(cudaMemset(d_counts.p, 0, 2 * sizeof(unsigned long long)));
   FCK(cudaMemcpy(d_items.p, tb.items.data(), (size_t) nitems * sizeof(FillItem), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_probes.p, probes.data(), 3 * (size_t) np * sizeof(double), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_rank.p, rank.data(), (size_t) np * sizeof(int), cudaMemcpyHostToDevice));
@@ -538,7 +556,8 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cudaEventRecord(e0));
   k_walk<<<(np + kWalkBlock - 1) / kWalkBlock, kWalkBlock>>>(d_items.as<FillItem>(), nitems, np, d_probes.as<double>(),
                                                              fp->ForceSoftening, fp->ErrTolTheta, fp->G,
-                                                             d_res.as<double>());
+                                                             d_res.as<double>(),
+                                                             d_counts.as<unsigned long long>());
   cudaError_t e = cudaGetLastError();
   cudaEventRecord(e1);
   if(e == cudaSuccess) {
@@ -552,10 +571,20 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   FCK(e);
-  if(ms_walk) *ms_walk = ms;
+  unsigned long long counts[2];
+  FCK(cudaMemcpy(counts, d_counts.p, sizeof(counts), cudaMemcpyDeviceToHost));
   FCK(cudaMemcpy(fg_dpotdr, d_out.p, (size_t) NN * sizeof(double), cudaMemcpyDeviceToHost));
   FCK(cudaMemcpy(fg_dpotdz, d_out.as<double>() + NN, (size_t) NN * sizeof(double), cudaMemcpyDeviceToHost));
   FCK(cudaMemcpy(fg_pot, d_out.as<double>() + 2 * (size_t) NN, (size_t) NN * sizeof(double),
                  cudaMemcpyDeviceToHost));
+  if(stats) {
+    stats->ms_walk = ms;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    stats->tree_items = nitems;
+    stats->tree_nodes = nitems - n;
+    stats->interactions = (long long) counts[0];
+    stats->node_tests = (long long) counts[1];
+  }
   return GALIC_OK;
 }

@@ -29,7 +29,8 @@ def fill_params(fg_nbin, fg_rmin, fg_fac, G, softening, theta=0.4, top_node_fact
 
 
 def force_grid_fill(fp, pos, mass):
-    """(FG_DPotDR, FG_DPotDz, FG_Pot, walk ms) for mass particles pos[n,3], mass[n]."""
+    """(FG_DPotDR, FG_DPotDz, FG_Pot, stats) for mass particles pos[n,3], mass[n];
+    stats is a dict of galic_fill_stats_t."""
     lib = _ffi.load_library()
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     mass = np.ascontiguousarray(mass, dtype=np.float64)
@@ -38,10 +39,10 @@ def force_grid_fill(fp, pos, mass):
         raise ValueError("pos must be [n, 3]")
     N = fp.FG_Nbin
     out = [np.empty((N, N)) for _ in range(3)]
-    ms = C.c_double(0.0)
+    st = _ffi.GalicFillStats()
     _check(lib.galic_force_grid_fill(C.byref(fp), n, _ffi.dptr(pos), _ffi.dptr(mass), _ffi.dptr(out[0]),
-                                     _ffi.dptr(out[1]), _ffi.dptr(out[2]), C.byref(ms)), "galic_force_grid_fill")
-    return out[0], out[1], out[2], ms.value
+                                     _ffi.dptr(out[1]), _ffi.dptr(out[2]), C.byref(st)), "galic_force_grid_fill")
+    return out[0], out[1], out[2], {k: getattr(st, k) for k, _ in _ffi.GalicFillStats._fields_}
 
 
 def peano_hilbert_key(x, y, z, bits):

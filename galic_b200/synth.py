@@ -357,6 +357,23 @@ def build_model(comps, seed=1, level=6, fg_nbin=256, outer_frac=0.980296, inner_
 
 # ------------------------------------------------------------------ named configurations
 
+def fill_sample(comps, counts, rmax, seed=7):
+    """Mass particles of the tree force-grid fill (grid.c:662-678): counts[k]
+    positions drawn from the density of comps[k], in the reference's P order
+    (halo, disk, bulge), with P[].Mass = component mass / count.  Returns
+    (pos[n, 3], mass[n])."""
+    rng = np.random.default_rng(seed)
+    order = sorted(range(len(comps)), key=lambda k: TYPE_OF[comps[k].kind])
+    pos, mass = [], []
+    for k in order:
+        n = int(counts[k])
+        if n <= 0:
+            continue
+        pos.append(_sample_positions(comps[k], n, rng, rmax))
+        mass.append(np.full(n, comps[k].mass / n))
+    return np.concatenate(pos), np.concatenate(mass)
+
+
 def config_halo(n=100000, seed=1, level=6):
     """Plain method: Hernquist M=100, a=30 kpc, isotropic; 64x64 (R,|z|) response grid (DG level 6)
     from 0.01a to 100a; 256x256 force grid; TorbitFac 5, ~200 steps/orbit."""

@@ -221,18 +221,27 @@ typedef struct {
   double TopNodeFactor;   /* All.TopNodeFactor (domain_toplevel.c:79) */
 } galic_fill_params_t;
 
+/* Diagnostics of one fill. */
+typedef struct {
+  double ms_walk;            /* device time of the tree walk (CUDA events) */
+  double ms_total;           /* host time of the whole call */
+  long long tree_items;      /* nodes + single-particle leaves of the tree */
+  long long tree_nodes;      /* internal nodes (forcetree.c Tree_NumNodes) */
+  long long interactions;    /* particle/node interactions summed over the probes */
+  long long node_tests;      /* opening tests summed over the probes */
+} galic_fill_stats_t;
+
 /* Replaces the tree part of forcedensitygrid_calculate (grid.c:621-750):
  * places the FG_Nbin^2 x 8 massless probe points of grid.c:680-704 beside
  * the n sampled mass particles (pos[3n], mass[n], in the reference's P order:
  * halo, disk, bulge, as drawn by grid.c:662-678), runs gravity()
  * (gravtree.c:35-50) with one MPI rank, and writes the section-averaged
  * FG_DPotDR, FG_DPotDz, FG_Pot (FG_Nbin^2 each, [iz * FG_Nbin + iR]).  The
- * results are bit-identical to the single-rank reference.  ms_walk (may be
- * NULL) receives the device time of the tree walk.  Mass particles closer
- * than DomainLen / 2^30 to one another (the MAX_TREE_LEVEL case of
- * forcetree.c:400-416) give GALIC_ERR_UNSUPPORTED. */
+ * results are bit-identical to the single-rank reference.  stats may be
+ * NULL.  Mass particles closer than DomainLen / 2^30 to one another (the
+ * MAX_TREE_LEVEL case of forcetree.c:400-416) give GALIC_ERR_UNSUPPORTED. */
 int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const double *pos, const double *mass,
-                          double *fg_dpotdr, double *fg_dpotdz, double *fg_pot, double *ms_walk);
+                          double *fg_dpotdr, double *fg_dpotdz, double *fg_pot, galic_fill_stats_t *stats);
 
 /* peano_hilbert_key (peano.c:331-347) of the integer cell (x, y, z) with
  * `bits` bits per dimension (bits <= 21). */

@@ -142,6 +142,9 @@ def test_gpu_fill_matches_reference_fixture(path):
     got = forcegrid.force_grid_fill(fp, pos, mass)
     for g, w in zip(got[:3], want):
         assert np.array_equal(g, w)
+    st = got[3]
+    assert st["tree_items"] > len(mass) and st["tree_nodes"] == st["tree_items"] - len(mass)
+    assert st["interactions"] > 0 and st["node_tests"] > 0 and st["ms_walk"] > 0
 
 
 @pytest.mark.gpu
