@@ -44,6 +44,7 @@ def parse():
                     help="form of the headline value; the other form is measured beside it")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's particle count")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ensemble-models", type=int, default=64, help="models of the batched ensemble (0: skip)")
     return ap.parse_args()
 
 
@@ -160,6 +161,48 @@ def measure_fill(model, steps, cpu, fp64_peak):
                                "sample": "the whole fill, single rank (the restatement is bit-identical to the "
                                          "reference's forcedensitygrid_calculate)"}
         res["speedup_e2e_vs_cpu"] = cpu_s / statistics.mean(walls)
+    return res
+
+
+def measure_ensemble(count, steps):
+    """Batched ensemble: `count` Hernquist halos of uneven N advanced per
+    iteration by one persistent FP32 launch replayed from a CUDA graph, tile
+    variant picked by the autotuner; beside it the same models one launch
+    sequence per model (galic_calc_all_response_fields each)."""
+    from galic_b200 import GALIC_FORM_FP32, Context, synth
+    from galic_b200.ensemble import Ensemble
+
+    models = synth.config_ensemble(count=count)
+    ctxs = []
+    for m in models:
+        c = Context(m.params)
+        c.load_model(m)
+        ctxs.append(c)
+    e = Ensemble(ctxs)
+    best, tune_ms = e.autotune(0.05)
+    e.calc_all()  # builds and runs the graph once
+    tot, kern, st = [], [], []
+    for _ in range(max(steps, 1)):
+        e.calc_all()
+        a, b, n, nodes = e.last_timing()
+        tot.append(a)
+        kern.append(b)
+        st.append(n)
+    seq_ms = 0.0
+    for c in ctxs:
+        c.calc_all_response_fields(GALIC_FORM_FP32)
+        seq_ms += c.last_timing()[0]
+    res = {"models": count, "particles": int(sum(m.n for m in models)),
+           "n_range": [int(min(m.n for m in models)), int(max(m.n for m in models))],
+           "orbit_steps_per_iteration": st[-1], "ms_per_iteration": statistics.mean(tot),
+           "ms_orbit_kernel": statistics.mean(kern), "value": st[-1] / (statistics.mean(tot) * 1e-3),
+           "unit": "orbit-steps/s", "variant": {"index": best, "block_min_blocks": Ensemble.variants()[best]},
+           "autotune_ms": [round(float(x), 3) for x in tune_ms], "graph_nodes": nodes,
+           "sequential_ms_per_iteration": seq_ms,
+           "speedup_vs_sequential": seq_ms / statistics.mean(tot)}
+    e.close()
+    for c in ctxs:
+        c.close()
     return res
 
 
@@ -390,6 +433,7 @@ def ours_arm(args, rank, world, local_rank):
         kern_avg = sum(kern_ms) / len(kern_ms)
         fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
+        ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
         if world == 1 and args.cpu_seconds > 0:
@@ -418,6 +462,7 @@ def ours_arm(args, rank, world, local_rank):
                           "unit": "orbit-steps/s"},
                 "cpu_baseline": cpu,
                 "force_grid_fill": fill,
+                "ensemble": ensemble,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,

@@ -123,6 +123,14 @@ SIGNATURES = [
     ("galic_last_kernel_launches", C.c_int, [VP]),
     ("galic_orbit_responses_noalloc", C.c_int,
      [C.POINTER(GalicParams), VP, VP, VP, VP, C.c_double, C.c_int, VP, VP, VP, VP, VP, VP, VP, VP]),
+    ("galic_ensemble_create", C.c_int, [C.POINTER(VP), C.c_int, C.POINTER(VP)]),
+    ("galic_ensemble_destroy", None, [VP]),
+    ("galic_ensemble_last_status", C.c_int, [VP]),
+    ("galic_ensemble_calc_all", C.c_int, [VP]),
+    ("galic_ensemble_variants", C.c_int, [PI, PI, C.c_int]),
+    ("galic_ensemble_set_variant", C.c_int, [VP, C.c_int]),
+    ("galic_ensemble_autotune", C.c_int, [VP, C.c_double, PI, PD]),
+    ("galic_ensemble_last_timing", C.c_int, [VP, PD, PD, PLL, PI]),
     ("galic_force_grid_fill", C.c_int,
      [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, C.POINTER(GalicFillStats)]),
     ("galic_peano_hilbert_key", C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),

@@ -11,66 +11,11 @@
 #include <string>
 #include <vector>
 
+#include "context.cuh"
 #include "galic_gpu.h"
 #include "kernels.cuh"
 #include "rep.cuh"
 
-struct galic_ctx {
-  galic_params_t prm;
-  int status = 0;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  DevModel dm{};
-  int G = 0, Ns = 0, L = 0;
-  // tables
-  double2 *d_fg_acc = nullptr;
-  double *d_fg_pot = nullptr, *d_vstream[4] = {nullptr, nullptr, nullptr, nullptr};
-  double *d_cellsize = nullptr, *d_dist = nullptr;
-  double *d_targets = nullptr;    // [4][6][Ns]
-  double *d_committed = nullptr;  // [4][10][G]
-  double *d_stacks = nullptr;     // [4][10][Ns]
-  FxWord *d_fx = nullptr;         // [4][10][G]
-  int *d_shift = nullptr;         // [4][10]
-  double *d_fit = nullptr;        // [4][7] + raw [4][5]
-  int *d_firstrun = nullptr;      // [4]
-  unsigned long long *d_counters = nullptr;  // tries[4], changes[4], steps
-  int *d_status = nullptr;
-  int *d_next = nullptr;
-  double *d_maxerr = nullptr;
-  double pot_min = 0;
-  bool have_fg = false, have_geom = false, have_response = false;
-  bool have_targets[4] = {false, false, false, false};
-  // particles
-  int n = 0;
-  double *d_pos = nullptr, *d_vel = nullptr, *d_mass = nullptr, *d_tint = nullptr, *d_vesc = nullptr;
-  double *d_ptargets = nullptr, *d_vdisp = nullptr;
-  int *d_type = nullptr, *d_orbits = nullptr;
-  int *d_order = nullptr;  // orbit processing order of the batched kernels (by initial radius)
-  // scratch of the per-orbit drop-ins and the repetition
-  int scratch_orbits = 0;
-  double *d_b_pos = nullptr, *d_b_vel = nullptr, *d_b_mass = nullptr, *d_b_time = nullptr, *d_grids = nullptr;
-  double *d_b_tall = nullptr, *d_b_err = nullptr;
-  int *d_b_type = nullptr, *d_b_norbit = nullptr, *d_b_status = nullptr;
-  long long *d_b_steps = nullptr;
-  int scratch_rep = 0;
-  int *d_idx = nullptr, *d_accepted = nullptr;
-  double *d_vel_try = nullptr, *d_F = nullptr, *d_inst_v = nullptr;
-  Cell *d_inst_cell = nullptr;
-  // diagnostics
-  long long last_steps = 0;
-  int last_launches = 0;
-  double last_max_egy_err = 0;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  // FP32 form: per type a quad table, 4 float4 per force-grid cell (iz, iR):
-  // DPotDR, DPotDz and Vstream[type] of the corners (iz,iR), (iz,iR+1),
-  // (iz+1,iR), (iz+1,iR+1), then padding
-  std::vector<double> h_dpotdr, h_dpotdz, h_vstream[4];
-  float4 *d_tab32[4] = {nullptr, nullptr, nullptr, nullptr};
-  float *d_cellsize32 = nullptr;
-  bool tab32_dirty = true;
-  std::vector<double> h_cellsize;
-  double last_ms_total = 0, last_ms_orbit = 0;
-};
 
 namespace {
 
@@ -173,6 +118,10 @@ int ensure_rep_scratch(galic_ctx *ctx, int count)
   return GALIC_OK;
 }
 
+}  // namespace
+
+namespace galic_internal {
+
 FitArgs make_fit_args(galic_ctx *ctx)
 {
   FitArgs f;
@@ -262,7 +211,9 @@ int ensure_tab32(galic_ctx *ctx)
   return GALIC_OK;
 }
 
-}  // namespace
+}  // namespace galic_internal
+
+using namespace galic_internal;
 
 extern "C" const char *galic_status_string(int status)
 {
@@ -392,6 +343,7 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
 extern "C" int galic_set_force_grid(galic_ctx *ctx, const double *pot, const double *dpotdr, const double *dpotdz)
 {
   if(!ctx || !pot || !dpotdr || !dpotdz) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   const int NF = ctx->prm.FG_Nbin * ctx->prm.FG_Nbin;
   std::vector<double2> acc(NF);
   double pmin = 0;
@@ -412,6 +364,7 @@ extern "C" int galic_set_force_grid(galic_ctx *ctx, const double *pot, const dou
 extern "C" int galic_set_vstream(galic_ctx *ctx, int type, const double *v)
 {
   if(!ctx || !v || type < 1 || type > 3) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   const int NF = ctx->prm.FG_Nbin * ctx->prm.FG_Nbin;
   int zero = 1;
   for(int i = 0; i < NF && zero; i++) {
@@ -429,6 +382,7 @@ extern "C" int galic_set_vstream(galic_ctx *ctx, int type, const double *v)
 extern "C" int galic_set_density_geometry(galic_ctx *ctx, const double *cellsize, const double *dist)
 {
   if(!ctx || !cellsize || !dist) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   CK(cudaMemcpy(ctx->d_cellsize, cellsize, ctx->G * sizeof(double), cudaMemcpyHostToDevice));
   ctx->h_cellsize.assign(cellsize, cellsize + ctx->G);
   ctx->tab32_dirty = true;
@@ -442,6 +396,7 @@ extern "C" int galic_set_targets(galic_ctx *ctx, int type, const double *dgs_mas
 {
   if(!ctx || type < 1 || type > 3 || !dgs_mass || !egs_mass || !egs_r || !egs_t || !egs_p || !egs_q)
     return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   const double *src[NT_TARGET] = {dgs_mass, egs_mass, egs_r, egs_t, egs_p, egs_q};
   for(int k = 0; k < NT_TARGET; k++)
     CK(cudaMemcpy(ctx->d_targets + ((size_t) type * NT_TARGET + k) * ctx->Ns, src[k], ctx->Ns * sizeof(double),
@@ -457,6 +412,7 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
     return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   for(int i = 0; i < n; i++)
     if(type[i] < 1 || type[i] > 3 || !(tint[i] > 0)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   if(n != ctx->n) {
     dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
     dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits); dfree(ctx->d_order);
@@ -809,6 +765,7 @@ extern "C" int galic_get_response(galic_ctx *ctx, int type, int which, double *o
 extern "C" int galic_set_step_cap(galic_ctx *ctx, long long cap)
 {
   if(!ctx || cap < 1) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  ctx->generation++;
   ctx->dm.step_cap = cap;
   return fail(ctx, GALIC_OK);
 }

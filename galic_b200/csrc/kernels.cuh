@@ -81,4 +81,28 @@ int calc_all_fp32_occupancy(int block);
 int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
                          const CalcAllArgs &a, int grid, int block, cudaStream_t s);
 
+// ---- ensemble of models in one persistent FP32 launch (orbit_fp32.cu)
+#define GALIC_ENSEMBLE_MAX 64
+struct EnsembleLaunch {
+  int nmodels;
+  int offset[GALIC_ENSEMBLE_MAX + 1];  // prefix sums of the models' orbit counts
+  DevModel dm[GALIC_ENSEMBLE_MAX];
+  const float4 *quad[GALIC_ENSEMBLE_MAX][4];
+  const float *cellsize32[GALIC_ENSEMBLE_MAX];
+  const void *members;  // device array of ensemble_member_bytes() per model
+  int *next;
+  FxWord *fx;           // [models * 4][NG_COMMITTED][Ngrid]
+  const int *shift;     // [models * 4][NG_COMMITTED]
+  unsigned long long *steps;
+  double *maxerr;
+  int *status;
+};
+int ensemble_variant_count();
+int ensemble_variant(int v, int *block, int *min_blocks);
+int ensemble_occupancy(int v);
+size_t ensemble_member_bytes();
+void ensemble_fill_member(void *dst, const DevModel &dm, const double *pos, const double *vel, const double *mass,
+                          const double *tint, const int *type, const int *order, int *orbits);
+cudaError_t launch_ensemble_fp32(const EnsembleLaunch &L, int v, int grid, cudaStream_t s);
+
 #endif

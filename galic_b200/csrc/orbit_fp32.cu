@@ -17,6 +17,9 @@
 // Built with --fmad=true (this file keeps contraction on).
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstring>
+
 #include "flush.cuh"
 #include "kernels.cuh"
 
@@ -35,6 +38,7 @@ struct Model32 {
   float dgmax;             // DG_Nbin - 1
   const float4 *quad[4];   // per type, per cell iz*N+iR: {DPotDR x4}, {DPotDz x4}, {Vstream x4}, pad
   const float *cellsize;
+  long long step_cap;
 };
 
 __device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
@@ -254,46 +258,152 @@ struct State32 {
 
 enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
 
-__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS) k_calc_all_fp32(DevModel M64, Model32 M, CalcAllArgs A,
-                                                                     long long step_cap)
+// Particle arrays of one model
+struct Particles32 {
+  const double *pos, *vel, *mass, *tint;
+  const int *type;
+  const int *order;  // processing order
+  int *orbits;
+};
+
+// Work source of one model (the context path): the model's constants are
+// kernel parameters, so every access is a constant-bank operand.
+struct SingleSrc {
+  DevModel M64;
+  Model32 M;
+  Particles32 P;
+  int n;
+  int *next;
+  FxWord *fx;        // [4][NG_COMMITTED][Ngrid]
+  const int *shift;  // [4][NG_COMMITTED]
+  unsigned long long *steps_total;
+  double *max_egy_err;
+  int *status;
+  __device__ __forceinline__ const Model32 &model(int) const { return M; }
+  __device__ __forceinline__ const DevModel &model64(int) const { return M64; }
+  __device__ __forceinline__ const Particles32 &particles(int) const { return P; }
+  __device__ __forceinline__ int gridset(int, int type) const { return type; }
+  __device__ __forceinline__ bool take(int &mi, int &p) const
+  {
+    const int k = atomicAdd(next, 1);
+    if(k >= n) return false;
+    mi = 0;
+    p = P.order ? P.order[k] : k;
+    return true;
+  }
+  __device__ __forceinline__ void flush_stats(int, unsigned long long st, double err, int stat) const
+  {
+    if(st) atomicAdd(steps_total, st);
+    if(err > 0) atomicMax((unsigned long long *) max_egy_err, (unsigned long long) __double_as_longlong(err));
+    if(stat) atomicMax(status, stat);
+  }
+};
+
+// Work source of an ensemble: orbits of all member models form one index
+// space (model-major, each model in its own processing order); per-step
+// constants of every model sit in the parameter space and are indexed by the
+// lane's model (uniform across a warp except where two models meet).
+struct EnsembleMember {
+  DevModel dm;
+  Particles32 part;
+};
+
+struct EnsembleSrc {
+  int nmodels, total;
+  int offset[GALIC_ENSEMBLE_MAX + 1];  // first orbit index of each model
+  Model32 m[GALIC_ENSEMBLE_MAX];
+  const EnsembleMember *mem;
+  int *next;
+  FxWord *fx;        // [models * 4][NG_COMMITTED][Ngrid]
+  const int *shift;  // [models * 4][NG_COMMITTED]
+  unsigned long long *steps;  // [models]
+  double *maxerr;             // [models]
+  int *status;                // [models]
+  __device__ __forceinline__ const Model32 &model(int mi) const { return m[mi]; }
+  __device__ __forceinline__ const DevModel &model64(int mi) const { return mem[mi].dm; }
+  __device__ __forceinline__ const Particles32 &particles(int mi) const { return mem[mi].part; }
+  __device__ __forceinline__ int gridset(int mi, int type) const { return 4 * mi + type; }
+  __device__ __forceinline__ bool take(int &mi, int &p) const
+  {
+    const int k = atomicAdd(next, 1);
+    if(k >= total) return false;
+    int lo = 0, hi = nmodels;
+    while(hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if(offset[mid] <= k)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    mi = lo;
+    p = mem[lo].part.order[k - offset[lo]];
+    return true;
+  }
+  __device__ __forceinline__ void flush_stats(int mi, unsigned long long st, double err, int stat) const
+  {
+    if(st) atomicAdd(&steps[mi], st);
+    if(err > 0) atomicMax((unsigned long long *) &maxerr[mi], (unsigned long long) __double_as_longlong(err));
+    if(stat) atomicMax(&status[mi], stat);
+  }
+};
+
+// log(FG_Fac) for the FP64 potential of the energy check (grid.c:68-74)
+__device__ __forceinline__ LogConsts pot_logs(const DevModel &M)
 {
-  __shared__ WarpQueue32 queues[CALC_ALL_BLOCK_FP32 / 32];
-  LogConsts L64 = make_log_consts(M64);
-  const int G = M64.DG_Ngrid;
+  LogConsts c;
+  c.lfg = gm_log(M.FG_Fac);
+  c.ldg = c.leg = 0.0;
+  return c;
+}
+
+template <int BLOCK, class Src>
+__device__ __forceinline__ void calc_all_fp32_body(const Src &S)
+{
+  __shared__ WarpQueue32 queues[BLOCK / 32];
+  const int G = S.model64(0).DG_Ngrid;
   State32 s;
   Sink32 sink;
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
-  sink.Nb = M.DG_Nbin;
   sink.cur = -1;
   sink.parked = false;
-  int p = -1;
+  int p = -1, mi = 0, stat_mi = 0;
   unsigned long long my_steps = 0;
   double my_err = 0;
   int my_status = 0;
 
   auto begin = [&]() -> bool {
-    int k = atomicAdd(A.next, 1);
-    if(k >= A.n) {
+    int nmi;
+    if(!S.take(nmi, p)) {
       p = -1;
       return false;
     }
-    p = A.order ? A.order[k] : k;
-    const int type = A.type[p];
-    sink.type = type;
-    sink.fac = A.mass[p] / A.tint[p];
+    if(nmi != stat_mi) {  // statistics are kept per model
+      S.flush_stats(stat_mi, my_steps, my_err, my_status);
+      my_steps = 0;
+      my_err = 0;
+      my_status = 0;
+      stat_mi = nmi;
+    }
+    mi = nmi;
+    const Model32 &M = S.model(mi);
+    const Particles32 &P = S.particles(mi);
+    const int type = P.type[p];
+    sink.Nb = M.DG_Nbin;
+    sink.type = S.gridset(mi, type);
+    sink.fac = P.mass[p] / P.tint[p];
     sink.cur = -1;
     double xd[3], vd[3];
     for(int i = 0; i < 3; i++) {
-      xd[i] = A.pos[3 * p + i];
-      vd[i] = A.vel[3 * p + i];
+      xd[i] = P.pos[3 * p + i];
+      vd[i] = P.vel[3 * p + i];
       s.x[i] = (float) xd[i];
       s.v[i] = (float) vd[i];
     }
     s.type = type;
     s.tovs = M.tovs[type];
     s.tall = 0;
-    s.timespan = A.tint[p];
+    s.timespan = P.tint[p];
     s.radsign_prev = 0.f;
     s.norbit = 0;
     s.flag = 0;
@@ -308,7 +418,8 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS) k_
     s.fz = c.fz;
     s.proj = project32(s.tovs, s.x, s.v, vstr);
     s.cs_cell = -1;
-    s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, L64, xd);
+    const DevModel &M64 = S.model64(mi);
+    s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, pot_logs(M64), xd);
     return true;
   };
 
@@ -316,11 +427,12 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS) k_
   for(;;) {
     const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
     if(full) {
-      warp_drain32(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
+      warp_drain32(*sink.q, full, S.fx, S.shift, G, S.model(0).DG_Nbin);
       sink.parked = false;
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
     if(state == LANE_ACTIVE) {
+      const Model32 &M = S.model(mi);
       // get_timestep (orbit_response.c:16-26)
       const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
       const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
@@ -362,43 +474,44 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS) k_
       if(!(s.tall == s.tall)) {
         s.status = ORBIT_NONFINITE;
         state = LANE_FINISH;
-      } else if(s.steps > step_cap) {
+      } else if(s.steps > M.step_cap) {
         s.status = ORBIT_STEP_CAP;
         state = LANE_FINISH;
       } else if(s.flag)
         state = LANE_FINISH;
     } else if(state == LANE_FINISH) {
       sink.park();
-      A.orbits[p] = s.norbit;
+      S.particles(mi).orbits[p] = s.norbit;
       my_steps += (unsigned long long) s.steps;
       if(s.status != ORBIT_OK)
         my_status = max(my_status, s.status);
       else {
+        const DevModel &M64 = S.model64(mi);
         double xd[3] = {s.x[0], s.x[1], s.x[2]};
         double vd0 = s.v[0], vd1 = s.v[1], vd2 = s.v[2];
-        double E1 = 0.5 * (vd0 * vd0 + vd1 * vd1 + vd2 * vd2) + forcegrid_pot(M64, L64, xd);
+        double E1 = 0.5 * (vd0 * vd0 + vd1 * vd1 + vd2 * vd2) + forcegrid_pot(M64, pot_logs(M64), xd);
         double e = fabs((E1 - s.E0) / s.E0);
         if(e > my_err) my_err = e;
       }
       state = begin() ? LANE_ACTIVE : LANE_DONE;
     }
   }
-  if(my_steps) atomicAdd(A.steps_total, my_steps);
-  if(my_err >= 0) atomicMax((unsigned long long *) A.max_egy_err, (unsigned long long) __double_as_longlong(my_err));
-  if(my_status) atomicMax(A.status, my_status);
+  S.flush_stats(stat_mi, my_steps, my_err, my_status);
 }
 
-}  // namespace
-
-int calc_all_fp32_occupancy(int block)
+__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS)
+    k_calc_all_fp32(const __grid_constant__ SingleSrc S)
 {
-  int blocks = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_calc_all_fp32, block, 0);
-  return blocks;
+  calc_all_fp32_body<CALC_ALL_BLOCK_FP32>(S);
 }
 
-int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
-                         const CalcAllArgs &a, int grid, int block, cudaStream_t s)
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_ensemble_fp32(const __grid_constant__ EnsembleSrc S)
+{
+  calc_all_fp32_body<BLOCK>(S);
+}
+
+Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32)
 {
   Model32 M;
   M.V200 = (float) M64.V200;
@@ -427,6 +540,120 @@ int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const
   M.fgmax = (float) (M64.FG_Nbin - 1);
   M.dgmax = (float) (M64.DG_Nbin - 1);
   M.cellsize = cellsize32;
-  k_calc_all_fp32<<<grid, block, 0, s>>>(M64, M, a, M64.step_cap);
+  M.step_cap = M64.step_cap;
+  return M;
+}
+
+// tile variants of the ensemble kernel: threads per CTA, CTAs per SM asked of
+// the register allocator
+struct Variant {
+  int block, min_blocks;
+};
+constexpr Variant kVariants[] = {{256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}, {384, 2}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+template <int V>
+void *variant_kernel()
+{
+  return (void *) k_ensemble_fp32<kVariants[V].block, kVariants[V].min_blocks>;
+}
+
+void *ensemble_kernel(int v)
+{
+  switch(v) {
+    case 0: return variant_kernel<0>();
+    case 1: return variant_kernel<1>();
+    case 2: return variant_kernel<2>();
+    case 3: return variant_kernel<3>();
+    case 4: return variant_kernel<4>();
+    default: return variant_kernel<5>();
+  }
+}
+
+}  // namespace
+
+int calc_all_fp32_occupancy(int block)
+{
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_calc_all_fp32, block, 0);
+  return blocks;
+}
+
+int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
+                         const CalcAllArgs &a, int grid, int block, cudaStream_t s)
+{
+  SingleSrc S;
+  S.M64 = M64;
+  S.M = make_model32(M64, quad, cellsize32);
+  S.P.pos = a.pos;
+  S.P.vel = a.vel;
+  S.P.mass = a.mass;
+  S.P.tint = a.tint;
+  S.P.type = a.type;
+  S.P.order = a.order;
+  S.P.orbits = a.orbits;
+  S.n = a.n;
+  S.next = a.next;
+  S.fx = a.fx;
+  S.shift = a.shift;
+  S.steps_total = a.steps_total;
+  S.max_egy_err = a.max_egy_err;
+  S.status = a.status;
+  k_calc_all_fp32<<<grid, block, 0, s>>>(S);
   return 1;
+}
+
+int ensemble_variant_count() { return kNumVariants; }
+
+int ensemble_variant(int v, int *block, int *min_blocks)
+{
+  if(v < 0 || v >= kNumVariants) return 0;
+  *block = kVariants[v].block;
+  *min_blocks = kVariants[v].min_blocks;
+  return 1;
+}
+
+int ensemble_occupancy(int v)
+{
+  int blocks = 0;
+  if(v < 0 || v >= kNumVariants) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ensemble_kernel(v), kVariants[v].block, 0);
+  return blocks;
+}
+
+size_t ensemble_member_bytes() { return sizeof(EnsembleMember); }
+
+void ensemble_fill_member(void *dst, const DevModel &dm, const double *pos, const double *vel, const double *mass,
+                          const double *tint, const int *type, const int *order, int *orbits)
+{
+  EnsembleMember m;
+  m.dm = dm;
+  m.part.pos = pos;
+  m.part.vel = vel;
+  m.part.mass = mass;
+  m.part.tint = tint;
+  m.part.type = type;
+  m.part.order = order;
+  m.part.orbits = orbits;
+  std::memcpy(dst, &m, sizeof(m));
+}
+
+cudaError_t launch_ensemble_fp32(const EnsembleLaunch &L, int v, int grid, cudaStream_t s)
+{
+  if(L.nmodels < 1 || L.nmodels > GALIC_ENSEMBLE_MAX || v < 0 || v >= kNumVariants) return cudaErrorInvalidValue;
+  EnsembleSrc S;
+  S.nmodels = L.nmodels;
+  S.total = L.offset[L.nmodels];
+  for(int k = 0; k <= L.nmodels; k++) S.offset[k] = L.offset[k];
+  for(int k = L.nmodels + 1; k <= GALIC_ENSEMBLE_MAX; k++) S.offset[k] = S.total;
+  for(int k = 0; k < L.nmodels; k++) S.m[k] = make_model32(L.dm[k], L.quad[k], L.cellsize32[k]);
+  S.mem = (const EnsembleMember *) L.members;
+  S.next = L.next;
+  S.fx = L.fx;
+  S.shift = L.shift;
+  S.steps = L.steps;
+  S.maxerr = L.maxerr;
+  S.status = L.status;
+  void *args[] = {&S};
+  return cudaLaunchKernel(ensemble_kernel(v), dim3(grid), dim3(kVariants[v].block), args, 0, s);
 }

@@ -374,6 +374,19 @@ def fill_sample(comps, counts, rmax, seed=7):
     return np.concatenate(pos), np.concatenate(mass)
 
 
+def config_ensemble(count=64, seed=4, n_min=10000, n_max=1000000, level=6):
+    """Batched ensemble: `count` Hernquist halos (M = 100) with N log-uniform in
+    [n_min, n_max], scale a uniform in [10, 50] kpc and anisotropy beta uniform
+    in [-0.5, 0.5] (TypeOfHaloVelocityStructure 1), each with its own 64x64
+    response grid (DG level 6) and 256^2 force grid; all drawn from `seed`."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count)).astype(int)
+    a = rng.uniform(10.0, 50.0, count)
+    beta = rng.uniform(-0.5, 0.5, count)
+    return [build_model([Component("halo", 100.0, float(a[k]), int(n[k]), beta=float(beta[k]), tovs=1)],
+                        seed=seed * 1000 + k, level=level) for k in range(count)]
+
+
 def config_halo(n=100000, seed=1, level=6):
     """Plain method: Hernquist M=100, a=30 kpc, isotropic; 64x64 (R,|z|) response grid (DG level 6)
     from 0.01a to 100a; 256x256 force grid; TorbitFac 5, ~200 steps/orbit."""

@@ -208,6 +208,39 @@ int galic_orbit_responses_noalloc(const galic_params_t *prm, const double *d_fg_
                                   const double *d_tint, const int *d_type, double *d_out, int *d_orbits,
                                   void *stream);
 
+/* ------------------------------------------------------- ensembles */
+
+/* An ensemble advances up to 64 contexts (galaxy models of any particle
+ * counts, same device, same DG_MaxLevel) together: one iteration is
+ * calc_all_response_fields with its calc_global_fit (main.c:151-362) for
+ * every member in the FP32 form, run as ONE persistent orbit launch over the
+ * orbits of all members plus each member's read-out and merit kernels, and
+ * replayed from a CUDA graph after the first call.  Each member's results
+ * (galic_get_fit / galic_get_response / galic_get_particles on the member)
+ * are identical to what galic_calc_all_response_fields(member,
+ * GALIC_FORM_FP32) gives, whatever the other members and the tile variant.
+ * No counterpart in the reference (one model per MPI job).  Uploading to a
+ * member after galic_ensemble_create makes the ensemble return
+ * GALIC_ERR_STATE; build a new one.  The members must outlive the ensemble. */
+typedef struct galic_ensemble galic_ensemble;
+int galic_ensemble_create(galic_ctx *const *members, int count, galic_ensemble **out);
+void galic_ensemble_destroy(galic_ensemble *e);
+int galic_ensemble_last_status(const galic_ensemble *e);
+/* one iteration of every member */
+int galic_ensemble_calc_all(galic_ensemble *e);
+/* tile variants of the orbit kernel (threads per CTA, CTAs per SM asked of
+ * the register allocator); returns their count, fills up to max entries */
+int galic_ensemble_variants(int *block, int *min_blocks, int max);
+int galic_ensemble_set_variant(galic_ensemble *e, int variant);
+/* times every variant on the first sample_fraction of each member's orbits
+ * (ms_per_variant may be NULL) and selects the fastest; the members'
+ * responses must be recomputed afterwards */
+int galic_ensemble_autotune(galic_ensemble *e, double sample_fraction, int *best, double *ms_per_variant);
+/* device times of the last iteration (CUDA events in the graph), orbit-steps
+ * summed over the members, and the number of nodes of the graph */
+int galic_ensemble_last_timing(const galic_ensemble *e, double *ms_total, double *ms_orbit_kernel,
+                               long long *orbit_steps, int *graph_nodes);
+
 /* ------------------------------------------------------- force-grid fill */
 
 /* Parameters of the tree force-grid fill, from `All` and the grid globals. */

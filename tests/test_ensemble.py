@@ -1,0 +1,125 @@
+"""Ensembles: several models advanced by one persistent FP32 launch per
+iteration, replayed from a CUDA graph (galic_ensemble_*).
+
+A member's results after an ensemble iteration must equal what the member's
+own galic_calc_all_response_fields(GALIC_FORM_FP32) gives: the orbit kernel is
+the same code, the fixed-point response sums are exact and independent of the
+order of deposits, so neither the other members nor the tile variant may
+change a bit.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from galic_b200 import GALIC_FORM_FP32, Context, _ffi, synth
+from galic_b200.ensemble import Ensemble
+
+
+def snapshot(ctx):
+    grids = {(t, w): ctx.response(t, w) for t in (1,) for w in range(_ffi.GRID_COUNT)}
+    vel, orbits, vdisp = ctx.particles()
+    return ctx.fit().copy(), grids, orbits.copy(), vdisp.copy()
+
+
+def assert_same(a, b):
+    fa, ga, oa, va = a
+    fb, gb, ob, vb = b
+    assert np.array_equal(fa, fb)
+    for k in ga:
+        assert np.array_equal(ga[k], gb[k]), k
+    assert np.array_equal(oa, ob)
+    assert np.array_equal(va, vb)
+
+
+def test_variants_listed_without_device():
+    v = Ensemble.variants()
+    assert len(v) >= 4
+    for block, minb in v:
+        assert block % 32 == 0 and block * minb <= 2048
+
+
+def test_create_argument_errors():
+    lib = _ffi.load_library()
+    h = C.c_void_p()
+    assert lib.galic_ensemble_create(None, 1, C.byref(h)) == 1
+    arr = (C.c_void_p * 1)(None)
+    assert lib.galic_ensemble_create(arr, 0, C.byref(h)) == 1
+    assert lib.galic_ensemble_create(arr, 65, C.byref(h)) == 1
+    assert lib.galic_ensemble_create(arr, 1, C.byref(h)) in (1, 4)  # NULL member (or no device)
+
+
+@pytest.fixture(scope="module")
+def members():
+    models = synth.config_ensemble(count=4, seed=9, n_min=2000, n_max=20000, level=5)
+    ctxs = []
+    for m in models:
+        c = Context(m.params)
+        c.load_model(m)
+        ctxs.append(c)
+    yield models, ctxs
+    for c in ctxs:
+        c.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_members_match_single_runs(members):
+    models, ctxs = members
+    alone = []
+    for c in ctxs:
+        c.calc_all_response_fields(GALIC_FORM_FP32)
+        alone.append(snapshot(c))
+    steps_alone = [c.last_orbit_steps() for c in ctxs]
+    with Ensemble(ctxs) as e:
+        for it in range(2):  # the second iteration replays the graph
+            e.calc_all()
+            for c, ref in zip(ctxs, alone):
+                assert_same(snapshot(c), ref)
+        ms_total, ms_orbit, steps, nodes = e.last_timing()
+        assert steps == sum(steps_alone)
+        assert [c.last_orbit_steps() for c in ctxs] == steps_alone
+        assert nodes >= 4 + 5 * len(ctxs)
+        assert ms_total >= ms_orbit > 0
+
+
+@pytest.mark.gpu
+def test_ensemble_independent_of_variant_and_autotune(members):
+    models, ctxs = members
+    with Ensemble(ctxs) as e:
+        e.calc_all()
+        ref = [snapshot(c) for c in ctxs]
+        for v in range(len(Ensemble.variants())):
+            e.set_variant(v)
+            e.calc_all()
+            for c, r in zip(ctxs, ref):
+                assert_same(snapshot(c), r)
+        best, ms = e.autotune(0.1)
+        assert 0 <= best < len(ms) and np.all(ms > 0)
+        e.calc_all()
+        for c, r in zip(ctxs, ref):
+            assert_same(snapshot(c), r)
+
+
+@pytest.mark.gpu
+def test_ensemble_subset_order_independent(members):
+    """A member's result does not depend on which other members share the launch."""
+    models, ctxs = members
+    with Ensemble(ctxs[::-1]) as e:
+        e.calc_all()
+        ref = [snapshot(c) for c in ctxs]
+    with Ensemble([ctxs[1], ctxs[3]]) as e:
+        e.calc_all()
+        assert_same(snapshot(ctxs[1]), ref[1])
+        assert_same(snapshot(ctxs[3]), ref[3])
+
+
+@pytest.mark.gpu
+def test_ensemble_invalidated_by_upload(members):
+    models, ctxs = members
+    with Ensemble(ctxs) as e:
+        e.calc_all()
+        m = models[0]
+        ctxs[0].set_particles(m.pos, m.vel, m.mass, m.tint, m.vesc, m.ptype, m.ptargets)
+        with pytest.raises(Exception) as err:
+            e.calc_all()
+        assert getattr(err.value, "status", None) == 9
