@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's particle count")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ensemble-models", type=int, default=64, help="models of the batched ensemble (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving stream (0: skip)")
+    ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
+    ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
     return ap.parse_args()
 
 
@@ -204,6 +207,68 @@ def measure_ensemble(count, steps):
     for c in ctxs:
         c.close()
     return res
+
+
+def serving_requests(count, seed, scale):
+    """The serving stream's requests: 70% halo-only (N log-uniform in
+    [1e4, 1e6] x scale), 30% halo+disk+bulge (N log-uniform in [1e5, 2e6] x
+    scale, masses and scale lengths of the composite shape times a seeded
+    factor in [0.5, 2])."""
+    from galic_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    C_ = synth.Component
+    out = []
+    for k in range(count):
+        if rng.random() < 0.7:
+            n = int(np.exp(rng.uniform(np.log(1e4 * scale), np.log(1e6 * scale))))
+            m = synth.build_model([C_("halo", 100.0, float(rng.uniform(10, 50)), max(n, 200), tovs=0)],
+                                  seed=seed * 1000 + k, level=6)
+        else:
+            n = np.exp(rng.uniform(np.log(1e5 * scale), np.log(2e6 * scale)))
+            f = float(rng.uniform(0.5, 2.0))
+            nh, nd, nb = (max(int(n * w), 100) for w in (0.75, 0.175, 0.075))
+            m = synth.build_model([C_("halo", 93.5 * f, 30.0 * f, nh, beta=0.2, tovs=1),
+                                   C_("disk", 5.0 * f, 3.5 * f, nd, z0=0.7 * f, tovs=3),
+                                   C_("bulge", 1.5 * f, 1.0 * f, nb, tovs=0)], seed=seed * 1000 + k, level=6)
+        out.append(m)
+    return out
+
+
+def measure_serving(count, mean_gap, scale, torch):
+    """Poisson stream of model-construction jobs through the serving loop:
+    admission by HBM budget, concurrent jobs on one GPU, per-job
+    time-to-convergence (submit to done)."""
+    from galic_b200 import GALIC_FORM_FP32
+    from galic_b200.serving import Server
+
+    models = serving_requests(count, 5, scale)
+    rng = np.random.default_rng(6)
+    arrivals = np.cumsum(rng.exponential(mean_gap, count))
+    free, total = torch.cuda.mem_get_info()
+    budget = int(0.5 * free)
+    schedule = dict(form=GALIC_FORM_FP32, max_iterations=2, reps_per_iteration=5, fraction_per_rep=0.001)
+    with Server(budget, workers=8) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for k, m in enumerate(models):
+            dt = arrivals[k] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(m, seed=1000 + k, **schedule))
+        res = [srv.wait(i, timeout=1800) for i in ids]
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+    ok = [r for r in res if r["status"] == 0]
+    lat = np.array([r["t_done"] - r["t_submit"] for r in ok])
+    steps = sum(r["orbit_steps"] for r in ok)
+    return {"requests": count, "completed": len(ok), "mean_gap_s": mean_gap, "particles_scale": scale,
+            "n_range": [int(min(m.n for m in models)), int(max(m.n for m in models))],
+            "schedule": {"calc_all": "fp32", "iterations": 2, "reps_per_iteration": 5,
+                         "fraction_per_rep": 0.001, "reps": "fp64"},
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "makespan_s": makespan, "orbit_steps": int(steps), "orbit_steps_per_s": steps / makespan,
+            "hbm_budget_bytes": budget, "peak_bytes": st["peak_bytes"], "peak_concurrent_jobs": st["peak_running"]}
 
 
 def cpu_model():
@@ -434,6 +499,8 @@ def ours_arm(args, rank, world, local_rank):
         fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
+        serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch)
+                   if args.serve_requests > 0 else None)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
         if world == 1 and args.cpu_seconds > 0:
@@ -463,6 +530,7 @@ def ours_arm(args, rank, world, local_rank):
                 "cpu_baseline": cpu,
                 "force_grid_fill": fill,
                 "ensemble": ensemble,
+                "serving": serving,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,

@@ -71,6 +71,37 @@ class GalicFillStats(C.Structure):
                 ("tree_nodes", C.c_longlong), ("interactions", C.c_longlong), ("node_tests", C.c_longlong)]
 
 
+PD_ = C.POINTER(C.c_double)
+
+
+class GalicJob(C.Structure):
+    """galic_job_t: one model-construction job of the serving loop."""
+    _fields_ = [
+        ("prm", C.POINTER(GalicParams)),
+        ("fg_pot", PD_), ("fg_dpotdr", PD_), ("fg_dpotdz", PD_),
+        ("vstream", PD_ * 4),
+        ("cellsize", PD_), ("dgs_distance", PD_),
+        ("targets", (PD_ * 6) * 4),
+        ("n", C.c_int),
+        ("pos", PD_), ("vel", PD_), ("mass", PD_), ("tint", PD_), ("vesc", PD_), ("ptargets", PD_),
+        ("type", C.POINTER(C.c_int)),
+        ("form", C.c_int), ("max_iterations", C.c_int), ("reps_per_iteration", C.c_int),
+        ("fraction_per_rep", C.c_double), ("converge_rel", C.c_double),
+        ("seed", C.c_uint64),
+        ("permutation", C.POINTER(C.c_int)),
+        ("vel_out", PD_),
+    ]
+
+
+class GalicJobResult(C.Structure):
+    """galic_job_result_t."""
+    _fields_ = [
+        ("status", C.c_int), ("iterations", C.c_int), ("reps", C.c_longlong), ("orbit_steps", C.c_longlong),
+        ("sall_first", C.c_double), ("sall_last", C.c_double), ("fit", C.c_double * 28),
+        ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_first_response", C.c_double), ("t_done", C.c_double),
+    ]
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
@@ -131,6 +162,12 @@ SIGNATURES = [
     ("galic_ensemble_set_variant", C.c_int, [VP, C.c_int]),
     ("galic_ensemble_autotune", C.c_int, [VP, C.c_double, PI, PD]),
     ("galic_ensemble_last_timing", C.c_int, [VP, PD, PD, PLL, PI]),
+    ("galic_server_create", C.c_int, [C.c_size_t, C.c_int, C.POINTER(VP)]),
+    ("galic_server_submit", C.c_int, [VP, C.POINTER(GalicJob), PI]),
+    ("galic_server_wait", C.c_int, [VP, C.c_int, C.c_double, C.POINTER(GalicJobResult)]),
+    ("galic_server_stats", C.c_int, [VP, C.POINTER(C.c_size_t), PI, PI, PI]),
+    ("galic_server_destroy", None, [VP]),
+    ("galic_job_device_bytes", C.c_size_t, [C.POINTER(GalicJob)]),
     ("galic_force_grid_fill", C.c_int,
      [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, C.POINTER(GalicFillStats)]),
     ("galic_peano_hilbert_key", C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),

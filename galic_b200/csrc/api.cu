@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -46,17 +47,38 @@ int fail(galic_ctx *c, int st)
     }                                                                                             \
   } while(0)
 
+// Device memory of a context comes from the device's stream-ordered pool
+// and is allocated and released in the context's stream: a context that
+// starts or ends does not synchronise the device, so contexts driven from
+// different host threads (the serving loop) do not stall one another.
 template <class T>
-cudaError_t dalloc(T **p, size_t count)
+cudaError_t dalloc(galic_ctx *ctx, T **p, size_t count)
 {
-  return cudaMalloc((void **) p, std::max<size_t>(count, 1) * sizeof(T));
+  return cudaMallocAsync((void **) p, std::max<size_t>(count, 1) * sizeof(T), ctx->stream);
 }
 
 template <class T>
-void dfree(T *&p)
+void dfree(galic_ctx *ctx, T *&p)
 {
-  if(p) cudaFree((void *) p);
+  if(p) cudaFreeAsync((void *) p, ctx->stream);
   p = nullptr;
+}
+
+// keep freed pool memory mapped (the default pool would return it to the
+// driver at every synchronisation); process-local, once per device
+cudaError_t keep_pool_memory(int device)
+{
+  static std::mutex mu;
+  static bool done[256] = {false};
+  std::lock_guard<std::mutex> lk(mu);
+  if(device < 0 || device >= 256 || done[device]) return cudaSuccess;
+  cudaMemPool_t pool;
+  cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
+  if(e != cudaSuccess) return e;
+  uint64_t threshold = UINT64_MAX;
+  e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  if(e == cudaSuccess) done[device] = true;
+  return e;
 }
 
 int stack_size(int L) { return ((1 << (2 + 2 * L)) - 1) / 3; }
@@ -83,20 +105,20 @@ int check_params(const galic_params_t *p)
 int ensure_orbit_scratch(galic_ctx *ctx, int count)
 {
   if(count <= ctx->scratch_orbits) return GALIC_OK;
-  dfree(ctx->d_b_pos); dfree(ctx->d_b_vel); dfree(ctx->d_b_mass); dfree(ctx->d_b_time); dfree(ctx->d_grids);
-  dfree(ctx->d_b_tall); dfree(ctx->d_b_err); dfree(ctx->d_b_type); dfree(ctx->d_b_norbit); dfree(ctx->d_b_status);
-  dfree(ctx->d_b_steps);
-  CK(dalloc(&ctx->d_b_pos, 3 * (size_t) count));
-  CK(dalloc(&ctx->d_b_vel, 3 * (size_t) count));
-  CK(dalloc(&ctx->d_b_mass, count));
-  CK(dalloc(&ctx->d_b_time, count));
-  CK(dalloc(&ctx->d_grids, (size_t) count * NF_ORBIT * ctx->G));
-  CK(dalloc(&ctx->d_b_tall, count));
-  CK(dalloc(&ctx->d_b_err, count));
-  CK(dalloc(&ctx->d_b_type, count));
-  CK(dalloc(&ctx->d_b_norbit, count));
-  CK(dalloc(&ctx->d_b_status, count));
-  CK(dalloc(&ctx->d_b_steps, count));
+  dfree(ctx, ctx->d_b_pos); dfree(ctx, ctx->d_b_vel); dfree(ctx, ctx->d_b_mass); dfree(ctx, ctx->d_b_time); dfree(ctx, ctx->d_grids);
+  dfree(ctx, ctx->d_b_tall); dfree(ctx, ctx->d_b_err); dfree(ctx, ctx->d_b_type); dfree(ctx, ctx->d_b_norbit); dfree(ctx, ctx->d_b_status);
+  dfree(ctx, ctx->d_b_steps);
+  CK(dalloc(ctx, &ctx->d_b_pos, 3 * (size_t) count));
+  CK(dalloc(ctx, &ctx->d_b_vel, 3 * (size_t) count));
+  CK(dalloc(ctx, &ctx->d_b_mass, count));
+  CK(dalloc(ctx, &ctx->d_b_time, count));
+  CK(dalloc(ctx, &ctx->d_grids, (size_t) count * NF_ORBIT * ctx->G));
+  CK(dalloc(ctx, &ctx->d_b_tall, count));
+  CK(dalloc(ctx, &ctx->d_b_err, count));
+  CK(dalloc(ctx, &ctx->d_b_type, count));
+  CK(dalloc(ctx, &ctx->d_b_norbit, count));
+  CK(dalloc(ctx, &ctx->d_b_status, count));
+  CK(dalloc(ctx, &ctx->d_b_steps, count));
   ctx->scratch_orbits = count;
   return GALIC_OK;
 }
@@ -106,14 +128,14 @@ int ensure_rep_scratch(galic_ctx *ctx, int count)
   int st = ensure_orbit_scratch(ctx, 2 * count);
   if(st) return st;
   if(count <= ctx->scratch_rep) return GALIC_OK;
-  dfree(ctx->d_idx); dfree(ctx->d_accepted); dfree(ctx->d_vel_try); dfree(ctx->d_F); dfree(ctx->d_inst_v);
-  dfree(ctx->d_inst_cell);
-  CK(dalloc(&ctx->d_idx, count));
-  CK(dalloc(&ctx->d_accepted, count));
-  CK(dalloc(&ctx->d_vel_try, 3 * (size_t) count));
-  CK(dalloc(&ctx->d_F, 2 * (size_t) count));
-  CK(dalloc(&ctx->d_inst_v, 4 * (size_t) count));
-  CK(dalloc(&ctx->d_inst_cell, count));
+  dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
+  dfree(ctx, ctx->d_inst_cell);
+  CK(dalloc(ctx, &ctx->d_idx, count));
+  CK(dalloc(ctx, &ctx->d_accepted, count));
+  CK(dalloc(ctx, &ctx->d_vel_try, 3 * (size_t) count));
+  CK(dalloc(ctx, &ctx->d_F, 2 * (size_t) count));
+  CK(dalloc(ctx, &ctx->d_inst_v, 4 * (size_t) count));
+  CK(dalloc(ctx, &ctx->d_inst_cell, count));
   ctx->scratch_rep = count;
   return GALIC_OK;
 }
@@ -185,7 +207,7 @@ int ensure_tab32(galic_ctx *ctx)
   const int N = ctx->prm.FG_Nbin;
   std::vector<float4> tab(4 * (size_t) NF, make_float4(0.f, 0.f, 0.f, 0.f));
   for(int t = 1; t <= 3; t++) {
-    if(!ctx->d_tab32[t]) CK(dalloc(&ctx->d_tab32[t], 4 * (size_t) NF));
+    if(!ctx->d_tab32[t]) CK(dalloc(ctx, &ctx->d_tab32[t], 4 * (size_t) NF));
     const bool hv = ctx->h_vstream[t].size() == (size_t) NF;
     for(int iz = 0; iz + 1 < N; iz++)
       for(int iR = 0; iR + 1 < N; iR++) {
@@ -201,12 +223,12 @@ int ensure_tab32(galic_ctx *ctx)
         e[1] = make_float4(z[0], z[1], z[2], z[3]);
         e[2] = make_float4(v[0], v[1], v[2], v[3]);
       }
-    CK(cudaMemcpy(ctx->d_tab32[t], tab.data(), 4 * (size_t) NF * sizeof(float4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->d_tab32[t], tab.data(), 4 * (size_t) NF * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
   }
-  if(!ctx->d_cellsize32) CK(dalloc(&ctx->d_cellsize32, ctx->G));
+  if(!ctx->d_cellsize32) CK(dalloc(ctx, &ctx->d_cellsize32, ctx->G));
   std::vector<float> cs(ctx->G);
   for(int i = 0; i < ctx->G; i++) cs[i] = (float) ctx->h_cellsize[i];
-  CK(cudaMemcpy(ctx->d_cellsize32, cs.data(), ctx->G * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_cellsize32, cs.data(), ctx->G * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   ctx->tab32_dirty = false;
   return GALIC_OK;
 }
@@ -238,6 +260,7 @@ extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
   ctx = new galic_ctx();
   ctx->prm = *prm;
   cudaGetDevice(&ctx->device);
+  CK(keep_pool_memory(ctx->device));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for(int k = 0; k < 3; k++) CK(cudaEventCreate(&ctx->ev[k]));
   CK(prepare_fit_kernels());
@@ -245,32 +268,32 @@ extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
   ctx->G = 1 << (2 * ctx->L);
   ctx->Ns = stack_size(ctx->L);
   const int NF = prm->FG_Nbin * prm->FG_Nbin;
-  CK(dalloc(&ctx->d_fg_acc, NF));
-  CK(dalloc(&ctx->d_fg_pot, NF));
+  CK(dalloc(ctx, &ctx->d_fg_acc, NF));
+  CK(dalloc(ctx, &ctx->d_fg_pot, NF));
   for(int t = 1; t <= 3; t++) {
-    CK(dalloc(&ctx->d_vstream[t], NF));
-    CK(cudaMemset(ctx->d_vstream[t], 0, NF * sizeof(double)));
+    CK(dalloc(ctx, &ctx->d_vstream[t], NF));
+    CK(cudaMemsetAsync(ctx->d_vstream[t], 0, NF * sizeof(double), ctx->stream));
   }
-  CK(cudaMemset(ctx->d_fg_acc, 0, NF * sizeof(double2)));
-  CK(cudaMemset(ctx->d_fg_pot, 0, NF * sizeof(double)));
-  CK(dalloc(&ctx->d_cellsize, ctx->G));
-  CK(dalloc(&ctx->d_dist, ctx->Ns));
-  CK(dalloc(&ctx->d_targets, (size_t) 4 * NT_TARGET * ctx->Ns));
-  CK(cudaMemset(ctx->d_targets, 0, (size_t) 4 * NT_TARGET * ctx->Ns * sizeof(double)));
-  CK(dalloc(&ctx->d_committed, (size_t) 4 * NG_COMMITTED * ctx->G));
-  CK(cudaMemset(ctx->d_committed, 0, (size_t) 4 * NG_COMMITTED * ctx->G * sizeof(double)));
-  CK(dalloc(&ctx->d_stacks, (size_t) 4 * NG_COMMITTED * ctx->Ns));
-  CK(dalloc(&ctx->d_fx, (size_t) 4 * NG_COMMITTED * ctx->G));
-  CK(dalloc(&ctx->d_shift, 4 * NG_COMMITTED));
-  CK(dalloc(&ctx->d_fit, 4 * 7 + 4 * 5));
-  CK(cudaMemset(ctx->d_fit, 0, (4 * 7 + 4 * 5) * sizeof(double)));
-  CK(dalloc(&ctx->d_firstrun, 4));
-  CK(cudaMemset(ctx->d_firstrun, 0, 4 * sizeof(int)));
-  CK(dalloc(&ctx->d_counters, 9));
-  CK(cudaMemset(ctx->d_counters, 0, 9 * sizeof(unsigned long long)));
-  CK(dalloc(&ctx->d_status, 1));
-  CK(dalloc(&ctx->d_next, 1));
-  CK(dalloc(&ctx->d_maxerr, 1));
+  CK(cudaMemsetAsync(ctx->d_fg_acc, 0, NF * sizeof(double2), ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_fg_pot, 0, NF * sizeof(double), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_cellsize, ctx->G));
+  CK(dalloc(ctx, &ctx->d_dist, ctx->Ns));
+  CK(dalloc(ctx, &ctx->d_targets, (size_t) 4 * NT_TARGET * ctx->Ns));
+  CK(cudaMemsetAsync(ctx->d_targets, 0, (size_t) 4 * NT_TARGET * ctx->Ns * sizeof(double), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_committed, (size_t) 4 * NG_COMMITTED * ctx->G));
+  CK(cudaMemsetAsync(ctx->d_committed, 0, (size_t) 4 * NG_COMMITTED * ctx->G * sizeof(double), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_stacks, (size_t) 4 * NG_COMMITTED * ctx->Ns));
+  CK(dalloc(ctx, &ctx->d_fx, (size_t) 4 * NG_COMMITTED * ctx->G));
+  CK(dalloc(ctx, &ctx->d_shift, 4 * NG_COMMITTED));
+  CK(dalloc(ctx, &ctx->d_fit, 4 * 7 + 4 * 5));
+  CK(cudaMemsetAsync(ctx->d_fit, 0, (4 * 7 + 4 * 5) * sizeof(double), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_firstrun, 4));
+  CK(cudaMemsetAsync(ctx->d_firstrun, 0, 4 * sizeof(int), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_counters, 9));
+  CK(cudaMemsetAsync(ctx->d_counters, 0, 9 * sizeof(unsigned long long), ctx->stream));
+  CK(dalloc(ctx, &ctx->d_status, 1));
+  CK(dalloc(ctx, &ctx->d_next, 1));
+  CK(dalloc(ctx, &ctx->d_maxerr, 1));
 
   DevModel &M = ctx->dm;
   M.V200 = prm->V200;
@@ -320,20 +343,20 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
 {
   if(!ctx) return;
   cudaStreamSynchronize(ctx->stream);
-  dfree(ctx->d_fg_acc); dfree(ctx->d_fg_pot);
-  for(int t = 0; t < 4; t++) dfree(ctx->d_vstream[t]);
-  dfree(ctx->d_cellsize); dfree(ctx->d_dist); dfree(ctx->d_targets); dfree(ctx->d_committed); dfree(ctx->d_stacks);
-  dfree(ctx->d_fx); dfree(ctx->d_shift); dfree(ctx->d_fit); dfree(ctx->d_firstrun); dfree(ctx->d_counters);
-  dfree(ctx->d_status); dfree(ctx->d_next); dfree(ctx->d_maxerr);
-  dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
-  dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits); dfree(ctx->d_order);
-  dfree(ctx->d_b_pos); dfree(ctx->d_b_vel); dfree(ctx->d_b_mass); dfree(ctx->d_b_time); dfree(ctx->d_grids);
-  dfree(ctx->d_b_tall); dfree(ctx->d_b_err); dfree(ctx->d_b_type); dfree(ctx->d_b_norbit); dfree(ctx->d_b_status);
-  dfree(ctx->d_b_steps);
-  dfree(ctx->d_idx); dfree(ctx->d_accepted); dfree(ctx->d_vel_try); dfree(ctx->d_F); dfree(ctx->d_inst_v);
-  dfree(ctx->d_inst_cell);
-  for(int t = 0; t < 4; t++) dfree(ctx->d_tab32[t]);
-  dfree(ctx->d_cellsize32);
+  dfree(ctx, ctx->d_fg_acc); dfree(ctx, ctx->d_fg_pot);
+  for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_vstream[t]);
+  dfree(ctx, ctx->d_cellsize); dfree(ctx, ctx->d_dist); dfree(ctx, ctx->d_targets); dfree(ctx, ctx->d_committed); dfree(ctx, ctx->d_stacks);
+  dfree(ctx, ctx->d_fx); dfree(ctx, ctx->d_shift); dfree(ctx, ctx->d_fit); dfree(ctx, ctx->d_firstrun); dfree(ctx, ctx->d_counters);
+  dfree(ctx, ctx->d_status); dfree(ctx, ctx->d_next); dfree(ctx, ctx->d_maxerr);
+  dfree(ctx, ctx->d_pos); dfree(ctx, ctx->d_vel); dfree(ctx, ctx->d_mass); dfree(ctx, ctx->d_tint); dfree(ctx, ctx->d_vesc);
+  dfree(ctx, ctx->d_ptargets); dfree(ctx, ctx->d_vdisp); dfree(ctx, ctx->d_type); dfree(ctx, ctx->d_orbits); dfree(ctx, ctx->d_order);
+  dfree(ctx, ctx->d_b_pos); dfree(ctx, ctx->d_b_vel); dfree(ctx, ctx->d_b_mass); dfree(ctx, ctx->d_b_time); dfree(ctx, ctx->d_grids);
+  dfree(ctx, ctx->d_b_tall); dfree(ctx, ctx->d_b_err); dfree(ctx, ctx->d_b_type); dfree(ctx, ctx->d_b_norbit); dfree(ctx, ctx->d_b_status);
+  dfree(ctx, ctx->d_b_steps);
+  dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
+  dfree(ctx, ctx->d_inst_cell);
+  for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_tab32[t]);
+  dfree(ctx, ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
     if(ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
   if(ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -355,9 +378,10 @@ extern "C" int galic_set_force_grid(galic_ctx *ctx, const double *pot, const dou
   ctx->h_dpotdr.assign(dpotdr, dpotdr + NF);
   ctx->h_dpotdz.assign(dpotdz, dpotdz + NF);
   ctx->tab32_dirty = true;
-  CK(cudaMemcpy(ctx->d_fg_acc, acc.data(), NF * sizeof(double2), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_fg_pot, pot, NF * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_fg_acc, acc.data(), NF * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_fg_pot, pot, NF * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   ctx->have_fg = true;
+  CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
 
@@ -375,7 +399,8 @@ extern "C" int galic_set_vstream(galic_ctx *ctx, int type, const double *v)
   ctx->dm.vstream_zero[type] = zero;
   ctx->h_vstream[type].assign(v, v + NF);
   ctx->tab32_dirty = true;
-  CK(cudaMemcpy(ctx->d_vstream[type], v, NF * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_vstream[type], v, NF * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
 
@@ -383,11 +408,12 @@ extern "C" int galic_set_density_geometry(galic_ctx *ctx, const double *cellsize
 {
   if(!ctx || !cellsize || !dist) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   ctx->generation++;
-  CK(cudaMemcpy(ctx->d_cellsize, cellsize, ctx->G * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_cellsize, cellsize, ctx->G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   ctx->h_cellsize.assign(cellsize, cellsize + ctx->G);
   ctx->tab32_dirty = true;
-  CK(cudaMemcpy(ctx->d_dist, dist, ctx->Ns * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_dist, dist, ctx->Ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   ctx->have_geom = true;
+  CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
 
@@ -399,9 +425,10 @@ extern "C" int galic_set_targets(galic_ctx *ctx, int type, const double *dgs_mas
   ctx->generation++;
   const double *src[NT_TARGET] = {dgs_mass, egs_mass, egs_r, egs_t, egs_p, egs_q};
   for(int k = 0; k < NT_TARGET; k++)
-    CK(cudaMemcpy(ctx->d_targets + ((size_t) type * NT_TARGET + k) * ctx->Ns, src[k], ctx->Ns * sizeof(double),
-                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->d_targets + ((size_t) type * NT_TARGET + k) * ctx->Ns, src[k], ctx->Ns * sizeof(double),
+                  cudaMemcpyHostToDevice, ctx->stream));
   ctx->have_targets[type] = true;
+  CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
 
@@ -414,28 +441,28 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
     if(type[i] < 1 || type[i] > 3 || !(tint[i] > 0)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   ctx->generation++;
   if(n != ctx->n) {
-    dfree(ctx->d_pos); dfree(ctx->d_vel); dfree(ctx->d_mass); dfree(ctx->d_tint); dfree(ctx->d_vesc);
-    dfree(ctx->d_ptargets); dfree(ctx->d_vdisp); dfree(ctx->d_type); dfree(ctx->d_orbits); dfree(ctx->d_order);
-    CK(dalloc(&ctx->d_order, n));
-    CK(dalloc(&ctx->d_pos, 3 * (size_t) n));
-    CK(dalloc(&ctx->d_vel, 3 * (size_t) n));
-    CK(dalloc(&ctx->d_mass, n));
-    CK(dalloc(&ctx->d_tint, n));
-    CK(dalloc(&ctx->d_vesc, n));
-    CK(dalloc(&ctx->d_ptargets, 4 * (size_t) n));
-    CK(dalloc(&ctx->d_vdisp, 4 * (size_t) n));
-    CK(dalloc(&ctx->d_type, n));
-    CK(dalloc(&ctx->d_orbits, n));
+    dfree(ctx, ctx->d_pos); dfree(ctx, ctx->d_vel); dfree(ctx, ctx->d_mass); dfree(ctx, ctx->d_tint); dfree(ctx, ctx->d_vesc);
+    dfree(ctx, ctx->d_ptargets); dfree(ctx, ctx->d_vdisp); dfree(ctx, ctx->d_type); dfree(ctx, ctx->d_orbits); dfree(ctx, ctx->d_order);
+    CK(dalloc(ctx, &ctx->d_order, n));
+    CK(dalloc(ctx, &ctx->d_pos, 3 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_vel, 3 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_mass, n));
+    CK(dalloc(ctx, &ctx->d_tint, n));
+    CK(dalloc(ctx, &ctx->d_vesc, n));
+    CK(dalloc(ctx, &ctx->d_ptargets, 4 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_vdisp, 4 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_type, n));
+    CK(dalloc(ctx, &ctx->d_orbits, n));
     ctx->n = n;
   }
-  CK(cudaMemcpy(ctx->d_pos, pos, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_vel, vel, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_mass, mass, n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_tint, tint, n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_vesc, vesc, n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice));
-  CK(cudaMemset(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double)));
+  CK(cudaMemcpyAsync(ctx->d_pos, pos, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_vel, vel, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_mass, mass, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_tint, tint, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_vesc, vesc, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double), ctx->stream));
   {
     // neighbouring lanes then integrate orbits that start at similar radii and
     // read nearby force-grid cells; results do not depend on the order
@@ -446,10 +473,11 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
       order[i] = i;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return r2[a] < r2[b]; });
-    CK(cudaMemcpy(ctx->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   }
-  CK(cudaMemset(ctx->d_orbits, 0, n * sizeof(int)));
+  CK(cudaMemsetAsync(ctx->d_orbits, 0, n * sizeof(int), ctx->stream));
   ctx->have_response = false;
+  CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
 
@@ -457,9 +485,9 @@ extern "C" int galic_get_particles(galic_ctx *ctx, double *vel, int *orbits, dou
 {
   if(!ctx || ctx->n == 0) return fail(ctx, GALIC_ERR_STATE);
   CK(cudaStreamSynchronize(ctx->stream));
-  if(vel) CK(cudaMemcpy(vel, ctx->d_vel, 3 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
-  if(orbits) CK(cudaMemcpy(orbits, ctx->d_orbits, ctx->n * sizeof(int), cudaMemcpyDeviceToHost));
-  if(vdisp) CK(cudaMemcpy(vdisp, ctx->d_vdisp, 4 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+  if(vel) CK(cudaMemcpyAsync(vel, ctx->d_vel, 3 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if(orbits) CK(cudaMemcpyAsync(orbits, ctx->d_orbits, ctx->n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if(vdisp) CK(cudaMemcpyAsync(vdisp, ctx->d_vdisp, 4 * (size_t) ctx->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   return fail(ctx, GALIC_OK);
 }
 
@@ -640,8 +668,11 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
 {
   if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
   if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
-  if(form == GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_UNSUPPORTED);
   if(!ctx->have_response) return fail(ctx, GALIC_ERR_STATE);
+  if(form == GALIC_FORM_FP32) {
+    int st = ensure_tab32(ctx);
+    if(st) return st;
+  }
   if(count < 0 || (count > 0 && !idx)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   // every particle at most once per repetition: the reference evaluates a
   // repetition against committed state and P[n] only changes for n itself
@@ -711,7 +742,8 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
   b.egy_err = ctx->d_b_err;
   b.status = ctx->d_b_status;
   b.with_egy = 1;
-  ctx->last_launches = launch_rep(ctx->dm, R, f, b, s);
+  ctx->last_launches = form == GALIC_FORM_FP32 ? launch_rep(ctx->dm, R, f, b, s, ctx->d_tab32, ctx->d_cellsize32)
+                                               : launch_rep(ctx->dm, R, f, b, s);
   int status = 0;
   std::vector<int> ost(2 * count);
   std::vector<long long> steps(2 * count);
@@ -735,7 +767,7 @@ extern "C" int galic_get_fit(galic_ctx *ctx, double *out)
 {
   if(!ctx || !out) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(out, ctx->d_fit, 4 * 7 * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(out, ctx->d_fit, 4 * 7 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   return fail(ctx, GALIC_OK);
 }
 
@@ -744,7 +776,7 @@ extern "C" int galic_get_counters(galic_ctx *ctx, long long *tries, long long *c
   if(!ctx || !tries || !changes) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   unsigned long long c[8];
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
   for(int t = 0; t < 4; t++) {
     tries[t] = (long long) c[t];
     changes[t] = (long long) c[4 + t];
@@ -757,8 +789,8 @@ extern "C" int galic_get_response(galic_ctx *ctx, int type, int which, double *o
   if(!ctx || !out || type < 1 || type > 3 || which < 0 || which >= GALIC_GRID_COUNT)
     return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(out, ctx->d_committed + ((size_t) type * NG_COMMITTED + which) * ctx->G, ctx->G * sizeof(double),
-                cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(out, ctx->d_committed + ((size_t) type * NG_COMMITTED + which) * ctx->G, ctx->G * sizeof(double),
+                cudaMemcpyDeviceToHost, ctx->stream));
   return fail(ctx, GALIC_OK);
 }
 

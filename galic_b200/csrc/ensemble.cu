@@ -290,6 +290,7 @@ extern "C" int galic_ensemble_calc_all(galic_ensemble *e)
     if(st) return st;
   }
   cudaStream_t s = e->stream;
+  for(galic_ctx *c : e->members) ECK(cudaStreamSynchronize(c->stream));  // members' own work first
   ECK(cudaGraphLaunch(e->exec, s));
   ECK(cudaMemcpyAsync(e->h_steps, e->d_steps, e->nmodels * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   ECK(cudaMemcpyAsync(e->h_maxerr, e->d_maxerr, e->nmodels * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -332,6 +333,7 @@ extern "C" int galic_ensemble_autotune(galic_ensemble *e, double sample_fraction
   }
   const int nv = ensemble_variant_count();
   cudaStream_t s = e->stream;
+  for(galic_ctx *c : e->members) ECK(cudaStreamSynchronize(c->stream));
   double best_ms = 1e300;
   int best_v = 0;
   for(int v = 0; v < nv; v++) {

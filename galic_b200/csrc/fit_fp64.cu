@@ -13,6 +13,8 @@
 //                 (main.c:488-498) and its commit (main.c:830-835).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "galic_gpu.h"
 #include "grng.h"
 #include "kernels.cuh"
@@ -325,12 +327,21 @@ __global__ void k_inst_delta(RepArgs R, FitArgs f)
 
 // the stack kernels keep a whole level-7 stack (171 KiB) in shared memory;
 // called once per context, on the context's device
+// the shared-memory opt-in of the stack kernels, once per device
 cudaError_t prepare_fit_kernels()
 {
-  cudaError_t e;
+  static std::mutex mu;
+  static bool done[256] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if(dev >= 0 && dev < 256 && done[dev]) return cudaSuccess;
   if((e = cudaFuncSetAttribute(k_fit_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if((e = cudaFuncSetAttribute(k_fit_diff, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
-  return cudaFuncSetAttribute(k_eval_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if((e = cudaFuncSetAttribute(k_eval_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  if(dev >= 0 && dev < 256) done[dev] = true;
+  return cudaSuccess;
 }
 
 int launch_global_fit(const FitArgs &f, cudaStream_t s)
@@ -343,14 +354,18 @@ int launch_global_fit(const FitArgs &f, cudaStream_t s)
   return 3;
 }
 
-int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s)
+int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s,
+               const float4 *const *quad32, const float *cellsize32)
 {
   int launches = 0;
   const int count = R.count;
   k_propose<<<(count + 63) / 64, 64, 0, s>>>(M, R);
   launches++;
   cudaMemsetAsync(b.grids, 0, (size_t) b.count * NF_ORBIT * M.DG_Ngrid * sizeof(double), s);
-  launch_orbits_dense(M, b, s);
+  if(quad32)
+    launch_orbits_dense_fp32(M, quad32, cellsize32, b, s);
+  else
+    launch_orbits_dense(M, b, s);
   launch_scale_dense(M, b, s);
   launches += 2;
   size_t smem = (size_t) f.Nstack * sizeof(double);

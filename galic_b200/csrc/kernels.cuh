@@ -69,6 +69,9 @@ struct FitArgs {
 };
 
 void launch_orbits_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s);
+// the same orbits in the FP32 form (orbit_fp32.cu), with egy fields
+void launch_orbits_dense_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
+                              const OrbitBatch &b, cudaStream_t s);
 void launch_scale_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s);
 int launch_calc_all_fp64(const DevModel &M, const CalcAllArgs &a, int grid, int block, cudaStream_t s);
 void launch_instantaneous(const DevModel &M, int n, const double *pos, const double *vel, const double *mass,

@@ -258,6 +258,88 @@ struct State32 {
 
 enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
 
+// orbit_response.c:172-206 in FP32: initial state of one orbit
+__device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const double *xd, const double *vd,
+                                             int type, double timespan)
+{
+  for(int i = 0; i < 3; i++) {
+    s.x[i] = (float) xd[i];
+    s.v[i] = (float) vd[i];
+  }
+  s.type = type;
+  s.tovs = M.tovs[type];
+  s.tall = 0;
+  s.timespan = timespan;
+  s.radsign_prev = 0.f;
+  s.norbit = 0;
+  s.flag = 0;
+  s.steps = 0;
+  s.status = ORBIT_OK;
+  float vstr;
+  accel32(M, type, s.x, s.a, &vstr);
+  Cell32 c = density_cell32(M, s.x);
+  s.iR = c.iR;
+  s.iz = c.iz;
+  s.fR = c.fR;
+  s.fz = c.fz;
+  s.proj = project32(s.tovs, s.x, s.v, vstr);
+  s.cs_cell = -1;
+}
+
+// one KDK step with its two deposits (orbit_response.c:211-458) in FP32;
+// false once the orbit has ended (time span reached, step cap, non-finite)
+template <class Sink>
+__device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink &sink)
+{
+  // get_timestep (orbit_response.c:16-26)
+  const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
+  const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
+  const float t1 = M.f_orb * M.V200 * frcp(aa);
+  const int dgc = s.iz * M.DG_Nbin + s.iR;
+  if(dgc != s.cs_cell) {
+    s.cs_cell = dgc;
+    s.cs_val = __ldg(&M.cellsize[dgc]);
+  }
+  const float t2 = M.f_cc * s.cs_val * frcp(vv);
+  double dt = (double) fminf(t1, t2);
+  if(s.timespan < dt + s.tall) {
+    dt = s.timespan - s.tall;
+    s.flag = 1;
+  }
+  const float hdt = 0.5f * (float) dt;
+  const float fdt = (float) dt;
+  sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+#pragma unroll
+  for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+#pragma unroll
+  for(int i = 0; i < 3; i++) s.x[i] = fmaf(fdt, s.v[i], s.x[i]);
+  float vstr;
+  accel32(M, s.type, s.x, s.a, &vstr);
+#pragma unroll
+  for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+  Cell32 c = density_cell32(M, s.x);
+  s.iR = c.iR;
+  s.iz = c.iz;
+  s.fR = c.fR;
+  s.fz = c.fz;
+  s.proj = project32(s.tovs, s.x, s.v, vstr);
+  sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+  s.tall += dt;
+  const float radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];
+  if(radsign > 0.f && s.radsign_prev < 0.f) s.norbit++;
+  s.radsign_prev = radsign;
+  s.steps++;
+  if(!(s.tall == s.tall)) {
+    s.status = ORBIT_NONFINITE;
+    return false;
+  }
+  if(s.steps > M.step_cap) {
+    s.status = ORBIT_STEP_CAP;
+    return false;
+  }
+  return !s.flag;
+}
+
 // Particle arrays of one model
 struct Particles32 {
   const double *pos, *vel, *mass, *tint;
@@ -397,27 +479,8 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
     for(int i = 0; i < 3; i++) {
       xd[i] = P.pos[3 * p + i];
       vd[i] = P.vel[3 * p + i];
-      s.x[i] = (float) xd[i];
-      s.v[i] = (float) vd[i];
     }
-    s.type = type;
-    s.tovs = M.tovs[type];
-    s.tall = 0;
-    s.timespan = P.tint[p];
-    s.radsign_prev = 0.f;
-    s.norbit = 0;
-    s.flag = 0;
-    s.steps = 0;
-    s.status = ORBIT_OK;
-    float vstr;
-    accel32(M, type, s.x, s.a, &vstr);
-    Cell32 c = density_cell32(M, s.x);
-    s.iR = c.iR;
-    s.iz = c.iz;
-    s.fR = c.fR;
-    s.fz = c.fz;
-    s.proj = project32(s.tovs, s.x, s.v, vstr);
-    s.cs_cell = -1;
+    orbit32_init(M, s, xd, vd, type, P.tint[p]);
     const DevModel &M64 = S.model64(mi);
     s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, pot_logs(M64), xd);
     return true;
@@ -432,53 +495,7 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
     if(state == LANE_ACTIVE) {
-      const Model32 &M = S.model(mi);
-      // get_timestep (orbit_response.c:16-26)
-      const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
-      const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
-      const float t1 = M.f_orb * M.V200 * frcp(aa);
-      const int dgc = s.iz * M.DG_Nbin + s.iR;
-      if(dgc != s.cs_cell) {
-        s.cs_cell = dgc;
-        s.cs_val = __ldg(&M.cellsize[dgc]);
-      }
-      const float t2 = M.f_cc * s.cs_val * frcp(vv);
-      double dt = (double) fminf(t1, t2);
-      if(s.timespan < dt + s.tall) {
-        dt = s.timespan - s.tall;
-        s.flag = 1;
-      }
-      const float hdt = 0.5f * (float) dt;
-      const float fdt = (float) dt;
-      sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
-#pragma unroll
-      for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
-#pragma unroll
-      for(int i = 0; i < 3; i++) s.x[i] = fmaf(fdt, s.v[i], s.x[i]);
-      float vstr;
-      accel32(M, s.type, s.x, s.a, &vstr);
-#pragma unroll
-      for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
-      Cell32 c = density_cell32(M, s.x);
-      s.iR = c.iR;
-      s.iz = c.iz;
-      s.fR = c.fR;
-      s.fz = c.fz;
-      s.proj = project32(s.tovs, s.x, s.v, vstr);
-      sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
-      s.tall += dt;
-      const float radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];
-      if(radsign > 0.f && s.radsign_prev < 0.f) s.norbit++;
-      s.radsign_prev = radsign;
-      s.steps++;
-      if(!(s.tall == s.tall)) {
-        s.status = ORBIT_NONFINITE;
-        state = LANE_FINISH;
-      } else if(s.steps > M.step_cap) {
-        s.status = ORBIT_STEP_CAP;
-        state = LANE_FINISH;
-      } else if(s.flag)
-        state = LANE_FINISH;
+      if(!orbit32_step(S.model(mi), s, sink)) state = LANE_FINISH;
     } else if(state == LANE_FINISH) {
       sink.park();
       S.particles(mi).orbits[p] = s.norbit;
@@ -509,6 +526,117 @@ template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_ensemble_fp32(const __grid_constant__ EnsembleSrc S)
 {
   calc_all_fp32_body<BLOCK>(S);
+}
+
+// Dense sink of one orbit: FP32 sums per corner of the current DG cell in
+// registers, added into the orbit's own FP64 grids [5][Ngrid] when the orbit
+// leaves the cell (corners shared with the next cell keep their sums).
+struct DenseSink32 {
+  double *grid;
+  int G, Nb;
+  int cur = -1, cur_iR = 0, cur_iz = 0;
+  float a[4][5];
+  __device__ __forceinline__ void flush_masked(const bool keep[4])
+  {
+#pragma unroll
+    for(int c = 0; c < 4; c++) {
+      if(keep[c]) continue;
+      const int off = cur + (c & 1) + ((c >> 1) ? Nb : 0);
+#pragma unroll
+      for(int f = 0; f < 5; f++)
+        if(a[c][f] != 0.f) grid[(size_t) f * G + off] += (double) a[c][f];
+    }
+  }
+  __device__ __forceinline__ void flush()
+  {
+    if(cur < 0) return;
+    const bool none[4] = {false, false, false, false};
+    flush_masked(none);
+    cur = -1;
+  }
+  __device__ __forceinline__ void move_to(int iR, int iz)
+  {
+    const int dz = iz - cur_iz, dR = iR - cur_iR;
+    if(cur >= 0 && dz >= -1 && dz <= 1 && dR >= -1 && dR <= 1) {
+      bool keep[4] = {false, false, false, false};
+      float na[4][5];
+#pragma unroll
+      for(int j = 0; j < 4; j++) {
+#pragma unroll
+        for(int f = 0; f < 5; f++) na[j][f] = 0.f;
+#pragma unroll
+        for(int k = 0; k < 4; k++) {
+          const bool same = ((k >> 1) == (j >> 1) + dz) && ((k & 1) == (j & 1) + dR);
+          keep[k] = keep[k] || same;
+#pragma unroll
+          for(int f = 0; f < 5; f++) na[j][f] = same ? a[k][f] : na[j][f];
+        }
+      }
+      flush_masked(keep);
+#pragma unroll
+      for(int j = 0; j < 4; j++)
+#pragma unroll
+        for(int f = 0; f < 5; f++) a[j][f] = na[j][f];
+    } else {
+      flush();
+#pragma unroll
+      for(int k = 0; k < 4; k++)
+#pragma unroll
+        for(int f = 0; f < 5; f++) a[k][f] = 0.f;
+    }
+    cur = iz * Nb + iR;
+    cur_iR = iR;
+    cur_iz = iz;
+  }
+  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
+  {
+    if(iz * Nb + iR != cur) move_to(iR, iz);
+    const float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
+#pragma unroll
+    for(int k = 0; k < 4; k++) {
+      a[k][0] += w[k];
+      a[k][1] = fmaf(w[k], p.vr2, a[k][1]);
+      a[k][2] = fmaf(w[k], p.vt2, a[k][2]);
+      a[k][3] = fmaf(w[k], p.vq2, a[k][3]);
+      a[k][4] = fmaf(w[k], p.vp2, a[k][4]);
+    }
+  }
+};
+
+// produce_orbit_response_field_mod (orbit_response.c:155-491) in the FP32
+// form, one thread per orbit, into dense per-orbit FP64 grids (unscaled; the
+// mass/tall normalisation follows in k_scale_dense)
+__global__ void __launch_bounds__(128) k_orbits_dense_fp32(const __grid_constant__ Model32 M,
+                                                          const __grid_constant__ DevModel M64, OrbitBatch b)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= b.count) return;
+  const int G = M64.DG_Ngrid;
+  DenseSink32 sink;
+  sink.grid = b.grids + (size_t) k * NF_ORBIT * G;
+  sink.G = G;
+  sink.Nb = M.DG_Nbin;
+  State32 s;
+  const double *xd = &b.pos[3 * k], *vd = &b.vel[3 * k];
+  orbit32_init(M, s, xd, vd, b.type[k], b.timespan[k]);
+  const LogConsts L = pot_logs(M64);
+  double x0[3] = {xd[0], xd[1], xd[2]};
+  const double E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, L, x0);
+  while(orbit32_step(M, s, sink)) {
+  }
+  sink.flush();
+  b.tall[k] = s.tall;
+  b.norbit[k] = s.norbit;
+  b.steps[k] = s.steps;
+  b.status[k] = s.status;
+  double err = -1.0;
+  if(s.status == ORBIT_OK) {
+    double x1[3] = {s.x[0], s.x[1], s.x[2]};
+    const double v0 = s.v[0], v1 = s.v[1], v2 = s.v[2];
+    const double E1 = 0.5 * (v0 * v0 + v1 * v1 + v2 * v2) + forcegrid_pot(M64, L, x1);
+    err = fabs((E1 - E0) / E0);
+  }
+  b.egy_err[k] = err;
 }
 
 Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32)
@@ -601,6 +729,14 @@ int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const
   S.status = a.status;
   k_calc_all_fp32<<<grid, block, 0, s>>>(S);
   return 1;
+}
+
+void launch_orbits_dense_fp32(const DevModel &M64, const float4 *const quad[4], const float *cellsize32,
+                              const OrbitBatch &b, cudaStream_t s)
+{
+  if(b.count <= 0) return;
+  const Model32 M = make_model32(M64, quad, cellsize32);
+  k_orbits_dense_fp32<<<(b.count + 127) / 128, 128, 0, s>>>(M, M64, b);
 }
 
 int ensemble_variant_count() { return kNumVariants; }

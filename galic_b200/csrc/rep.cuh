@@ -32,6 +32,8 @@ struct RepArgs {
   int *status;
 };
 
-int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s);
+// quad32/cellsize32 non-null: the orbits of the repetition in the FP32 form
+int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s,
+               const float4 *const *quad32 = nullptr, const float *cellsize32 = nullptr);
 
 #endif

@@ -144,7 +144,10 @@ int galic_calc_all_response_fields(galic_ctx *ctx, int form);
  * (main.c:808-841), which ends in calc_global_fit.  Proposals for idx[k] are
  * drawn from Philox stream (seed, idx[k], rep_serial).  All count
  * particles are evaluated against the committed state, as in the reference
- * (accepted changes only reach `_delta` grids until the commit). */
+ * (accepted changes only reach `_delta` grids until the commit).  form:
+ * GALIC_FORM_FP64 integrates the old and trial orbits bit-exactly as the
+ * CPU restatement; GALIC_FORM_FP32 integrates them in the FP32 form (the
+ * merit function and the commit stay FP64). */
 int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial, int form);
 
 /* Merit values of the last calc_global_fit: per type (index 1..3)
@@ -240,6 +243,57 @@ int galic_ensemble_autotune(galic_ensemble *e, double sample_fraction, int *best
  * summed over the members, and the number of nodes of the graph */
 int galic_ensemble_last_timing(const galic_ensemble *e, double *ms_total, double *ms_orbit_kernel,
                                long long *orbit_steps, int *graph_nodes);
+
+/* ------------------------------------------------------- serving */
+
+/* One model-construction job: GALIC's run (main.c:69-107) from the point
+ * where the grids and the initial particles exist.  Arrays are in the
+ * layouts of the galic_set_* calls and must stay valid until the job is
+ * done.  No counterpart in the reference (one model per MPI job). */
+typedef struct {
+  const galic_params_t *prm;
+  const double *fg_pot, *fg_dpotdr, *fg_dpotdz;  /* FG_Nbin^2 each */
+  const double *vstream[4];                      /* [1..3]; NULL = zero */
+  const double *cellsize, *dgs_distance;         /* DG_Ngrid, DG_Nstack */
+  const double *targets[4][6];                   /* [type 1..3]: DGs_Mass, EGs_Mass, r, t, p, q stacks */
+  int n;
+  const double *pos, *vel, *mass, *tint, *vesc, *ptargets;
+  const int *type;
+  int form;                  /* form of calc_all_response_fields and of the repetitions' orbits */
+  int max_iterations;        /* All.MaximumNumberOfSteps */
+  int reps_per_iteration;    /* All.IndepenentOptimizationsPerStep */
+  double fraction_per_rep;   /* All.FractionToOptimizeIndependendly: n_per_cpu = 1 + f n (main.c:129) */
+  double converge_rel;       /* stop after an iteration that lowers Sall by less than this fraction; 0 = never */
+  uint64_t seed;             /* proposal streams (seed, particle, repetition) */
+  const int *permutation;    /* optimisation order (main.c:137-139); NULL = 0..n-1 */
+  double *vel_out;           /* n x 3 final velocities, or NULL */
+} galic_job_t;
+
+typedef struct {
+  int status;                /* galic_status of the job */
+  int iterations;
+  long long reps;
+  long long orbit_steps;     /* calc_all and every repetition */
+  double sall_first, sall_last;  /* Sall (main.c:1270) summed over types, after calc_all / at the end */
+  double fit[28];            /* galic_get_fit at the end */
+  double t_submit, t_admit, t_first_response, t_done;  /* seconds since the server started */
+} galic_job_result_t;
+
+/* Worker threads run admitted jobs concurrently on the current device; a
+ * queued job is admitted (first fit, in arrival order) when a worker is free
+ * and its device footprint (galic_job_device_bytes) fits what the running
+ * jobs leave of hbm_budget_bytes.  A job larger than the whole budget ends
+ * with GALIC_ERR_BUDGET. */
+typedef struct galic_server galic_server;
+int galic_server_create(size_t hbm_budget_bytes, int workers, galic_server **out);
+int galic_server_submit(galic_server *s, const galic_job_t *job, int *job_id);
+/* waits up to timeout_s for the job; GALIC_ERR_STATE if it is not done */
+int galic_server_wait(galic_server *s, int job_id, double timeout_s, galic_job_result_t *res);
+int galic_server_stats(galic_server *s, size_t *peak_bytes, int *peak_running, int *queued, int *running);
+/* finishes every submitted job, then stops the workers */
+void galic_server_destroy(galic_server *s);
+/* device bytes the server reserves for a job */
+size_t galic_job_device_bytes(const galic_job_t *job);
 
 /* ------------------------------------------------------- force-grid fill */
 

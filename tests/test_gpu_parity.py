@@ -176,3 +176,37 @@ def test_fp32_form_close_to_fp64():
     assert abs(s32 - s64) <= 1e-3 * s64
     assert err < 1e-3
     assert ferr < 1e-3
+
+
+def test_fp32_repetition_close_to_fp64():
+    """An optimisation repetition with FP32 orbits against the FP64 one from the
+    same committed state: identical proposals (same Philox streams), nearly all
+    accept decisions equal, the merit values close; repeatable bit for bit."""
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64
+
+    m = synth.config_halo_disk(n_halo=8000, n_disk=2000, level=6, seed=8)
+    idx = np.random.default_rng(3).permutation(m.n)[:200]
+    out = {}
+    for name, form in (("fp64", GALIC_FORM_FP64), ("fp32", GALIC_FORM_FP32), ("fp32b", GALIC_FORM_FP32)):
+        with Context(m.params) as ctx:
+            ctx.load_model(m)
+            ctx.calc_all_response_fields(GALIC_FORM_FP64)
+            v0 = ctx.particles()[0]
+            ctx.optimize_rep(idx, 77, 0, form)
+            vel = ctx.particles()[0]
+            out[name] = (ctx.fit(), vel, ctx.counters(), v0)
+    f64, v64, (t64, c64), v0 = out["fp64"]
+    f32, v32, (t32, c32), _ = out["fp32"]
+    assert np.array_equal(out["fp32b"][0], f32) and np.array_equal(out["fp32b"][1], v32)
+    assert np.array_equal(t64, t32)
+    moved64 = np.any(v64[idx] != v0[idx], axis=1)
+    moved32 = np.any(v32[idx] != v0[idx], axis=1)
+    agree = np.mean(moved64 == moved32)
+    both = moved64 & moved32
+    assert np.array_equal(v64[idx][both], v32[idx][both])  # same proposal where both accept
+    a, b = f32[1:3, :5], f64[1:3, :5]
+    nz = b != 0
+    ferr = np.max(np.abs(a[nz] - b[nz]) / np.abs(b[nz]))
+    print(f"fp32 repetition: accept decisions agree {agree:.3f}, fit {ferr:.3e}")
+    assert agree >= 0.9
+    assert ferr < 1e-2
