@@ -143,6 +143,9 @@ SIGNATURES = [
      [VP, PD, PD, C.c_int, PD, PD, PD, PD, PD, C.c_double, C.c_double, PI, C.c_int]),
     ("galic_produce_orbit_response_field", C.c_double, [VP, PD, PD, C.c_int, PD, C.c_double, C.c_double, PI]),
     ("galic_calc_all_response_fields", C.c_int, [VP, C.c_int]),
+    ("galic_calc_all_shard", C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
+    ("galic_accumulators", C.c_int, [VP, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    ("galic_calc_all_finish", C.c_int, [VP]),
     ("galic_optimize_rep", C.c_int, [VP, PI, C.c_int, C.c_uint64, C.c_uint32, C.c_int]),
     ("galic_get_fit", C.c_int, [VP, PD]),
     ("galic_get_counters", C.c_int, [VP, PLL, PLL]),

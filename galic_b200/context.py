@@ -110,6 +110,13 @@ class Context:
     def calc_all_response_fields(self, form=_ffi.GALIC_FORM_FP64):
         _check(self.lib.galic_calc_all_response_fields(self.h, form), "galic_calc_all_response_fields")
 
+    def calc_all_shard(self, form, rank, world):
+        """This rank's part of a sharded calc_all (galic_calc_all_shard)."""
+        _check(self.lib.galic_calc_all_shard(self.h, int(form), int(rank), int(world)), "galic_calc_all_shard")
+
+    def calc_all_finish(self):
+        _check(self.lib.galic_calc_all_finish(self.h), "galic_calc_all_finish")
+
     def optimize_rep(self, idx, seed, rep_serial, form=_ffi.GALIC_FORM_FP64):
         idx = np.ascontiguousarray(idx, dtype=np.int32)
         _check(self.lib.galic_optimize_rep(self.h, _ffi.iptr(idx), len(idx), int(seed), int(rep_serial), form),

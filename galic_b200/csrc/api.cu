@@ -580,18 +580,26 @@ extern "C" double galic_produce_orbit_response_field(galic_ctx *ctx, double *pos
   return one_orbit(ctx, pos, vel, g, mass, timespan, orbitstaken, 1, 0);
 }
 
-extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
+namespace {
+
+int check_calc_all(galic_ctx *ctx, int form)
 {
-  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
   if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   if(ctx->n == 0 || !ctx->have_geom) return fail(ctx, GALIC_ERR_STATE);
   if(form == GALIC_FORM_FP32) {
     int st = ensure_tab32(ctx);
     if(st) return st;
   }
-  const galic_params_t &p = ctx->prm;
   for(int t = 1; t <= 3; t++)
-    if(p.NType[t] > 0 && !ctx->have_targets[t]) return fail(ctx, GALIC_ERR_STATE);
+    if(ctx->prm.NType[t] > 0 && !ctx->have_targets[t]) return fail(ctx, GALIC_ERR_STATE);
+  return GALIC_OK;
+}
+
+// main.c:151-231 for the orbits order[first + k * stride] and the particles
+// first, first + stride, ...: zeroes the accumulators and leaves every
+// deposit in fixed point (no synchronisation)
+int enqueue_orbits(galic_ctx *ctx, int form, int first, int stride, int *launches)
+{
   cudaStream_t s = ctx->stream;
   const int G = ctx->G;
   int shift[4 * NG_COMMITTED];
@@ -604,7 +612,9 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   CK(cudaMemsetAsync(ctx->d_maxerr, 0, sizeof(double), s));
   CK(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), s));
   CalcAllArgs a;
-  a.n = ctx->n;
+  a.n = first < ctx->n ? (ctx->n - first + stride - 1) / stride : 0;
+  a.first = first;
+  a.stride = stride;
   a.pos = ctx->d_pos;
   a.vel = ctx->d_vel;
   a.mass = ctx->d_mass;
@@ -618,27 +628,43 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   a.steps_total = ctx->d_counters + 8;
   a.max_egy_err = ctx->d_maxerr;
   a.status = ctx->d_status;
-  int launches = 0;
   const int block = form == GALIC_FORM_FP32 ? 256 : 128;
   int per_sm = form == GALIC_FORM_FP32 ? calc_all_fp32_occupancy(block) : calc_all_occupancy(block);
   if(per_sm < 1) per_sm = 1;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   int grid = per_sm * sms;
-  int need = (ctx->n + block - 1) / block;
+  const int need = (a.n + block - 1) / block;
   if(grid > need) grid = need;
   CK(cudaEventRecord(ctx->ev[1], s));
-  if(form == GALIC_FORM_FP32)
-    launches += launch_calc_all_fp32(ctx->dm, ctx->d_tab32, ctx->d_cellsize32, a, grid, block, s);
-  else
-    launches += launch_calc_all_fp64(ctx->dm, a, grid, block, s);
+  if(grid > 0) {
+    if(form == GALIC_FORM_FP32)
+      *launches += launch_calc_all_fp32(ctx->dm, ctx->d_tab32, ctx->d_cellsize32, a, grid, block, s);
+    else
+      *launches += launch_calc_all_fp64(ctx->dm, a, grid, block, s);
+  }
   CK(cudaEventRecord(ctx->ev[2], s));
   launch_instantaneous(ctx->dm, ctx->n, ctx->d_pos, ctx->d_vel, ctx->d_mass, ctx->d_type, ctx->d_vdisp, ctx->d_fx,
-                       ctx->d_shift, G, s);
-  launch_fx_finalize(ctx->d_fx, ctx->d_shift, ctx->d_committed, 4 * NG_COMMITTED, G, s);
-  launches += 2;
-  FitArgs f = make_fit_args(ctx);
-  launches += launch_global_fit(f, s);
+                       ctx->d_shift, G, s, first, stride);
+  *launches += 1;
+  CK(cudaGetLastError());
+  return GALIC_OK;
+}
+
+// fixed point -> committed grids, then calc_global_fit (main.c:251-362)
+int enqueue_finish(galic_ctx *ctx, int *launches)
+{
+  launch_fx_finalize(ctx->d_fx, ctx->d_shift, ctx->d_committed, 4 * NG_COMMITTED, ctx->G, ctx->stream);
+  *launches += 1;
+  *launches += launch_global_fit(make_fit_args(ctx), ctx->stream);
+  CK(cudaGetLastError());
+  return GALIC_OK;
+}
+
+// waits for the stream; records timing, steps and the worst orbit status
+int collect(galic_ctx *ctx, int launches, bool with_timing)
+{
+  cudaStream_t s = ctx->stream;
   int status = 0;
   unsigned long long steps = 0;
   CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -649,16 +675,67 @@ extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
   CK(cudaEventRecord(ev_end, s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
-  float ms_total = 0, ms_orbit = 0;
-  CK(cudaEventElapsedTime(&ms_total, ctx->ev[0], ev_end));
-  CK(cudaEventElapsedTime(&ms_orbit, ctx->ev[1], ctx->ev[2]));
+  if(with_timing) {
+    float ms_total = 0, ms_orbit = 0;
+    CK(cudaEventElapsedTime(&ms_total, ctx->ev[0], ev_end));
+    CK(cudaEventElapsedTime(&ms_orbit, ctx->ev[1], ctx->ev[2]));
+    ctx->last_ms_total = ms_total;
+    ctx->last_ms_orbit = ms_orbit;
+  }
   cudaEventDestroy(ev_end);
-  ctx->last_ms_total = ms_total;
-  ctx->last_ms_orbit = ms_orbit;
   ctx->last_steps = (long long) steps;
   ctx->last_launches = launches;
   if(status == ORBIT_STEP_CAP) return fail(ctx, GALIC_ERR_STEP_CAP);
   if(status == ORBIT_NONFINITE) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  return GALIC_OK;
+}
+
+}  // namespace
+
+extern "C" int galic_calc_all_response_fields(galic_ctx *ctx, int form)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  int st = check_calc_all(ctx, form);
+  if(st) return st;
+  int launches = 0;
+  if((st = enqueue_orbits(ctx, form, 0, 1, &launches))) return st;
+  if((st = enqueue_finish(ctx, &launches))) return st;
+  if((st = collect(ctx, launches, true))) return st;
+  ctx->have_response = true;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_calc_all_shard(galic_ctx *ctx, int form, int rank, int world)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(world < 1 || rank < 0 || rank >= world) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  int st = check_calc_all(ctx, form);
+  if(st) return st;
+  int launches = 0;
+  ctx->have_response = false;
+  ctx->shard_form = form;
+  if((st = enqueue_orbits(ctx, form, rank, world, &launches))) return st;
+  return fail(ctx, collect(ctx, launches, true));
+}
+
+extern "C" int galic_accumulators(galic_ctx *ctx, void **device_ptr, size_t *words)
+{
+  if(!ctx || !device_ptr || !words) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  *device_ptr = (void *) ctx->d_fx;
+  *words = (size_t) 4 * NG_COMMITTED * ctx->G * 2;
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_calc_all_finish(galic_ctx *ctx)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(ctx->shard_form < 0) return fail(ctx, GALIC_ERR_STATE);
+  int launches = 0;
+  int st = enqueue_finish(ctx, &launches);
+  if(st) return st;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->last_launches = launches;
+  ctx->shard_form = -1;
   ctx->have_response = true;
   return fail(ctx, GALIC_OK);
 }

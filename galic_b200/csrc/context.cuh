@@ -69,6 +69,8 @@ struct galic_ctx {
   double last_ms_total = 0, last_ms_orbit = 0;
   // bumped by every upload; an ensemble built over this context checks it
   unsigned generation = 0;
+  // form of a galic_calc_all_shard awaiting galic_calc_all_finish, else -1
+  int shard_form = -1;
 };
 
 namespace galic_internal {

@@ -41,7 +41,8 @@ struct OrbitBatch {
 };
 
 struct CalcAllArgs {
-  int n;
+  int n;                      // orbits of this launch: order[first + k * stride], k < n
+  int first = 0, stride = 1;
   const double *pos, *vel, *mass, *tint;
   const int *type;
   const int *order;           // processing order (longest first)
@@ -74,8 +75,10 @@ void launch_orbits_dense_fp32(const DevModel &M64, const float4 *const quad[4], 
                               const OrbitBatch &b, cudaStream_t s);
 void launch_scale_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s);
 int launch_calc_all_fp64(const DevModel &M, const CalcAllArgs &a, int grid, int block, cudaStream_t s);
+// particles first, first + stride, ... below n
 void launch_instantaneous(const DevModel &M, int n, const double *pos, const double *vel, const double *mass,
-                          const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid, cudaStream_t s);
+                          const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid, cudaStream_t s,
+                          int first = 0, int stride = 1);
 void launch_fx_finalize(const FxWord *fx, const int *shift, double *committed, int count, int Ngrid, cudaStream_t s);
 int launch_global_fit(const FitArgs &f, cudaStream_t s);
 cudaError_t prepare_fit_kernels();

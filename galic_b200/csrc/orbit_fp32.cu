@@ -354,7 +354,7 @@ struct SingleSrc {
   DevModel M64;
   Model32 M;
   Particles32 P;
-  int n;
+  int n, first, stride;  // orbits order[first + k * stride], k < n
   int *next;
   FxWord *fx;        // [4][NG_COMMITTED][Ngrid]
   const int *shift;  // [4][NG_COMMITTED]
@@ -370,7 +370,8 @@ struct SingleSrc {
     const int k = atomicAdd(next, 1);
     if(k >= n) return false;
     mi = 0;
-    p = P.order ? P.order[k] : k;
+    const int kk = first + k * stride;
+    p = P.order ? P.order[kk] : kk;
     return true;
   }
   __device__ __forceinline__ void flush_stats(int, unsigned long long st, double err, int stat) const
@@ -721,6 +722,8 @@ int launch_calc_all_fp32(const DevModel &M64, const float4 *const quad[4], const
   S.P.order = a.order;
   S.P.orbits = a.orbits;
   S.n = a.n;
+  S.first = a.first;
+  S.stride = a.stride;
   S.next = a.next;
   S.fx = a.fx;
   S.shift = a.shift;

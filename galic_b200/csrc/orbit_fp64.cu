@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevMod
       p = -1;
       return false;
     }
+    k = A.first + k * A.stride;
     p = A.order ? A.order[k] : k;
     int type = A.type[p];
     sink.type = type;
@@ -204,10 +205,11 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevMod
 
 // main.c:226-229 for every particle: vdisp = projections of the current
 // velocity; the instantaneous energy grids get mass and mass * v^2
-__global__ void k_instantaneous(DevModel M, int n, const double *pos, const double *vel, const double *mass,
-                                const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid)
+__global__ void k_instantaneous(DevModel M, int n, int first, int stride, const double *pos, const double *vel,
+                                const double *mass, const int *type, double *vdisp, FxWord *fx, const int *shift,
+                                int Ngrid)
 {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = first + (blockIdx.x * blockDim.x + threadIdx.x) * stride;
   if(k >= n) return;
   LogConsts L = make_log_consts(M);
   int t = type[k];
@@ -272,10 +274,13 @@ int launch_calc_all_fp64(const DevModel &M, const CalcAllArgs &a, int grid, int 
 }
 
 void launch_instantaneous(const DevModel &M, int n, const double *pos, const double *vel, const double *mass,
-                          const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid, cudaStream_t s)
+                          const int *type, double *vdisp, FxWord *fx, const int *shift, int Ngrid, cudaStream_t s,
+                          int first, int stride)
 {
-  if(n <= 0) return;
-  k_instantaneous<<<(n + 127) / 128, 128, 0, s>>>(M, n, pos, vel, mass, type, vdisp, fx, shift, Ngrid);
+  if(n <= first || stride < 1) return;
+  const int count = (n - first + stride - 1) / stride;
+  k_instantaneous<<<(count + 127) / 128, 128, 0, s>>>(M, n, first, stride, pos, vel, mass, type, vdisp, fx, shift,
+                                                      Ngrid);
 }
 
 void launch_fx_finalize(const FxWord *fx, const int *shift, double *committed, int count, int Ngrid, cudaStream_t s)

@@ -139,6 +139,22 @@ double galic_produce_orbit_response_field(galic_ctx *ctx, double *pos, double *v
  * accumulation, adds the instantaneous energy grid, and evaluates the fit. */
 int galic_calc_all_response_fields(galic_ctx *ctx, int form);
 
+/* calc_all_response_fields split for a model sharded over `world` ranks
+ * (the reference's MPI layout, main.c:201-231 with the Allreduce of
+ * main.c:259-285): galic_calc_all_shard integrates the orbits
+ * order[rank + k * world] and the instantaneous energy of particles
+ * rank, rank + world, ... into the context's fixed-point accumulators
+ * (zeroed first); the caller sums the accumulators of all ranks elementwise
+ * as 64-bit integers (galic_accumulators gives their device address and
+ * count of int64 words: exact, so the sum equals a one-rank pass bit for bit)
+ * and then calls galic_calc_all_finish on every rank, which converts them to
+ * the committed grids and evaluates calc_global_fit.  Per-particle state
+ * written by the pass (orbit counts, instantaneous dispersions) is valid for
+ * the rank's own particles only. */
+int galic_calc_all_shard(galic_ctx *ctx, int form, int rank, int world);
+int galic_accumulators(galic_ctx *ctx, void **device_ptr, size_t *words);
+int galic_calc_all_finish(galic_ctx *ctx);
+
 /* One optimisation repetition: init_updates (main.c:844-874), optimize(n)
  * for n = idx[0..count-1] (main.c:365-527) and commit_updates
  * (main.c:808-841), which ends in calc_global_fit.  Proposals for idx[k] are
