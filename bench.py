@@ -268,7 +268,7 @@ def measure_serving(count, mean_gap, scale, torch):
     return {"requests": count, "completed": len(ok), "mean_gap_s": mean_gap, "particles_scale": scale,
             "n_range": [int(min(m.n for m in models)), int(max(m.n for m in models))],
             "schedule": {"calc_all": "fp32", "iterations": 2, "reps_per_iteration": 5,
-                         "fraction_per_rep": 0.001, "reps": "fp64"},
+                         "fraction_per_rep": 0.001, "reps": "fp32 orbits, fp64 merit"},
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "makespan_s": makespan, "orbit_steps": int(steps), "orbit_steps_per_s": steps / makespan,
             "hbm_budget_bytes": budget, "peak_bytes": st["peak_bytes"], "peak_concurrent_jobs": st["peak_running"]}
