@@ -39,23 +39,23 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
   __syncwarp();
 }
 
-// FP32 variant: the lane parks its FP32 sums and the orbit's FP64 scale; the
-// drain forms the FP64 product and adds it as ONE signed 64-bit fixed-point
-// word, X = round(v * 2^(shift-24)), to the high word of the bin (the low
-// word stays zero, so fx_value reads it unchanged).  shift - 24 is chosen so
-// that no bin can overflow 2^62; the resolution (~2^-62 of the bound) is far
-// inside the FP32 form's tolerance, and one atomic per value instead of two
-// halves the L2 atomic traffic.
+// FP32 variant.  A lane parks only the values that leave its accumulators,
+// each already as (word index, value x 2^(shift-24) in FP32): the orbit's
+// mass/Tint and the field's fixed-point scale are folded into one FP32 factor
+// per field class when the orbit starts.  The drain rounds each item to one
+// signed 64-bit fixed-point word, X = round(scaled value), and adds it to the
+// high word of the bin (the low word stays zero, so fx_value reads it
+// unchanged).  shift - 24 is chosen so that no bin can overflow 2^62; the
+// FP32 rounding of the scaled value (2^-24 relative) is far inside the FP32
+// form's tolerance, and one atomic per value instead of two halves the L2
+// atomic traffic.
 struct WarpQueue32 {
-  float val[32][20];
-  double fac[32];
-  int cell[32];
-  int type[32];
+  int2 item[32][20];  // {fixed-point word index, __float_as_int(scaled value)}
+  int count[32];
   int list[32];
 };
 
-__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, unsigned full, FxWord *fx, const int *shift, int G,
-                                             int Nb)
+__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, unsigned full, FxWord *fx)
 {
   const int lane = threadIdx.x & 31;
   if(full & (1u << lane)) q.list[__popc(full & ((1u << lane) - 1))] = lane;
@@ -64,14 +64,10 @@ __device__ __forceinline__ void warp_drain32(WarpQueue32 &q, unsigned full, FxWo
   for(int it = lane; it < items; it += 32) {
     const int s = q.list[it / 20];
     const int k = it - (it / 20) * 20;
-    const int corner = k / 5, f = k - corner * 5;
-    const int off = (corner & 1) + ((corner >> 1) ? Nb : 0);
-    const int t = q.type[s];
-    const float vf = q.val[s][k];
-    if(vf == 0.f) continue;
-    const double v = (double) vf * q.fac[s];
-    const long long X = __double2ll_rn(ldexp(v, shift[t * NG_COMMITTED + f] - 24));
-    if(X) atomicAdd(&fx[((size_t) t * NG_COMMITTED + f) * G + q.cell[s] + off].hi, (unsigned long long) X);
+    if(k >= q.count[s]) continue;
+    const int2 e = q.item[s][k];
+    const long long X = __float2ll_rn(__int_as_float(e.y));
+    if(X) atomicAdd(&fx[e.x].hi, (unsigned long long) X);
   }
   __syncwarp();
 }

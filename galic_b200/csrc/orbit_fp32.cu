@@ -165,75 +165,54 @@ __device__ __forceinline__ Cell32 density_cell32(const Model32 &M, const float *
   return cell32(br, bz, M.DG_Nbin, M.dgmax);
 }
 
-// Register-merged FP32 sums per corner of the current DG cell.  When the
-// orbit moves to a neighbouring cell, the corners the two cells share keep
-// their sums (moved to their slot in the new cell) and only the corners left
-// behind are parked in the warp queue (the drain skips the zero entries);
-// any other move parks all four.
-struct Sink32 {
-  WarpQueue32 *q;
-  int lane, type, Nb;
-  double fac;
-  int cur, cur_iR, cur_iz;
-  bool parked;
+// Register-merged FP32 sums for the four grid nodes of the current DG cell.
+// A node (z, r) always lives in accumulator slot ((z & 1) << 1) | (r & 1):
+// the four nodes of any cell have the four parities, so when the orbit moves
+// to a neighbouring cell the nodes both cells share stay in their slots
+// untouched, and only the slots whose node changes are flushed and cleared.
+// A deposit's corner c = 2 dz + dr of the cell lands in slot c ^ parity(cell).
+struct NodeAcc {
+  int cur = -1, cur_iR = 0, cur_iz = 0;
   float a[4][5];
-  __device__ __forceinline__ void park_masked(const bool keep[4])
+  __device__ __forceinline__ int parity() const { return ((cur_iz & 1) << 1) | (cur_iR & 1); }
+  // slot s of cell (iz, iR) holds node (iz + node_dz(s, iz), iR + node_dr(s, iR))
+  __device__ __forceinline__ static int node_dz(int s, int iz) { return ((s >> 1) ^ iz) & 1; }
+  __device__ __forceinline__ static int node_dr(int s, int iR) { return (s ^ iR) & 1; }
+  // slots whose node is not a node of cell (iz, iR)
+  __device__ __forceinline__ void leaving(int iR, int iz, bool out[4]) const
   {
 #pragma unroll
-    for(int c = 0; c < 4; c++)
-#pragma unroll
-      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = keep[c] ? 0.f : a[c][f];
-    q->fac[lane] = fac;
-    q->cell[lane] = cur;
-    q->type[lane] = type;
-    parked = true;
+    for(int s = 0; s < 4; s++)
+      out[s] = (cur_iz + node_dz(s, cur_iz) != iz + node_dz(s, iz)) ||
+               (cur_iR + node_dr(s, cur_iR) != iR + node_dr(s, iR));
   }
-  __device__ __forceinline__ void park()
+  __device__ __forceinline__ void clear(const bool which[4])
   {
-    if(cur < 0) return;
-    const bool none[4] = {false, false, false, false};
-    park_masked(none);
-    cur = -1;
+#pragma unroll
+    for(int s = 0; s < 4; s++)
+#pragma unroll
+      for(int f = 0; f < 5; f++) a[s][f] = which[s] ? 0.f : a[s][f];
   }
-  __device__ __forceinline__ void move_to(int iR, int iz)
+  __device__ __forceinline__ void accumulate(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
   {
-    const int dz = iz - cur_iz, dR = iR - cur_iR;
-    if(cur >= 0 && dz >= -1 && dz <= 1 && dR >= -1 && dR <= 1) {
-      bool keep[4] = {false, false, false, false};
-      float na[4][5];
-#pragma unroll
-      for(int j = 0; j < 4; j++) {
-#pragma unroll
-        for(int f = 0; f < 5; f++) na[j][f] = 0.f;
-#pragma unroll
-        for(int k = 0; k < 4; k++) {
-          // new corner j = (iz + (j>>1), iR + (j&1)) is old corner k = (cur_iz + (k>>1), cur_iR + (k&1))
-          const bool same = ((k >> 1) == (j >> 1) + dz) && ((k & 1) == (j & 1) + dR);
-          keep[k] = keep[k] || same;
-#pragma unroll
-          for(int f = 0; f < 5; f++) na[j][f] = same ? a[k][f] : na[j][f];
-        }
-      }
-      park_masked(keep);
-#pragma unroll
-      for(int j = 0; j < 4; j++)
-#pragma unroll
-        for(int f = 0; f < 5; f++) a[j][f] = na[j][f];
-    } else {
-      park();
-#pragma unroll
-      for(int k = 0; k < 4; k++)
-#pragma unroll
-        for(int f = 0; f < 5; f++) a[k][f] = 0.f;
+    // corner weights, then permuted from corners c to slots s = c ^ parity
+    float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
+    if(iR & 1) {
+      float t = w[0];
+      w[0] = w[1];
+      w[1] = t;
+      t = w[2];
+      w[2] = w[3];
+      w[3] = t;
     }
-    cur = iz * Nb + iR;
-    cur_iR = iR;
-    cur_iz = iz;
-  }
-  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
-  {
-    if(iz * Nb + iR != cur) move_to(iR, iz);
-    const float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
+    if(iz & 1) {
+      float t = w[0];
+      w[0] = w[2];
+      w[2] = t;
+      t = w[1];
+      w[1] = w[3];
+      w[3] = t;
+    }
 #pragma unroll
     for(int k = 0; k < 4; k++) {
       a[k][0] += w[k];
@@ -242,6 +221,64 @@ struct Sink32 {
       a[k][3] = fmaf(w[k], p.vq2, a[k][3]);
       a[k][4] = fmaf(w[k], p.vp2, a[k][4]);
     }
+  }
+};
+
+// Sink of the batched kernels: on a cell change the nonzero sums of the
+// leaving nodes are parked in the lane's slot of the warp queue as
+// (word index, scaled value) items, and the warp drains all parked slots
+// together (flush.cuh).
+struct Sink32 : NodeAcc {
+  WarpQueue32 *q;
+  int lane, Nb, G;
+  int gbase;                // first word of the orbit's grid set: gridset * NG_COMMITTED * G
+  float scale_m, scale_e;   // mass/Tint x 2^(shift-24) of the mass and energy fields
+  bool parked;
+  __device__ __forceinline__ void park_masked(const bool out[4])
+  {
+    int n = 0;
+#pragma unroll
+    for(int s = 0; s < 4; s++) {
+      if(!out[s]) continue;
+      const int node = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
+#pragma unroll
+      for(int f = 0; f < 5; f++) {
+        const float v = a[s][f];
+        if(v != 0.f) {
+          q->item[lane][n] = make_int2(gbase + f * G + node, __float_as_int(v * (f == 0 ? scale_m : scale_e)));
+          n++;
+        }
+      }
+    }
+    q->count[lane] = n;
+    parked = true;
+  }
+  __device__ __forceinline__ void park()
+  {
+    if(cur < 0) return;
+    const bool all[4] = {true, true, true, true};
+    park_masked(all);
+    cur = -1;
+  }
+  __device__ __forceinline__ void move_to(int iR, int iz)
+  {
+    if(cur >= 0) {
+      bool out[4];
+      leaving(iR, iz, out);
+      park_masked(out);
+      clear(out);
+    } else {
+      const bool all[4] = {true, true, true, true};
+      clear(all);
+    }
+    cur = iz * Nb + iR;
+    cur_iR = iR;
+    cur_iz = iz;
+  }
+  __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
+  {
+    if(iz * Nb + iR != cur) move_to(iR, iz);
+    accumulate(iR, iz, hdt, fR, fz, p);
   }
 };
 
@@ -448,6 +485,7 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
   Sink32 sink;
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
+  sink.G = G;
   sink.cur = -1;
   sink.parked = false;
   int p = -1, mi = 0, stat_mi = 0;
@@ -473,8 +511,13 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
     const Particles32 &P = S.particles(mi);
     const int type = P.type[p];
     sink.Nb = M.DG_Nbin;
-    sink.type = S.gridset(mi, type);
-    sink.fac = P.mass[p] / P.tint[p];
+    {
+      const int gs = S.gridset(mi, type);
+      const double fac = P.mass[p] / P.tint[p];
+      sink.gbase = gs * NG_COMMITTED * G;
+      sink.scale_m = (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_MASS_S] - 24);
+      sink.scale_e = (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_R_S] - 24);
+    }
     sink.cur = -1;
     double xd[3], vd[3];
     for(int i = 0; i < 3; i++) {
@@ -491,7 +534,7 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
   for(;;) {
     const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
     if(full) {
-      warp_drain32(*sink.q, full, S.fx, S.shift, G, S.model(0).DG_Nbin);
+      warp_drain32(*sink.q, full, S.fx);
       sink.parked = false;
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
@@ -529,78 +572,46 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_ensemble_fp32(const __grid_cons
   calc_all_fp32_body<BLOCK>(S);
 }
 
-// Dense sink of one orbit: FP32 sums per corner of the current DG cell in
-// registers, added into the orbit's own FP64 grids [5][Ngrid] when the orbit
-// leaves the cell (corners shared with the next cell keep their sums).
-struct DenseSink32 {
+// Dense sink of one orbit: the node sums of NodeAcc, added into the orbit's
+// own FP64 grids [5][Ngrid] when their node leaves the current cell.
+struct DenseSink32 : NodeAcc {
   double *grid;
   int G, Nb;
-  int cur = -1, cur_iR = 0, cur_iz = 0;
-  float a[4][5];
-  __device__ __forceinline__ void flush_masked(const bool keep[4])
+  __device__ __forceinline__ void flush_nodes(const bool out[4])
   {
 #pragma unroll
-    for(int c = 0; c < 4; c++) {
-      if(keep[c]) continue;
-      const int off = cur + (c & 1) + ((c >> 1) ? Nb : 0);
+    for(int s = 0; s < 4; s++) {
+      if(!out[s]) continue;
+      const int node = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
 #pragma unroll
       for(int f = 0; f < 5; f++)
-        if(a[c][f] != 0.f) grid[(size_t) f * G + off] += (double) a[c][f];
+        if(a[s][f] != 0.f) grid[(size_t) f * G + node] += (double) a[s][f];
     }
   }
   __device__ __forceinline__ void flush()
   {
     if(cur < 0) return;
-    const bool none[4] = {false, false, false, false};
-    flush_masked(none);
+    const bool all[4] = {true, true, true, true};
+    flush_nodes(all);
     cur = -1;
-  }
-  __device__ __forceinline__ void move_to(int iR, int iz)
-  {
-    const int dz = iz - cur_iz, dR = iR - cur_iR;
-    if(cur >= 0 && dz >= -1 && dz <= 1 && dR >= -1 && dR <= 1) {
-      bool keep[4] = {false, false, false, false};
-      float na[4][5];
-#pragma unroll
-      for(int j = 0; j < 4; j++) {
-#pragma unroll
-        for(int f = 0; f < 5; f++) na[j][f] = 0.f;
-#pragma unroll
-        for(int k = 0; k < 4; k++) {
-          const bool same = ((k >> 1) == (j >> 1) + dz) && ((k & 1) == (j & 1) + dR);
-          keep[k] = keep[k] || same;
-#pragma unroll
-          for(int f = 0; f < 5; f++) na[j][f] = same ? a[k][f] : na[j][f];
-        }
-      }
-      flush_masked(keep);
-#pragma unroll
-      for(int j = 0; j < 4; j++)
-#pragma unroll
-        for(int f = 0; f < 5; f++) a[j][f] = na[j][f];
-    } else {
-      flush();
-#pragma unroll
-      for(int k = 0; k < 4; k++)
-#pragma unroll
-        for(int f = 0; f < 5; f++) a[k][f] = 0.f;
-    }
-    cur = iz * Nb + iR;
-    cur_iR = iR;
-    cur_iz = iz;
   }
   __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
   {
-    if(iz * Nb + iR != cur) move_to(iR, iz);
-    const float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
-#pragma unroll
-    for(int k = 0; k < 4; k++) {
-      a[k][0] += w[k];
-      a[k][1] = fmaf(w[k], p.vr2, a[k][1]);
-      a[k][2] = fmaf(w[k], p.vt2, a[k][2]);
-      a[k][3] = fmaf(w[k], p.vq2, a[k][3]);
-      a[k][4] = fmaf(w[k], p.vp2, a[k][4]);
+    if(iz * Nb + iR != cur) {
+      if(cur >= 0) {
+        bool out[4];
+        leaving(iR, iz, out);
+        flush_nodes(out);
+        clear(out);
+      } else {
+        const bool all[4] = {true, true, true, true};
+        clear(all);
+      }
+      cur = iz * Nb + iR;
+      cur_iR = iR;
+      cur_iz = iz;
     }
+    accumulate(iR, iz, hdt, fR, fz, p);
   }
 };
 
@@ -678,7 +689,7 @@ Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const flo
 struct Variant {
   int block, min_blocks;
 };
-constexpr Variant kVariants[] = {{256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}, {384, 2}};
+constexpr Variant kVariants[] = {{256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}, {128, 5}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <int V>
