@@ -50,25 +50,26 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
 // form's tolerance, and one atomic per value instead of two halves the L2
 // atomic traffic.
 struct WarpQueue32 {
-  int2 item[32][20];  // {fixed-point word index, __float_as_int(scaled value)}
-  int count[32];
-  int list[32];
+  int2 item[32 * 20];  // {fixed-point word index, __float_as_int(scaled value)}, packed
+  int n;               // items parked since the last drain
 };
 
-__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, unsigned full, FxWord *fx)
+// a lane reserves room for `count` items; returns the first index
+__device__ __forceinline__ int queue32_reserve(WarpQueue32 &q, int count) { return atomicAdd(&q.n, count); }
+
+// all 32 lanes call this at the same point of the loop
+__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, FxWord *fx)
 {
-  const int lane = threadIdx.x & 31;
-  if(full & (1u << lane)) q.list[__popc(full & ((1u << lane) - 1))] = lane;
   __syncwarp();
-  const int items = __popc(full) * 20;
+  const int lane = threadIdx.x & 31;
+  const int items = q.n;
   for(int it = lane; it < items; it += 32) {
-    const int s = q.list[it / 20];
-    const int k = it - (it / 20) * 20;
-    if(k >= q.count[s]) continue;
-    const int2 e = q.item[s][k];
+    const int2 e = q.item[it];
     const long long X = __float2ll_rn(__int_as_float(e.y));
     if(X) atomicAdd(&fx[e.x].hi, (unsigned long long) X);
   }
+  __syncwarp();
+  if(lane == 0) q.n = 0;
   __syncwarp();
 }
 

@@ -238,19 +238,21 @@ struct Sink32 : NodeAcc {
   {
     int n = 0;
 #pragma unroll
+    for(int s = 0; s < 4; s++)
+#pragma unroll
+      for(int f = 0; f < 5; f++) n += (out[s] && a[s][f] != 0.f) ? 1 : 0;
+    if(n == 0) return;
+    int at = queue32_reserve(*q, n);
+#pragma unroll
     for(int s = 0; s < 4; s++) {
       if(!out[s]) continue;
       const int node = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
 #pragma unroll
       for(int f = 0; f < 5; f++) {
         const float v = a[s][f];
-        if(v != 0.f) {
-          q->item[lane][n] = make_int2(gbase + f * G + node, __float_as_int(v * (f == 0 ? scale_m : scale_e)));
-          n++;
-        }
+        if(v != 0.f) q->item[at++] = make_int2(gbase + f * G + node, __float_as_int(v * (f == 0 ? scale_m : scale_e)));
       }
     }
-    q->count[lane] = n;
     parked = true;
   }
   __device__ __forceinline__ void park()
@@ -480,6 +482,8 @@ template <int BLOCK, class Src>
 __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
 {
   __shared__ WarpQueue32 queues[BLOCK / 32];
+  if((threadIdx.x & 31) == 0) queues[threadIdx.x >> 5].n = 0;
+  __syncwarp();
   const int G = S.model64(0).DG_Ngrid;
   State32 s;
   Sink32 sink;
@@ -532,9 +536,8 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
 
   int state = begin() ? LANE_ACTIVE : LANE_DONE;
   for(;;) {
-    const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
-    if(full) {
-      warp_drain32(*sink.q, full, S.fx);
+    if(__any_sync(0xffffffffu, sink.parked)) {
+      warp_drain32(*sink.q, S.fx);
       sink.parked = false;
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
