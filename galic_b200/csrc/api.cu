@@ -464,15 +464,18 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
   CK(cudaMemcpyAsync(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double), ctx->stream));
   {
-    // neighbouring lanes then integrate orbits that start at similar radii and
-    // read nearby force-grid cells; results do not depend on the order
+    // by type, then by radius: neighbouring lanes then integrate orbits of one
+    // type (one velocity structure, no divergent projections) that start at
+    // similar radii and read nearby force-grid cells; results do not depend
+    // on the order
     std::vector<double> r2(n);
     std::vector<int> order(n);
     for(int i = 0; i < n; i++) {
       r2[i] = pos[3 * i] * pos[3 * i] + pos[3 * i + 1] * pos[3 * i + 1] + pos[3 * i + 2] * pos[3 * i + 2];
       order[i] = i;
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return r2[a] < r2[b]; });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return type[a] != type[b] ? type[a] < type[b] : r2[a] < r2[b]; });
     CK(cudaMemcpyAsync(ctx->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   }
   CK(cudaMemsetAsync(ctx->d_orbits, 0, n * sizeof(int), ctx->stream));
