@@ -33,6 +33,7 @@ struct Model32 {
   float GMb, Ab, eps_b;
   int tabulated, analytic_halo, analytic_bulge;
   int tovs[4];
+  int vstream_zero[4];     // FG_Vstream[type] identically zero: its corners are not read
   int FG_Nbin, DG_Nbin;
   float fgmax;             // FG_Nbin - 1
   float dgmax;             // DG_Nbin - 1
@@ -83,7 +84,8 @@ __device__ __forceinline__ void accel32(const Model32 &M, int type, const float 
   Cell32 c = cell32(jd, id, N, M.fgmax);
   // corners in the quad: (iz,iR), (iz,iR+1), (iz+1,iR), (iz+1,iR+1)
   const float4 *Q = M.quad[type] + 4 * (c.iz * N + c.iR);
-  const float4 qR = __ldg(&Q[0]), qZ = __ldg(&Q[1]), qV = __ldg(&Q[2]);
+  const float4 qR = __ldg(&Q[0]), qZ = __ldg(&Q[1]);
+  const float4 qV = M.vstream_zero[type] ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(&Q[2]);
   const float w00 = (1.f - c.fR) * (1.f - c.fz), w01 = c.fR * (1.f - c.fz);
   const float w10 = (1.f - c.fR) * c.fz, w11 = c.fR * c.fz;
   *vstr = qV.x * w00 + qV.z * w10 + qV.y * w01 + qV.w * w11;
@@ -289,6 +291,7 @@ struct State32 {
   double tall, timespan, E0;
   int iR, iz;
   float fR, fz, radsign_prev;
+  float pend;    // weight of the deferred end-of-step deposit
   int cs_cell;   // DG cell whose size is cached in cs_val
   float cs_val;
   Proj32 proj;
@@ -323,10 +326,14 @@ __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const
   s.fz = c.fz;
   s.proj = project32(s.tovs, s.x, s.v, vstr);
   s.cs_cell = -1;
+  s.pend = 0.f;
 }
 
 // one KDK step with its two deposits (orbit_response.c:211-458) in FP32;
-// false once the orbit has ended (time span reached, step cap, non-finite)
+// false once the orbit has ended (time span reached, step cap, non-finite).
+// The end-of-step deposit and the next step's start deposit sit at the same
+// position, cell and projections, so they are made as one deposit with the
+// two half-step weights added (the last one when the orbit ends).
 template <class Sink>
 __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink &sink)
 {
@@ -347,7 +354,7 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   }
   const float hdt = 0.5f * (float) dt;
   const float fdt = (float) dt;
-  sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+  sink.add(s.iR, s.iz, hdt + s.pend, s.fR, s.fz, s.proj);
 #pragma unroll
   for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
 #pragma unroll
@@ -362,7 +369,7 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   s.fR = c.fR;
   s.fz = c.fz;
   s.proj = project32(s.tovs, s.x, s.v, vstr);
-  sink.add(s.iR, s.iz, hdt, s.fR, s.fz, s.proj);
+  s.pend = hdt;
   s.tall += dt;
   const float radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];
   if(radsign > 0.f && s.radsign_prev < 0.f) s.norbit++;
@@ -376,6 +383,7 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
     s.status = ORBIT_STEP_CAP;
     return false;
   }
+  if(s.flag) sink.add(s.iR, s.iz, s.pend, s.fR, s.fz, s.proj);
   return !s.flag;
 }
 
@@ -676,6 +684,7 @@ Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const flo
   M.analytic_bulge = M64.analytic_bulge;
   for(int t = 0; t < 4; t++) {
     M.tovs[t] = M64.tovs[t];
+    M.vstream_zero[t] = M64.vstream_zero[t];
     M.quad[t] = quad[t];
   }
   M.FG_Nbin = M64.FG_Nbin;
