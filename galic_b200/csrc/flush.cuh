@@ -39,10 +39,11 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
   __syncwarp();
 }
 
-// FP32 variant.  A lane parks only the values that leave its accumulators,
-// each already as (word index, value x 2^(shift-24) in FP32): the orbit's
-// mass/Tint and the field's fixed-point scale are folded into one FP32 factor
-// per field class when the orbit starts.  The drain rounds each item to one
+// FP32 variant.  A lane parks one record per grid node that leaves its
+// accumulators: the node's word index and its five sums already scaled by
+// value x 2^(shift-24) in FP32 (the orbit's mass/Tint and the field's
+// fixed-point scale are folded into one FP32 factor per field class when the
+// orbit starts).  The drain rounds each item to one
 // signed 64-bit fixed-point word, X = round(scaled value), and adds it to the
 // high word of the bin (the low word stays zero, so fx_value reads it
 // unchanged).  shift - 24 is chosen so that no bin can overflow 2^62; the
@@ -50,23 +51,28 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
 // form's tolerance, and one atomic per value instead of two halves the L2
 // atomic traffic.
 struct WarpQueue32 {
-  int2 item[32 * 20];  // {fixed-point word index, __float_as_int(scaled value)}, packed
-  int n;               // items parked since the last drain
+  int base[32 * 4];      // word of the node's mass field; field f is base + f * Ngrid
+  float val[32 * 4][5];  // the node's five sums, scaled to fixed point
+  int n;                 // records parked since the last drain
 };
 
-// a lane reserves room for `count` items; returns the first index
+// a lane reserves room for `count` node records; returns the first index
 __device__ __forceinline__ int queue32_reserve(WarpQueue32 &q, int count) { return atomicAdd(&q.n, count); }
 
-// all 32 lanes call this at the same point of the loop
-__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, FxWord *fx)
+// all 32 lanes call this at the same point of the loop; each lane adds the
+// five words of one parked node record at a time
+__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, FxWord *fx, int G)
 {
   __syncwarp();
   const int lane = threadIdx.x & 31;
-  const int items = q.n;
-  for(int it = lane; it < items; it += 32) {
-    const int2 e = q.item[it];
-    const long long X = __float2ll_rn(__int_as_float(e.y));
-    if(X) atomicAdd(&fx[e.x].hi, (unsigned long long) X);
+  const int records = q.n;
+  for(int r = lane; r < records; r += 32) {
+    const int b = q.base[r];
+#pragma unroll
+    for(int f = 0; f < 5; f++) {
+      const long long X = __float2ll_rn(q.val[r][f]);
+      if(X) atomicAdd(&fx[b + f * G].hi, (unsigned long long) X);
+    }
   }
   __syncwarp();
   if(lane == 0) q.n = 0;

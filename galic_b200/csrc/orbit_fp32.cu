@@ -238,22 +238,24 @@ struct Sink32 : NodeAcc {
   bool parked;
   __device__ __forceinline__ void park_masked(const bool out[4])
   {
+    // a node with no mass has no deposit at all (every field is weight x ...)
+    bool rec[4];
     int n = 0;
 #pragma unroll
-    for(int s = 0; s < 4; s++)
-#pragma unroll
-      for(int f = 0; f < 5; f++) n += (out[s] && a[s][f] != 0.f) ? 1 : 0;
+    for(int s = 0; s < 4; s++) {
+      rec[s] = out[s] && a[s][0] != 0.f;
+      n += rec[s] ? 1 : 0;
+    }
     if(n == 0) return;
     int at = queue32_reserve(*q, n);
 #pragma unroll
     for(int s = 0; s < 4; s++) {
-      if(!out[s]) continue;
-      const int node = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
+      if(!rec[s]) continue;
+      q->base[at] = gbase + (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
+      q->val[at][0] = a[s][0] * scale_m;
 #pragma unroll
-      for(int f = 0; f < 5; f++) {
-        const float v = a[s][f];
-        if(v != 0.f) q->item[at++] = make_int2(gbase + f * G + node, __float_as_int(v * (f == 0 ? scale_m : scale_e)));
-      }
+      for(int f = 1; f < 5; f++) q->val[at][f] = a[s][f] * scale_e;
+      at++;
     }
     parked = true;
   }
@@ -545,7 +547,7 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
   int state = begin() ? LANE_ACTIVE : LANE_DONE;
   for(;;) {
     if(__any_sync(0xffffffffu, sink.parked)) {
-      warp_drain32(*sink.q, S.fx);
+      warp_drain32(*sink.q, S.fx, G);
       sink.parked = false;
     }
     if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
