@@ -631,7 +631,7 @@ int enqueue_orbits(galic_ctx *ctx, int form, int first, int stride, int *launche
   a.steps_total = ctx->d_counters + 8;
   a.max_egy_err = ctx->d_maxerr;
   a.status = ctx->d_status;
-  const int block = form == GALIC_FORM_FP32 ? 256 : 128;
+  const int block = form == GALIC_FORM_FP32 ? CALC_ALL_BLOCK_FP32 : CALC_ALL_BLOCK_FP64;
   int per_sm = form == GALIC_FORM_FP32 ? calc_all_fp32_occupancy(block) : calc_all_occupancy(block);
   if(per_sm < 1) per_sm = 1;
   int sms = 148;

@@ -54,6 +54,8 @@ struct WarpQueue32 {
   int base[32 * 4];      // word of the node's mass field; field f is base + f * Ngrid
   float val[32 * 4][5];  // the node's five sums, scaled to fixed point
   int n;                 // records parked since the last drain
+  int gbase[32];         // per lane: first word of its orbit's grid set
+  float2 scale[32];      // per lane: {mass field, energy fields} fixed-point factors
 };
 
 // a lane reserves room for `count` node records; returns the first index

@@ -16,12 +16,12 @@ enum { F_M = 0, F_R = 1, F_T = 2, F_Q = 3, F_P = 4, NF_ORBIT = 5 };
 enum { NG_COMMITTED = 10 };
 // threads per CTA of the persistent orbit kernels
 #define CALC_ALL_BLOCK_FP64 128
-#define CALC_ALL_BLOCK_FP32 256
+#define CALC_ALL_BLOCK_FP32 128
 #ifndef GALIC_FP64_MIN_BLOCKS
 #define GALIC_FP64_MIN_BLOCKS 3
 #endif
 #ifndef GALIC_FP32_MIN_BLOCKS
-#define GALIC_FP32_MIN_BLOCKS 2
+#define GALIC_FP32_MIN_BLOCKS 5
 #endif
 // target stacks per type: DGs_MassTarget, EGs_MassTarget, EGs_EgyTarget_{r,t,p,q}
 enum { T_DGM = 0, T_EGM = 1, T_R = 2, T_T = 3, T_P = 4, T_Q = 5, NT_TARGET = 6 };

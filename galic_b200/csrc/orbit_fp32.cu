@@ -232,10 +232,16 @@ struct NodeAcc {
 // together (flush.cuh).
 struct Sink32 : NodeAcc {
   WarpQueue32 *q;
-  int lane, Nb, G;
-  int gbase;                // first word of the orbit's grid set: gridset * NG_COMMITTED * G
-  float scale_m, scale_e;   // mass/Tint x 2^(shift-24) of the mass and energy fields
+  int lane, Nb;
   bool parked;
+  // the orbit's first word (grid set x NG_COMMITTED x Ngrid) and the scale
+  // factors mass/Tint x 2^(shift-24) of the mass and energy fields, kept in
+  // the lane's queue header (read only when parking)
+  __device__ __forceinline__ void set_orbit(int gbase, float scale_m, float scale_e)
+  {
+    q->gbase[lane] = gbase;
+    q->scale[lane] = make_float2(scale_m, scale_e);
+  }
   __device__ __forceinline__ void park_masked(const bool out[4])
   {
     // a node with no mass has no deposit at all (every field is weight x ...)
@@ -248,13 +254,15 @@ struct Sink32 : NodeAcc {
     }
     if(n == 0) return;
     int at = queue32_reserve(*q, n);
+    const int gbase = q->gbase[lane];
+    const float2 sc = q->scale[lane];
 #pragma unroll
     for(int s = 0; s < 4; s++) {
       if(!rec[s]) continue;
       q->base[at] = gbase + (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
-      q->val[at][0] = a[s][0] * scale_m;
+      q->val[at][0] = a[s][0] * sc.x;
 #pragma unroll
-      for(int f = 1; f < 5; f++) q->val[at][f] = a[s][f] * scale_e;
+      for(int f = 1; f < 5; f++) q->val[at][f] = a[s][f] * sc.y;
       at++;
     }
     parked = true;
@@ -290,7 +298,7 @@ struct Sink32 : NodeAcc {
 
 struct State32 {
   float x[3], v[3], a[3];
-  double tall, timespan, E0;
+  double tall, timespan;
   int iR, iz;
   float fR, fz, radsign_prev;
   float pend;    // weight of the deferred end-of-step deposit
@@ -479,6 +487,14 @@ struct EnsembleSrc {
   }
 };
 
+// per-lane values used only when an orbit starts or ends (shared memory)
+struct LaneAux {
+  double E0;                // energy at the orbit start (orbit_response.c:203)
+  double err;               // largest relative energy error of the lane's orbits of model stat_mi
+  unsigned long long steps; // their orbit-steps
+  int status, stat_mi, p;
+};
+
 // log(FG_Fac) for the FP64 potential of the energy check (grid.c:68-74)
 __device__ __forceinline__ LogConsts pot_logs(const DevModel &M)
 {
@@ -492,33 +508,38 @@ template <int BLOCK, class Src>
 __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
 {
   __shared__ WarpQueue32 queues[BLOCK / 32];
+  // values a lane needs only when an orbit starts or ends, out of registers
+  __shared__ LaneAux aux_all[BLOCK];
+  LaneAux &aux = aux_all[threadIdx.x];
   if((threadIdx.x & 31) == 0) queues[threadIdx.x >> 5].n = 0;
+  aux.p = -1;
+  aux.stat_mi = 0;
+  aux.steps = 0;
+  aux.err = 0;
+  aux.status = 0;
   __syncwarp();
   const int G = S.model64(0).DG_Ngrid;
   State32 s;
   Sink32 sink;
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
-  sink.G = G;
   sink.cur = -1;
   sink.parked = false;
-  int p = -1, mi = 0, stat_mi = 0;
-  unsigned long long my_steps = 0;
-  double my_err = 0;
-  int my_status = 0;
+  int mi = 0;
 
   auto begin = [&]() -> bool {
-    int nmi;
+    int nmi, p;
     if(!S.take(nmi, p)) {
-      p = -1;
+      aux.p = -1;
       return false;
     }
-    if(nmi != stat_mi) {  // statistics are kept per model
-      S.flush_stats(stat_mi, my_steps, my_err, my_status);
-      my_steps = 0;
-      my_err = 0;
-      my_status = 0;
-      stat_mi = nmi;
+    aux.p = p;
+    if(nmi != aux.stat_mi) {  // statistics are kept per model
+      S.flush_stats(aux.stat_mi, aux.steps, aux.err, aux.status);
+      aux.steps = 0;
+      aux.err = 0;
+      aux.status = 0;
+      aux.stat_mi = nmi;
     }
     mi = nmi;
     const Model32 &M = S.model(mi);
@@ -528,9 +549,8 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
     {
       const int gs = S.gridset(mi, type);
       const double fac = P.mass[p] / P.tint[p];
-      sink.gbase = gs * NG_COMMITTED * G;
-      sink.scale_m = (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_MASS_S] - 24);
-      sink.scale_e = (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_R_S] - 24);
+      sink.set_orbit(gs * NG_COMMITTED * G, (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_MASS_S] - 24),
+                     (float) ldexp(fac, S.shift[gs * NG_COMMITTED + GALIC_GRID_R_S] - 24));
     }
     sink.cur = -1;
     double xd[3], vd[3];
@@ -540,7 +560,7 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
     }
     orbit32_init(M, s, xd, vd, type, P.tint[p]);
     const DevModel &M64 = S.model64(mi);
-    s.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, pot_logs(M64), xd);
+    aux.E0 = 0.5 * (vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]) + forcegrid_pot(M64, pot_logs(M64), xd);
     return true;
   };
 
@@ -555,22 +575,22 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
       if(!orbit32_step(S.model(mi), s, sink)) state = LANE_FINISH;
     } else if(state == LANE_FINISH) {
       sink.park();
-      S.particles(mi).orbits[p] = s.norbit;
-      my_steps += (unsigned long long) s.steps;
+      S.particles(mi).orbits[aux.p] = s.norbit;
+      aux.steps += (unsigned long long) s.steps;
       if(s.status != ORBIT_OK)
-        my_status = max(my_status, s.status);
+        aux.status = max(aux.status, s.status);
       else {
         const DevModel &M64 = S.model64(mi);
         double xd[3] = {s.x[0], s.x[1], s.x[2]};
         double vd0 = s.v[0], vd1 = s.v[1], vd2 = s.v[2];
         double E1 = 0.5 * (vd0 * vd0 + vd1 * vd1 + vd2 * vd2) + forcegrid_pot(M64, pot_logs(M64), xd);
-        double e = fabs((E1 - s.E0) / s.E0);
-        if(e > my_err) my_err = e;
+        double e = fabs((E1 - aux.E0) / aux.E0);
+        if(e > aux.err) aux.err = e;
       }
       state = begin() ? LANE_ACTIVE : LANE_DONE;
     }
   }
-  S.flush_stats(stat_mi, my_steps, my_err, my_status);
+  S.flush_stats(aux.stat_mi, aux.steps, aux.err, aux.status);
 }
 
 __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP32, GALIC_FP32_MIN_BLOCKS)
@@ -703,7 +723,7 @@ Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const flo
 struct Variant {
   int block, min_blocks;
 };
-constexpr Variant kVariants[] = {{256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}, {128, 5}};
+constexpr Variant kVariants[] = {{128, 5}, {256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <int V>
