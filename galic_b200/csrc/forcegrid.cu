@@ -13,14 +13,16 @@
 //  * the oct-tree (forcetree.c:139-495) is the set of cubes that belong to the
 //    top-level domain tree (domain_toplevel.c:18-171: the root and every cube
 //    holding more than a fraction 1/(TopNodeFactor*MultipleDomains) of all
-//    points, probes included, are split) or contain at least two mass
-//    particles.  It is laid out in depth-first order with children in Morton
-//    order (x bit 0, y bit 1, z bit 2), which is the reference's threaded
-//    nextnode/sibling order (forcetree.c:591-722): the first child of item i
-//    is item i+1 and `skip` is the item after i's subtree;
-//  * node moments are summed over the children in that order
-//    (forcetree.c:622-690; force_treeupdate_toplevel forcetree.c:817-890
-//    recomputes the top nodes with the same sums);
+//    points, probes included, are split; built on the host, a few hundred
+//    cubes) or contain at least two mass particles (built on the GPU from the
+//    particles' Morton order).  It is laid out in depth-first order with
+//    children in Morton order (x bit 0, y bit 1, z bit 2), which is the
+//    reference's threaded nextnode/sibling order (forcetree.c:591-722): the
+//    first child of item i is item i+1 and `skip` is the item after i's
+//    subtree;
+//  * node moments are summed over the children in that order, one level at a
+//    time from the deepest (forcetree.c:622-690; force_treeupdate_toplevel
+//    forcetree.c:817-890 recomputes the top nodes with the same sums);
 //  * the walk (forcetree_walk.c:12-222) opens a node when
 //    (float) len*len > r2*theta*theta, with the side length held as a float
 //    (allvars.h:1096), and uses the reference's spline-softened kernel;
@@ -193,6 +195,7 @@ __global__ void __launch_bounds__(kWalkBlock) k_walk(const FillItem *__restrict_
       }
     }
     next = it.skip < 0 ? 0xFFFFFFFFu : (unsigned) it.skip;
+    if(next <= cur) next = 0xFFFFFFFFu;  // skips always point forward; never loop
     const double mass = it.mass;
     if(mass != 0.0) {
       n_int++;
@@ -271,115 +274,272 @@ __global__ void k_readout(int NN, int np, const int *__restrict__ rank, const do
   out[2 * NN + cell] = p / kSections;
 }
 
-// ------------------------------------------------------------------ host tree
+// ------------------------------------------------------------- tree on the GPU
+//
+// The oct-tree below the top-level tree is built from the mass particles in
+// Morton order.  Particle k's Morton key holds the digits
+// x_bit | y_bit << 1 | z_bit << 2 of levels 1..31 of its 52-bit coordinates
+// (levels 1..21 in `hi`, 22..31 in `lo`).  With lam[k] the number of leading
+// levels particles k and k+1 share, the cubes holding >= 2 particles that
+// start at particle k are the levels in (max(lam[k-1], L), lam[k]], L the
+// level of the particle's top leaf; they precede particle k's leaf item in
+// the depth-first order, shallowest first.  So every item's position follows
+// from a prefix sum, and a node's `skip` is the first item of the first
+// particle after its cube.
 
-struct TreeBuilder {
-  const unsigned long long *ix, *iy, *iz;  // 52-bit coordinates of the mass particles
-  const double *pos, *mass;
-  const unsigned long long *keys;          // sorted keys of all points
+constexpr int kTreeLevels = kMaxTreeLevel + 1;  // a cube of this level with two particles is refused
+
+__global__ void k_morton(int n, const double *__restrict__ pos, double cx, double cy, double cz, double inv_len,
+                         unsigned long long *__restrict__ hi, unsigned long long *__restrict__ lo,
+                         int *__restrict__ idx)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const unsigned long long x = int_coord(pos[3 * (size_t) i + 0], cx, inv_len);
+  const unsigned long long y = int_coord(pos[3 * (size_t) i + 1], cy, inv_len);
+  const unsigned long long z = int_coord(pos[3 * (size_t) i + 2], cz, inv_len);
+  unsigned long long h = 0, l = 0;
+  for(int lev = 1; lev <= kTreeLevels; lev++) {
+    const int b = 52 - lev;
+    const unsigned long long d = ((x >> b) & 1) | (((y >> b) & 1) << 1) | (((z >> b) & 1) << 2);
+    if(lev <= kBits)
+      h = (h << 3) | d;
+    else
+      l = (l << 3) | d;
+  }
+  hi[i] = h;
+  lo[i] = l;
+  idx[i] = i;
+}
+
+template <class T>
+__global__ void k_gather(int n, const T *__restrict__ src, const int *__restrict__ idx, T *__restrict__ dst)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k < n) dst[k] = src[idx[k]];
+}
+
+// levels shared by particles k and k+1 (kTreeLevels: identical keys)
+__device__ __forceinline__ int shared_levels(unsigned long long h0, unsigned long long l0, unsigned long long h1,
+                                             unsigned long long l1)
+{
+  if(h0 != h1) return (__clzll((long long) (h0 ^ h1)) - 1) / 3;
+  if(l0 != l1) return kBits + (__clzll((long long) (l0 ^ l1)) - (64 - 3 * (kTreeLevels - kBits))) / 3;
+  return kTreeLevels;
+}
+
+// top leaf of each particle (leaves sorted by their first Morton key), the
+// nodes that start at it and its item count; flags a level-31 pair
+__global__ void k_particle_nodes(int n, const unsigned long long *__restrict__ hi, const unsigned long long *__restrict__ lo,
+                                 int nleaves, const unsigned long long *__restrict__ leaf_start,
+                                 const int *__restrict__ leaf_level, int *__restrict__ leaf_of, int *__restrict__ lo_lev,
+                                 int *__restrict__ nitem, int *__restrict__ too_deep)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= n) return;
+  const unsigned long long h = hi[k];
+  int a = 0, b = nleaves;  // last leaf whose start <= h
+  while(b - a > 1) {
+    const int m = (a + b) >> 1;
+    if(leaf_start[m] <= h)
+      a = m;
+    else
+      b = m;
+  }
+  const int L = leaf_level[a];
+  const int next = (k + 1 < n) ? shared_levels(h, lo[k], hi[k + 1], lo[k + 1]) : -1;
+  const int prev = (k > 0) ? shared_levels(hi[k - 1], lo[k - 1], h, lo[k]) : -1;
+  if(next >= kTreeLevels) *too_deep = 1;
+  const int lo_l = max(prev, L);
+  const int c = next > lo_l ? next - lo_l : 0;  // next > L implies k+1 is in the same leaf
+  leaf_of[k] = a;
+  lo_lev[k] = lo_l;
+  nitem[k] = c + 1;
+}
+
+// first item offset (exclusive scan) of each top leaf's first particle and
+// the end offset of its last particle
+__global__ void k_leaf_ranges(int n, const int *__restrict__ leaf_of, const int *__restrict__ off,
+                              const int *__restrict__ nitem, int *__restrict__ leaf_first, int *__restrict__ leaf_off0,
+                              int *__restrict__ leaf_off1)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= n) return;
+  const int T = leaf_of[k];
+  if(k == 0 || leaf_of[k - 1] != T) {
+    leaf_first[T] = k;
+    leaf_off0[T] = off[k];
+  }
+  if(k == n - 1 || leaf_of[k + 1] != T) leaf_off1[T] = off[k] + nitem[k];
+}
+
+// the items of particle k: its nodes (levels lo_lev+1 .. lo_lev+c) and its leaf
+__global__ void k_particle_items(int n, int nitems, double dom_len, const unsigned long long *__restrict__ hi,
+                                 const unsigned long long *__restrict__ lo, const int *__restrict__ sorted,
+                                 const double *__restrict__ pos, const double *__restrict__ mass,
+                                 const int *__restrict__ leaf_of, const int *__restrict__ lo_lev,
+                                 const int *__restrict__ nitem, const int *__restrict__ off,
+                                 const int *__restrict__ leaf_item, const int *__restrict__ leaf_skip,
+                                 const int *__restrict__ leaf_off0, FillItem *__restrict__ items)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k >= n) return;
+  const int T = leaf_of[k];
+  const int first_item = leaf_item[T] + 1 - leaf_off0[T];  // item of offset o is first_item + o
+  const int base = first_item + off[k];
+  const int c = nitem[k] - 1;
+  const int p = sorted[k];
+  const unsigned long long h = hi[k], l = lo[k];
+  for(int j = 0; j < c; j++) {
+    const int lev = lo_lev[k] + 1 + j;
+    // end of the cube: first particle after k outside it (binary search in
+    // the particles of the same leaf, which follow k in Morton order)
+    int a = k, b = n;  // a inside, b outside
+    while(b - a > 1) {
+      const int m = (a + b) >> 1;
+      const bool inside = leaf_of[m] == T && shared_levels(h, l, hi[m], lo[m]) >= lev;
+      if(inside)
+        a = m;
+      else
+        b = m;
+    }
+    const int g = b;
+    const int skip = (g < n && leaf_of[g] == T) ? first_item + off[g] : leaf_skip[T];
+    FillItem it;
+    it.x = pos[3 * (size_t) p + 0];  // replaced by the centre of mass (the node holds >= 2 particles)
+    it.y = pos[3 * (size_t) p + 1];
+    it.z = pos[3 * (size_t) p + 2];
+    it.mass = 0;
+    it.len = (float) ldexp(dom_len, -lev);
+    it.skip = skip < nitems ? skip : -1;
+    it.pad[0] = lev;
+    it.pad[1] = 0;
+    items[base + j] = it;
+  }
+  FillItem leaf;
+  leaf.x = pos[3 * (size_t) p + 0];
+  leaf.y = pos[3 * (size_t) p + 1];
+  leaf.z = pos[3 * (size_t) p + 2];
+  leaf.mass = mass[p];
+  leaf.len = -1.f;
+  leaf.skip = base + c + 1 < nitems ? base + c + 1 : -1;
+  leaf.pad[0] = -1;
+  leaf.pad[1] = 0;
+  items[base + c] = leaf;
+}
+
+__global__ void k_scatter_items(int count, const int *__restrict__ at, const FillItem *__restrict__ src,
+                                FillItem *__restrict__ items)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if(k < count) items[at[k]] = src[k];
+}
+
+// force_update_node_recursive (forcetree.c:622-690) for the nodes of one
+// level: mass and centre of mass summed over the daughters in Morton order
+// (the daughters follow the node, linked by their skips); a node without
+// mass keeps the centre it was written with
+__global__ void k_moments(int nitems, int level, FillItem *__restrict__ items)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= nitems || items[i].pad[0] != level) return;
+  const int end = items[i].skip < 0 ? nitems : items[i].skip;
+  double m = 0, s0 = 0, s1 = 0, s2 = 0;
+  for(int c = i + 1; c < end;) {
+    const FillItem d = items[c];
+    m += d.mass;
+    s0 += d.mass * d.x;
+    s1 += d.mass * d.y;
+    s2 += d.mass * d.z;
+    const int nx = (d.len < 0.f) ? c + 1 : (d.skip < 0 ? nitems : d.skip);
+    c = nx > c ? nx : nitems;  // skips always point forward; never loop
+  }
+  if(m) {
+    items[i].x = s0 / m;
+    items[i].y = s1 / m;
+    items[i].z = s2 / m;
+  }
+  items[i].mass = m;
+}
+
+// ------------------------------------------------------------------ host: top tree
+//
+// domain_determineTopTree / domain_do_local_refine (domain_toplevel.c:18-190)
+// with one rank: the root is split; a cube is split when it holds more than
+// 1/(TopNodeFactor * MultipleDomains) of all points (probes included) and is
+// above level 21.  Cubes are enumerated depth first with daughters in Morton
+// order; their float centres follow force_create_empty_nodes
+// (forcetree.c:543-547).
+
+struct TopCube {
+  int level;
+  bool refined;
+  unsigned long long mort;  // Morton prefix of `level` digits
+  float centre[3];
+  float len;
+  int item = 0, skip = 0, size = 0;  // set once the leaves' particle items are known
+  int leaf = -1;                     // index among the leaves
+};
+
+struct TopTree {
+  const unsigned long long *keys;  // sorted Peano-Hilbert keys of all points
   size_t nkeys;
   double fac_load, limit, len;
   const PhTables *ph;
-  std::vector<FillItem> items;
-  std::vector<int> scratch;
-  bool too_deep = false;
+  std::vector<TopCube> cubes;
 
-  // number of points whose key starts with the level-`level` prefix
   size_t count_prefix(unsigned long long prefix, int level) const
   {
     const int sh = 3 * (kBits - level);
     const unsigned long long lo = prefix << sh, hi = (prefix + 1) << sh;
-    const unsigned long long *a = std::lower_bound(keys, keys + nkeys, lo);
-    const unsigned long long *b = (level == 0) ? keys + nkeys : std::lower_bound(keys, keys + nkeys, hi);
-    return (size_t) (b - a);
+    return (size_t) (std::lower_bound(keys, keys + nkeys, hi) - std::lower_bound(keys, keys + nkeys, lo));
   }
 
-  // Node for the cube at `level` with coordinate prefix (x52, y52, z52) that
-  // holds the mass particles list[0..cnt).  `top`: the cube is a node of the
-  // top-level tree, with Peano-Hilbert prefix `php` and curve state `rot`;
-  // centre: its float centre (forcetree.c:543-547), the node's position when
-  // it holds no mass (forcetree.c:684-689).
-  void build(int level, int *list, int cnt, unsigned long long x52, unsigned long long y52, unsigned long long z52,
-             const float centre[3], bool top, int rot, unsigned long long php)
+  void build(int level, unsigned long long mort, const float centre[3], int rot, unsigned long long php)
   {
-    const int me = (int) items.size();
-    items.push_back(FillItem{});
-    FillItem node{};
-    node.len = (float) (len * std::ldexp(1.0, -level));
-    if(level >= 52) {  // coincident particles: unreachable below MAX_TREE_LEVEL
-      too_deep = true;
-      node.skip = (int) items.size();
-      items[me] = node;
-      return;
-    }
-    const bool refined =
-        top && (level == 0 || (level < kBits && fac_load * (double) count_prefix(php, level) > limit));
-    const int bit = 51 - level;
-    int count[8] = {0, 0, 0, 0, 0, 0, 0, 0}, start[9];
-    auto digit = [&](int p) {
-      return (int) (((ix[p] >> bit) & 1) | (((iy[p] >> bit) & 1) << 1) | (((iz[p] >> bit) & 1) << 2));
-    };
-    for(int k = 0; k < cnt; k++) count[digit(list[k])]++;
-    start[0] = 0;
-    for(int d = 0; d < 8; d++) start[d + 1] = start[d] + count[d];
-    if(cnt > 1) {
-      int fill[8];
-      for(int d = 0; d < 8; d++) fill[d] = start[d];
-      std::copy(list, list + cnt, scratch.begin());
-      for(int k = 0; k < cnt; k++) list[fill[digit(scratch[k])]++] = scratch[k];
-    }
-    const double lenhalf = 0.25 * (double) node.len;
-    double m = 0, s[3] = {0, 0, 0};
+    const int me = (int) cubes.size();
+    TopCube c;
+    c.level = level;
+    c.mort = mort;
+    c.len = (float) (len * std::ldexp(1.0, -level));
+    for(int j = 0; j < 3; j++) c.centre[j] = centre[j];
+    c.refined = level == 0 || (level < kBits && fac_load * (double) count_prefix(php, level) > limit);
+    cubes.push_back(c);
+    if(!c.refined) return;
+    const double lenhalf = 0.25 * (double) c.len;
     for(int d = 0; d < 8; d++) {
-      const int n = count[d];
-      if(refined || n >= 2) {
-        if(!refined && level + 1 > kMaxTreeLevel) too_deep = true;
-        const int xb = d & 1, yb = (d >> 1) & 1, zb = (d >> 2) & 1;
-        const int pix = (xb << 2) | (yb << 1) | zb;
-        float cc[3];
-        cc[0] = (float) (centre[0] + (2 * xb - 1) * lenhalf);
-        cc[1] = (float) (centre[1] + (2 * yb - 1) * lenhalf);
-        cc[2] = (float) (centre[2] + (2 * zb - 1) * lenhalf);
-        const int child = (int) items.size();
-        build(level + 1, list + start[d], n, x52 | ((unsigned long long) xb << bit),
-              y52 | ((unsigned long long) yb << bit), z52 | ((unsigned long long) zb << bit), cc, refined,
-              ph->rot[rot][pix], (php << 3) | ph->sub[rot][pix]);
-        const FillItem &c = items[child];
-        m += c.mass;
-        s[0] += c.mass * c.x;
-        s[1] += c.mass * c.y;
-        s[2] += c.mass * c.z;
-      } else if(n == 1) {
-        const int p = list[start[d]];
-        FillItem leaf{};
-        leaf.x = pos[3 * (size_t) p + 0];
-        leaf.y = pos[3 * (size_t) p + 1];
-        leaf.z = pos[3 * (size_t) p + 2];
-        leaf.mass = mass[p];
-        leaf.len = -1.f;
-        leaf.skip = (int) items.size() + 1;
-        items.push_back(leaf);
-        m += leaf.mass;
-        s[0] += leaf.mass * leaf.x;
-        s[1] += leaf.mass * leaf.y;
-        s[2] += leaf.mass * leaf.z;
+      const int xb = d & 1, yb = (d >> 1) & 1, zb = (d >> 2) & 1;
+      const int pix = (xb << 2) | (yb << 1) | zb;
+      float cc[3];
+      cc[0] = (float) (cubes[me].centre[0] + (2 * xb - 1) * lenhalf);
+      cc[1] = (float) (cubes[me].centre[1] + (2 * yb - 1) * lenhalf);
+      cc[2] = (float) (cubes[me].centre[2] + (2 * zb - 1) * lenhalf);
+      build(level + 1, (mort << 3) | (unsigned long long) d, cc, ph->rot[rot][pix], (php << 3) | ph->sub[rot][pix]);
+    }
+  }
+
+  // item index, subtree size and skip of every cube, given each leaf's
+  // particle item count; returns the item count of the whole tree
+  int layout(const std::vector<int> &leaf_items)
+  {
+    int next = 0;
+    // depth-first order = the order of `cubes`; a cube's subtree ends where
+    // the next cube of its level or shallower starts
+    for(auto &c : cubes) {
+      c.item = next++;
+      if(!c.refined) next += leaf_items[c.leaf];
+    }
+    const int total = next;
+    std::vector<int> stack;  // open cubes
+    for(int i = 0; i < (int) cubes.size(); i++) {
+      while(!stack.empty() && cubes[stack.back()].level >= cubes[i].level) {
+        cubes[stack.back()].skip = cubes[i].item;
+        stack.pop_back();
       }
+      stack.push_back(i);
     }
-    if(m) {
-      s[0] /= m;
-      s[1] /= m;
-      s[2] /= m;
-    } else {
-      s[0] = centre[0];
-      s[1] = centre[1];
-      s[2] = centre[2];
-    }
-    node.x = s[0];
-    node.y = s[1];
-    node.z = s[2];
-    node.mass = m;
-    node.skip = (int) items.size();
-    items[me] = node;
+    for(int i : stack) cubes[i].skip = total;
+    return total;
   }
 };
 
@@ -494,37 +654,120 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cudaMemcpy(keys.data(), d_key2.p, (size_t) ntot * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   FCK(cudaMemcpy(order.data(), d_idx2.p, (size_t) ntot * sizeof(int), cudaMemcpyDeviceToHost));
 
-  // oct-tree of the mass particles (forcetree.c:139-722)
-  std::vector<unsigned long long> ix(n), iy(n), iz(n);
-  for(int i = 0; i < n; i++) {
-    ix[i] = int_coord(pos[3 * (size_t) i + 0], corner[0], inv_len);
-    iy[i] = int_coord(pos[3 * (size_t) i + 1], corner[1], inv_len);
-    iz[i] = int_coord(pos[3 * (size_t) i + 2], corner[2], inv_len);
-  }
-  TreeBuilder tb;
-  tb.ix = ix.data();
-  tb.iy = iy.data();
-  tb.iz = iz.data();
-  tb.pos = pos;
-  tb.mass = mass;
-  tb.keys = keys.data();
-  tb.nkeys = keys.size();
-  tb.fac_load = 1.0 / (double) ntot;                              // domain.c:149
-  tb.limit = 1.0 / (fp->TopNodeFactor * fp->MultipleDomains * 1);  // one rank
-  tb.len = len;
-  tb.ph = &host_tables();
-  tb.scratch.resize(n);
-  tb.items.reserve(2 * (size_t) n + 64);
+  // top-level tree (host, a few hundred cubes) from the sorted keys
+  TopTree tt;
+  tt.keys = keys.data();
+  tt.nkeys = keys.size();
+  tt.fac_load = 1.0 / (double) ntot;                              // domain.c:149
+  tt.limit = 1.0 / (fp->TopNodeFactor * fp->MultipleDomains * 1);  // one rank
+  tt.len = len;
+  tt.ph = &host_tables();
   {
-    std::vector<int> list(n);
-    for(int i = 0; i < n; i++) list[i] = i;
     const float c0[3] = {(float) centre[0], (float) centre[1], (float) centre[2]};
-    tb.build(0, list.data(), n, 0, 0, 0, c0, true, 0, 0);
+    tt.build(0, 0, c0, 0, 0);
   }
-  if(tb.too_deep) return GALIC_ERR_UNSUPPORTED;
-  const int nitems = (int) tb.items.size();
-  for(auto &it : tb.items)
-    if(it.skip >= nitems) it.skip = -1;
+  std::vector<unsigned long long> leaf_start;
+  std::vector<int> leaf_level;
+  for(auto &c : tt.cubes)
+    if(!c.refined) {
+      c.leaf = (int) leaf_start.size();
+      leaf_start.push_back(c.mort << (63 - 3 * c.level));
+      leaf_level.push_back(c.level);
+    }
+  const int nleaves = (int) leaf_start.size();
+
+  // oct-tree of the mass particles below the top leaves (forcetree.c:139-722),
+  // built on the GPU from their Morton order
+  DevBuf d_mass, d_hi, d_lo, d_hi2, d_lo2, d_pidx, d_pidx2, d_pidx3, d_lstart, d_llevel, d_leaf_of, d_lolev, d_nitem,
+      d_off, d_flag, d_loff0, d_loff1, d_lfirst, d_litem, d_lskip, d_tmp2;
+  const int TB = 256, TG = (n + TB - 1) / TB;
+  FCK(cudaMalloc(&d_mass.p, (size_t) n * sizeof(double)));
+  FCK(cudaMemcpy(d_mass.p, mass, (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
+  for(DevBuf *b : {&d_hi, &d_lo, &d_hi2, &d_lo2}) FCK(cudaMalloc(&b->p, (size_t) n * sizeof(unsigned long long)));
+  for(DevBuf *b : {&d_pidx, &d_pidx2, &d_pidx3, &d_leaf_of, &d_lolev, &d_nitem, &d_off})
+    FCK(cudaMalloc(&b->p, (size_t) n * sizeof(int)));
+  FCK(cudaMalloc(&d_lstart.p, nleaves * sizeof(unsigned long long)));
+  FCK(cudaMalloc(&d_llevel.p, nleaves * sizeof(int)));
+  for(DevBuf *b : {&d_loff0, &d_loff1, &d_lfirst, &d_litem, &d_lskip}) FCK(cudaMalloc(&b->p, nleaves * sizeof(int)));
+  FCK(cudaMalloc(&d_flag.p, sizeof(int)));
+  FCK(cudaMemset(d_flag.p, 0, sizeof(int)));
+  FCK(cudaMemset(d_loff0.p, 0, nleaves * sizeof(int)));
+  FCK(cudaMemset(d_loff1.p, 0, nleaves * sizeof(int)));
+  FCK(cudaMemcpy(d_lstart.p, leaf_start.data(), nleaves * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_llevel.p, leaf_level.data(), nleaves * sizeof(int), cudaMemcpyHostToDevice));
+  k_morton<<<TG, TB>>>(n, d_pos.as<double>(), corner[0], corner[1], corner[2], inv_len,
+                       d_hi.as<unsigned long long>(), d_lo.as<unsigned long long>(), d_pidx.as<int>());
+  FCK(cudaGetLastError());
+  {
+    // Morton order: stable sorts by the low digits, then by the high digits
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    FCK(cub::DeviceRadixSort::SortPairs(nullptr, b1, d_lo.as<unsigned long long>(), d_lo2.as<unsigned long long>(),
+                                        d_pidx.as<int>(), d_pidx2.as<int>(), n, 0, 3 * (kTreeLevels - kBits)));
+    FCK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_hi2.as<unsigned long long>(), d_hi.as<unsigned long long>(),
+                                        d_pidx2.as<int>(), d_pidx3.as<int>(), n, 0, 3 * kBits));
+    FCK(cub::DeviceScan::ExclusiveSum(nullptr, b3, d_nitem.as<int>(), d_off.as<int>(), n));
+    FCK(cudaMalloc(&d_tmp2.p, std::max(b1, std::max(b2, b3))));
+    size_t bb = b1;
+    FCK(cub::DeviceRadixSort::SortPairs(d_tmp2.p, bb, d_lo.as<unsigned long long>(), d_lo2.as<unsigned long long>(),
+                                        d_pidx.as<int>(), d_pidx2.as<int>(), n, 0, 3 * (kTreeLevels - kBits)));
+    k_gather<<<TG, TB>>>(n, d_hi.as<unsigned long long>(), d_pidx2.as<int>(), d_hi2.as<unsigned long long>());
+    bb = b2;
+    FCK(cub::DeviceRadixSort::SortPairs(d_tmp2.p, bb, d_hi2.as<unsigned long long>(), d_hi.as<unsigned long long>(),
+                                        d_pidx2.as<int>(), d_pidx3.as<int>(), n, 0, 3 * kBits));
+    // d_hi: high digits in Morton order; the low digits follow them
+    k_gather<<<TG, TB>>>(n, d_lo.as<unsigned long long>(), d_pidx3.as<int>(), d_lo2.as<unsigned long long>());
+    k_particle_nodes<<<TG, TB>>>(n, d_hi.as<unsigned long long>(), d_lo2.as<unsigned long long>(), nleaves,
+                                 d_lstart.as<unsigned long long>(), d_llevel.as<int>(), d_leaf_of.as<int>(),
+                                 d_lolev.as<int>(), d_nitem.as<int>(), d_flag.as<int>());
+    bb = b3;
+    FCK(cub::DeviceScan::ExclusiveSum(d_tmp2.p, bb, d_nitem.as<int>(), d_off.as<int>(), n));
+    k_leaf_ranges<<<TG, TB>>>(n, d_leaf_of.as<int>(), d_off.as<int>(), d_nitem.as<int>(), d_lfirst.as<int>(),
+                              d_loff0.as<int>(), d_loff1.as<int>());
+    FCK(cudaGetLastError());
+  }
+  int too_deep = 0;
+  FCK(cudaMemcpy(&too_deep, d_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if(too_deep) return GALIC_ERR_UNSUPPORTED;  // particles closer than DomainLen / 2^30
+  std::vector<int> loff0(nleaves), loff1(nleaves), leaf_items(nleaves);
+  FCK(cudaMemcpy(loff0.data(), d_loff0.p, nleaves * sizeof(int), cudaMemcpyDeviceToHost));
+  FCK(cudaMemcpy(loff1.data(), d_loff1.p, nleaves * sizeof(int), cudaMemcpyDeviceToHost));
+  for(int T = 0; T < nleaves; T++) leaf_items[T] = loff1[T] - loff0[T];
+  const int nitems = tt.layout(leaf_items);
+  std::vector<int> litem(nleaves), lskip(nleaves), at;
+  std::vector<FillItem> top_items;
+  for(const auto &c : tt.cubes) {
+    if(!c.refined) {
+      litem[c.leaf] = c.item;
+      lskip[c.leaf] = c.skip;
+    }
+    FillItem it{};
+    it.x = c.centre[0];
+    it.y = c.centre[1];
+    it.z = c.centre[2];
+    it.mass = 0;
+    it.len = c.len;
+    it.skip = c.skip < nitems ? c.skip : -1;
+    it.pad[0] = c.level;
+    top_items.push_back(it);
+    at.push_back(c.item);
+  }
+  DevBuf d_items, d_top, d_at;
+  FCK(cudaMalloc(&d_items.p, (size_t) nitems * sizeof(FillItem)));
+  FCK(cudaMalloc(&d_top.p, top_items.size() * sizeof(FillItem)));
+  FCK(cudaMalloc(&d_at.p, at.size() * sizeof(int)));
+  FCK(cudaMemcpy(d_top.p, top_items.data(), top_items.size() * sizeof(FillItem), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_at.p, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_litem.p, litem.data(), nleaves * sizeof(int), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_lskip.p, lskip.data(), nleaves * sizeof(int), cudaMemcpyHostToDevice));
+  k_scatter_items<<<((int) at.size() + 127) / 128, 128>>>((int) at.size(), d_at.as<int>(), d_top.as<FillItem>(),
+                                                          d_items.as<FillItem>());
+  k_particle_items<<<TG, TB>>>(n, nitems, len, d_hi.as<unsigned long long>(), d_lo2.as<unsigned long long>(),
+                               d_pidx3.as<int>(), d_pos.as<double>(), d_mass.as<double>(), d_leaf_of.as<int>(),
+                               d_lolev.as<int>(), d_nitem.as<int>(), d_off.as<int>(), d_litem.as<int>(),
+                               d_lskip.as<int>(), d_loff0.as<int>(), d_items.as<FillItem>());
+  for(int lev = kTreeLevels - 1; lev >= 0; lev--)
+    k_moments<<<(nitems + 255) / 256, 256>>>(nitems, lev, d_items.as<FillItem>());
+  FCK(cudaGetLastError());
 
   // probes in key order (SoA) and the key-order rank of each probe
   std::vector<double> probes(3 * (size_t) np);
@@ -536,8 +779,7 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     for(int j = 0; j < 3; j++) probes[(size_t) j * np + t] = P[3 * ((size_t) n + id) + j];
     t++;
   }
-  DevBuf d_items, d_probes, d_res, d_rank, d_trig, d_out, d_counts;
-  FCK(cudaMalloc(&d_items.p, (size_t) nitems * sizeof(FillItem)));
+  DevBuf d_probes, d_res, d_rank, d_trig, d_out, d_counts;
   FCK(cudaMalloc(&d_probes.p, 3 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_res.p, 4 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_rank.p, (size_t) np * sizeof(int)));
@@ -545,7 +787,6 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cudaMalloc(&d_out.p, 3 * (size_t) NN * sizeof(double)));
   FCK(cudaMalloc(&d_counts.p, 2 * sizeof(unsigned long long)));
   FCK(cudaMemset(d_counts.p, 0, 2 * sizeof(unsigned long long)));
-  FCK(cudaMemcpy(d_items.p, tb.items.data(), (size_t) nitems * sizeof(FillItem), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_probes.p, probes.data(), 3 * (size_t) np * sizeof(double), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_rank.p, rank.data(), (size_t) np * sizeof(int), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_trig.p, trig, sizeof(trig), cudaMemcpyHostToDevice));
