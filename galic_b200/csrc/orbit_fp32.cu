@@ -51,23 +51,17 @@ struct Cell32 {
 
 __device__ __forceinline__ Cell32 cell32(float br, float bz, int nbin, float bmax)
 {
+  // (grid.c:20-55 / 494-534) inside the grid: bin = floor, fraction = rest;
+  // beyond its last node: bin = nbin - 2, fraction 1 (branch-free)
   Cell32 c;
   br = fmaxf(br, 0.f);
   bz = fmaxf(bz, 0.f);
-  int binr = (br < bmax) ? (int) br : nbin - 1;
-  int binz = (bz < bmax) ? (int) bz : nbin - 1;
-  c.fR = br - (float) binr;
-  c.fz = bz - (float) binz;
-  if(binr >= nbin - 1) {
-    binr = nbin - 2;
-    c.fR = 1.f;
-  }
-  if(binz >= nbin - 1) {
-    binz = nbin - 2;
-    c.fz = 1.f;
-  }
-  c.iR = binr;
-  c.iz = binz;
+  const bool in_r = br < bmax, in_z = bz < bmax;
+  const float fbr = floorf(br), fbz = floorf(bz);
+  c.iR = in_r ? (int) fbr : nbin - 2;
+  c.iz = in_z ? (int) fbz : nbin - 2;
+  c.fR = in_r ? br - fbr : 1.f;
+  c.fz = in_z ? bz - fbz : 1.f;
   return c;
 }
 
@@ -183,10 +177,20 @@ struct NodeAcc {
   // slots whose node is not a node of cell (iz, iR)
   __device__ __forceinline__ void leaving(int iR, int iz, bool out[4]) const
   {
+    // along one axis a move by d leaves the node whose parity is that of the
+    // boundary left behind (d = +1: the lower node, d = -1: the upper one),
+    // both nodes when |d| > 1, none when d = 0
+    const int dz = iz - cur_iz, dr = iR - cur_iR;
+    const int bz = (dz > 0 ? cur_iz : cur_iz + 1) & 1, br = (dr > 0 ? cur_iR : cur_iR + 1) & 1;
+    const bool zall = dz > 1 || dz < -1, rall = dr > 1 || dr < -1;
+    bool lz[2], lr[2];
 #pragma unroll
-    for(int s = 0; s < 4; s++)
-      out[s] = (cur_iz + node_dz(s, cur_iz) != iz + node_dz(s, iz)) ||
-               (cur_iR + node_dr(s, cur_iR) != iR + node_dr(s, iR));
+    for(int b = 0; b < 2; b++) {
+      lz[b] = zall || (dz != 0 && b == bz);
+      lr[b] = rall || (dr != 0 && b == br);
+    }
+#pragma unroll
+    for(int s = 0; s < 4; s++) out[s] = lz[s >> 1] || lr[s & 1];
   }
   __device__ __forceinline__ void clear(const bool which[4])
   {
@@ -197,24 +201,12 @@ struct NodeAcc {
   }
   __device__ __forceinline__ void accumulate(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
   {
-    // corner weights, then permuted from corners c to slots s = c ^ parity
-    float w[4] = {hdt * (1.f - fR) * (1.f - fz), hdt * fR * (1.f - fz), hdt * (1.f - fR) * fz, hdt * fR * fz};
-    if(iR & 1) {
-      float t = w[0];
-      w[0] = w[1];
-      w[1] = t;
-      t = w[2];
-      w[2] = w[3];
-      w[3] = t;
-    }
-    if(iz & 1) {
-      float t = w[0];
-      w[0] = w[2];
-      w[2] = t;
-      t = w[1];
-      w[1] = w[3];
-      w[3] = t;
-    }
+    // weights in slot order: slot s holds corner (dz, dr) = ((s >> 1) ^ (iz & 1), (s & 1) ^ (iR & 1))
+    const bool oz = iz & 1, orr = iR & 1;
+    const float z0 = oz ? fz : 1.f - fz, z1 = oz ? 1.f - fz : fz;
+    const float r0 = orr ? fR : 1.f - fR, r1 = orr ? 1.f - fR : fR;
+    const float hz0 = hdt * z0, hz1 = hdt * z1;
+    const float w[4] = {hz0 * r0, hz0 * r1, hz1 * r0, hz1 * r1};
 #pragma unroll
     for(int k = 0; k < 4; k++) {
       a[k][0] += w[k];
