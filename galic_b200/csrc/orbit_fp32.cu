@@ -294,7 +294,7 @@ struct State32 {
   int iR, iz;
   float fR, fz, radsign_prev;
   float pend;    // weight of the deferred end-of-step deposit
-  int cs_cell;   // DG cell whose size is cached in cs_val
+  int cs_cell;   // DG cell whose size is in cs_val (the current cell)
   float cs_val;
   Proj32 proj;
   int norbit, flag, type, tovs, steps, status;
@@ -327,7 +327,8 @@ __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const
   s.fR = c.fR;
   s.fz = c.fz;
   s.proj = project32(s.tovs, s.x, s.v, vstr);
-  s.cs_cell = -1;
+  s.cs_cell = s.iz * M.DG_Nbin + s.iR;
+  s.cs_val = __ldg(&M.cellsize[s.cs_cell]);
   s.pend = 0.f;
 }
 
@@ -343,11 +344,6 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   const float vv = sqrtf(s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
   const float aa = sqrtf(s.a[0] * s.a[0] + s.a[1] * s.a[1] + s.a[2] * s.a[2]);
   const float t1 = M.f_orb * M.V200 * frcp(aa);
-  const int dgc = s.iz * M.DG_Nbin + s.iR;
-  if(dgc != s.cs_cell) {
-    s.cs_cell = dgc;
-    s.cs_val = __ldg(&M.cellsize[dgc]);
-  }
   const float t2 = M.f_cc * s.cs_val * frcp(vv);
   double dt = (double) fminf(t1, t2);
   if(s.timespan < dt + s.tall) {
@@ -370,6 +366,15 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   s.iz = c.iz;
   s.fR = c.fR;
   s.fz = c.fz;
+  {
+    // DG_CellSize of the new cell for the next step's time step, loaded now
+    // so that its latency overlaps the rest of this step
+    const int dgc = s.iz * M.DG_Nbin + s.iR;
+    if(dgc != s.cs_cell) {
+      s.cs_cell = dgc;
+      s.cs_val = __ldg(&M.cellsize[dgc]);
+    }
+  }
   s.proj = project32(s.tovs, s.x, s.v, vstr);
   s.pend = hdt;
   s.tall += dt;
