@@ -462,6 +462,105 @@ __global__ void k_moments(int nitems, int level, FillItem *__restrict__ items)
   items[i].mass = m;
 }
 
+// ------------------------------------------------------------- point set on the GPU
+
+// probe points of grid.c:680-704 from the host's r1[j], z1[k], cos/sin of the
+// section angles (glibc values): one IEEE product per coordinate, as there
+__global__ void k_probe_points(int n, int N, const double *__restrict__ r1, const double *__restrict__ z1,
+                               const double *__restrict__ trig, double *__restrict__ pos)
+{
+  const int NN = N * N;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if(q >= kSections * NN) return;
+  const int sct = q / NN, rem = q - sct * NN, k = rem / N, j = rem - k * N;
+  double *P = pos + 3 * ((size_t) n + q);
+  P[0] = r1[j] * trig[sct];
+  P[1] = r1[j] * trig[kSections + sct];
+  P[2] = z1[k];
+}
+
+// per-block minimum and maximum of each axis (domain_box.c:27-39); the host
+// finishes the reduction.  Extremes are order independent (a +0/-0 tie
+// leaves the length, centre and corner unchanged).
+__global__ void __launch_bounds__(256) k_extent(int ntot, const double *__restrict__ pos, double *__restrict__ part)
+{
+  __shared__ double sh[6][256];
+  double mn[3] = {1e306, 1e306, 1e306}, mx[3] = {-1e306, -1e306, -1e306};
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x)
+#pragma unroll
+    for(int j = 0; j < 3; j++) {
+      const double v = pos[3 * (size_t) i + j];
+      if(mn[j] > v) mn[j] = v;
+      if(mx[j] < v) mx[j] = v;
+    }
+#pragma unroll
+  for(int j = 0; j < 3; j++) {
+    sh[j][threadIdx.x] = mn[j];
+    sh[3 + j][threadIdx.x] = mx[j];
+  }
+  __syncthreads();
+  for(int h = 128; h > 0; h >>= 1) {
+    if(threadIdx.x < h)
+#pragma unroll
+      for(int j = 0; j < 3; j++) {
+        if(sh[j][threadIdx.x] > sh[j][threadIdx.x + h]) sh[j][threadIdx.x] = sh[j][threadIdx.x + h];
+        if(sh[3 + j][threadIdx.x] < sh[3 + j][threadIdx.x + h]) sh[3 + j][threadIdx.x] = sh[3 + j][threadIdx.x + h];
+      }
+    __syncthreads();
+  }
+  if(threadIdx.x < 6) part[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// number of points whose key lies in each queried cube (Peano-Hilbert
+// prefix of `level` digits), by binary search in the sorted keys
+__global__ void k_count_prefix(int nq, const unsigned long long *__restrict__ prefix, const int *__restrict__ level,
+                               const unsigned long long *__restrict__ keys, int nkeys, int *__restrict__ count)
+{
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if(q >= nq) return;
+  const int sh = 3 * (kBits - level[q]);
+  const unsigned long long lo = prefix[q] << sh, hi = (prefix[q] + 1) << sh;
+  int a = 0, b = nkeys;
+  while(a < b) {
+    const int m = (a + b) >> 1;
+    if(keys[m] < lo)
+      a = m + 1;
+    else
+      b = m;
+  }
+  int c = a, d = nkeys;
+  while(c < d) {
+    const int m = (c + d) >> 1;
+    if(keys[m] < hi)
+      c = m + 1;
+    else
+      d = m;
+  }
+  count[q] = c - a;
+}
+
+// probes in key order (SoA) and the key-order rank of every probe; before[r]
+// is the number of probes at sorted positions below r
+__global__ void k_probe_order(int ntot, int n, int np, const int *__restrict__ order, const int *__restrict__ before,
+                              const double *__restrict__ pos, double *__restrict__ probes, int *__restrict__ rank)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if(r >= ntot) return;
+  const int i = order[r];
+  if(i < n) return;
+  const int t = before[r];
+  rank[i - n] = t;
+  probes[t] = pos[3 * (size_t) i + 0];
+  probes[np + t] = pos[3 * (size_t) i + 1];
+  probes[2 * (size_t) np + t] = pos[3 * (size_t) i + 2];
+}
+
+__global__ void k_is_probe(int ntot, int n, const int *__restrict__ order, int *__restrict__ flag)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if(r < ntot) flag[r] = order[r] >= n ? 1 : 0;
+}
+
 // ------------------------------------------------------------------ host: top tree
 //
 // domain_determineTopTree / domain_do_local_refine (domain_toplevel.c:18-190)
@@ -482,40 +581,87 @@ struct TopCube {
 };
 
 struct TopTree {
-  const unsigned long long *keys;  // sorted Peano-Hilbert keys of all points
-  size_t nkeys;
   double fac_load, limit, len;
   const PhTables *ph;
-  std::vector<TopCube> cubes;
+  std::vector<TopCube> cubes;  // depth-first order
 
-  size_t count_prefix(unsigned long long prefix, int level) const
+  // counts(prefixes, levels) -> point counts of those cubes.  Cubes are
+  // created level by level (a cube's split depends only on its own count)
+  // and then listed depth first.
+  template <class Counts>
+  int build(const float centre0[3], Counts counts)
   {
-    const int sh = 3 * (kBits - level);
-    const unsigned long long lo = prefix << sh, hi = (prefix + 1) << sh;
-    return (size_t) (std::lower_bound(keys, keys + nkeys, hi) - std::lower_bound(keys, keys + nkeys, lo));
-  }
-
-  void build(int level, unsigned long long mort, const float centre[3], int rot, unsigned long long php)
-  {
-    const int me = (int) cubes.size();
-    TopCube c;
-    c.level = level;
-    c.mort = mort;
-    c.len = (float) (len * std::ldexp(1.0, -level));
-    for(int j = 0; j < 3; j++) c.centre[j] = centre[j];
-    c.refined = level == 0 || (level < kBits && fac_load * (double) count_prefix(php, level) > limit);
-    cubes.push_back(c);
-    if(!c.refined) return;
-    const double lenhalf = 0.25 * (double) c.len;
-    for(int d = 0; d < 8; d++) {
-      const int xb = d & 1, yb = (d >> 1) & 1, zb = (d >> 2) & 1;
-      const int pix = (xb << 2) | (yb << 1) | zb;
-      float cc[3];
-      cc[0] = (float) (cubes[me].centre[0] + (2 * xb - 1) * lenhalf);
-      cc[1] = (float) (cubes[me].centre[1] + (2 * yb - 1) * lenhalf);
-      cc[2] = (float) (cubes[me].centre[2] + (2 * zb - 1) * lenhalf);
-      build(level + 1, (mort << 3) | (unsigned long long) d, cc, ph->rot[rot][pix], (php << 3) | ph->sub[rot][pix]);
+    struct Node {
+      TopCube c;
+      int rot;
+      unsigned long long php;
+      int child0 = -1;  // first of 8 daughters in Morton order
+    };
+    std::vector<Node> all(1);
+    all[0].c.level = 0;
+    all[0].c.mort = 0;
+    all[0].c.len = (float) len;
+    for(int j = 0; j < 3; j++) all[0].c.centre[j] = centre0[j];
+    all[0].c.refined = true;  // the root is always split (domain_toplevel.c:43-46)
+    all[0].rot = 0;
+    all[0].php = 0;
+    std::vector<int> frontier{0};
+    while(!frontier.empty()) {
+      std::vector<int> fresh;
+      for(int f : frontier) {
+        all[f].child0 = (int) all.size();
+        const Node par = all[f];
+        const double lenhalf = 0.25 * (double) par.c.len;
+        for(int d = 0; d < 8; d++) {
+          const int xb = d & 1, yb = (d >> 1) & 1, zb = (d >> 2) & 1;
+          const int pix = (xb << 2) | (yb << 1) | zb;
+          Node ch;
+          ch.c.level = par.c.level + 1;
+          ch.c.mort = (par.c.mort << 3) | (unsigned long long) d;
+          ch.c.len = (float) (len * std::ldexp(1.0, -ch.c.level));
+          ch.c.centre[0] = (float) (par.c.centre[0] + (2 * xb - 1) * lenhalf);
+          ch.c.centre[1] = (float) (par.c.centre[1] + (2 * yb - 1) * lenhalf);
+          ch.c.centre[2] = (float) (par.c.centre[2] + (2 * zb - 1) * lenhalf);
+          ch.c.refined = false;
+          ch.rot = ph->rot[par.rot][pix];
+          ch.php = (par.php << 3) | ph->sub[par.rot][pix];
+          fresh.push_back((int) all.size());
+          all.push_back(ch);
+        }
+      }
+      // a daughter is split when fac_load * Count > limit and it can be
+      // (domain_toplevel.c:146-178)
+      std::vector<unsigned long long> pre;
+      std::vector<int> lev, idx;
+      for(int k : fresh)
+        if(all[k].c.level < kBits) {
+          pre.push_back(all[k].php);
+          lev.push_back(all[k].c.level);
+          idx.push_back(k);
+        }
+      std::vector<int> cnt(pre.size(), 0);
+      if(!pre.empty()) {
+        const int st = counts(pre, lev, cnt);
+        if(st) return st;
+      }
+      frontier.clear();
+      for(size_t q = 0; q < idx.size(); q++)
+        if(fac_load * (double) cnt[q] > limit) {
+          all[idx[q]].c.refined = true;
+          frontier.push_back(idx[q]);
+        }
     }
+    // depth-first listing, daughters in Morton order
+    cubes.clear();
+    std::vector<int> stack{0};
+    while(!stack.empty()) {
+      const int k = stack.back();
+      stack.pop_back();
+      cubes.push_back(all[k].c);
+      if(all[k].c.refined)
+        for(int d = 7; d >= 0; d--) stack.push_back(all[k].child0 + d);
+    }
+    return 0;
   }
 
   // item index, subtree size and skip of every cube, given each leaf's
@@ -587,9 +733,8 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   const int N = fp->FG_Nbin, NN = N * N, np = NN * kSections, ntot = n + np;
 
   // probe points (grid.c:680-704), in the reference's point order: mass
-  // particles, then s, k (z), j (R)
-  std::vector<double> P(3 * (size_t) ntot);
-  std::memcpy(P.data(), pos, 3 * (size_t) n * sizeof(double));
+  // particles, then s, k (z), j (R); the glibc values r1[j], z1[k] and the
+  // section angles' cos/sin come from the host, the products from the GPU
   std::vector<double> r1(N), z1(N);
   for(int j = 0; j < N; j++) r1[j] = fp->FG_Rmin * (std::pow(fp->FG_Fac, j) - 1.0);
   for(int k = 0; k < N; k++) z1[k] = fp->FG_Rmin * (std::pow(fp->FG_Fac, k) - 1.0);
@@ -598,21 +743,34 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     const double phi = 2 * M_PI / kSections * s;
     trig[s] = std::cos(phi);
     trig[kSections + s] = std::sin(phi);
-    for(int k = 0; k < N; k++)
-      for(int j = 0; j < N; j++) {
-        const size_t q = (size_t) n + (size_t) s * NN + (size_t) k * N + j;
-        P[3 * q + 0] = r1[j] * trig[s];
-        P[3 * q + 1] = r1[j] * trig[kSections + s];
-        P[3 * q + 2] = z1[k];
-      }
   }
+  if(!upload_tables()) {
+    fprintf(stderr, "galic_cuda: Peano-Hilbert table upload failed\n");
+    return GALIC_ERR_CUDA;
+  }
+  DevBuf d_pos, d_key, d_key2, d_idx, d_idx2, d_tmp, d_r1, d_z1, d_trig, d_part;
+  FCK(cudaMalloc(&d_pos.p, 3 * (size_t) ntot * sizeof(double)));
+  FCK(cudaMalloc(&d_r1.p, N * sizeof(double)));
+  FCK(cudaMalloc(&d_z1.p, N * sizeof(double)));
+  FCK(cudaMalloc(&d_trig.p, sizeof(trig)));
+  FCK(cudaMemcpy(d_pos.p, pos, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_r1.p, r1.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_z1.p, z1.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  FCK(cudaMemcpy(d_trig.p, trig, sizeof(trig), cudaMemcpyHostToDevice));
+  k_probe_points<<<(np + 255) / 256, 256>>>(n, N, d_r1.as<double>(), d_z1.as<double>(), d_trig.as<double>(),
+                                            d_pos.as<double>());
+  FCK(cudaGetLastError());
   // domain_findExtent (domain_box.c:20-65)
+  const int EB = 592;
+  FCK(cudaMalloc(&d_part.p, 6 * EB * sizeof(double)));
+  k_extent<<<EB, 256>>>(ntot, d_pos.as<double>(), d_part.as<double>());
+  std::vector<double> part(6 * EB);
+  FCK(cudaMemcpy(part.data(), d_part.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
   double xmin[3] = {1e306, 1e306, 1e306}, xmax[3] = {-1e306, -1e306, -1e306};
-  for(size_t i = 0; i < (size_t) ntot; i++)
+  for(int b = 0; b < EB; b++)
     for(int j = 0; j < 3; j++) {
-      const double v = P[3 * i + j];
-      if(xmin[j] > v) xmin[j] = v;
-      if(xmax[j] < v) xmax[j] = v;
+      if(xmin[j] > part[6 * b + j]) xmin[j] = part[6 * b + j];
+      if(xmax[j] < part[6 * b + 3 + j]) xmax[j] = part[6 * b + 3 + j];
     }
   double len = 0;
   for(int j = 0; j < 3; j++)
@@ -626,18 +784,11 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   const double inv_len = 1.0 / len;
   if(!(len > 0) || !std::isfinite(inv_len)) return GALIC_ERR_INVALID_ARGUMENT;
 
-  if(!upload_tables()) {
-    fprintf(stderr, "galic_cuda: Peano-Hilbert table upload failed\n");
-    return GALIC_ERR_CUDA;
-  }
   // keys of all points and their stable key order (peano.c:63-104)
-  DevBuf d_pos, d_key, d_key2, d_idx, d_idx2, d_tmp;
-  FCK(cudaMalloc(&d_pos.p, 3 * (size_t) ntot * sizeof(double)));
   FCK(cudaMalloc(&d_key.p, (size_t) ntot * sizeof(unsigned long long)));
   FCK(cudaMalloc(&d_key2.p, (size_t) ntot * sizeof(unsigned long long)));
   FCK(cudaMalloc(&d_idx.p, (size_t) ntot * sizeof(int)));
   FCK(cudaMalloc(&d_idx2.p, (size_t) ntot * sizeof(int)));
-  FCK(cudaMemcpy(d_pos.p, P.data(), 3 * (size_t) ntot * sizeof(double), cudaMemcpyHostToDevice));
   k_keys<<<(ntot + 255) / 256, 256>>>(ntot, d_pos.as<double>(), corner[0], corner[1], corner[2], inv_len,
                                       d_key.as<unsigned long long>(), d_idx.as<int>());
   FCK(cudaGetLastError());
@@ -649,22 +800,40 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cub::DeviceRadixSort::SortPairs(d_tmp.p, tmp_bytes, d_key.as<unsigned long long>(),
                                       d_key2.as<unsigned long long>(), d_idx.as<int>(), d_idx2.as<int>(), ntot, 0,
                                       3 * kBits));
-  std::vector<unsigned long long> keys(ntot);
-  std::vector<int> order(ntot);
-  FCK(cudaMemcpy(keys.data(), d_key2.p, (size_t) ntot * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-  FCK(cudaMemcpy(order.data(), d_idx2.p, (size_t) ntot * sizeof(int), cudaMemcpyDeviceToHost));
 
-  // top-level tree (host, a few hundred cubes) from the sorted keys
+  // top-level tree (host, a few hundred cubes; counts from the sorted keys)
   TopTree tt;
-  tt.keys = keys.data();
-  tt.nkeys = keys.size();
   tt.fac_load = 1.0 / (double) ntot;                              // domain.c:149
   tt.limit = 1.0 / (fp->TopNodeFactor * fp->MultipleDomains * 1);  // one rank
   tt.len = len;
   tt.ph = &host_tables();
   {
+    DevBuf d_qp, d_ql, d_qc;
+    size_t cap = 0;
+    auto counts = [&](const std::vector<unsigned long long> &pre, const std::vector<int> &lev,
+                      std::vector<int> &cnt) -> int {
+      const size_t nq = pre.size();
+      if(nq > cap) {
+        cudaFree(d_qp.p);
+        cudaFree(d_ql.p);
+        cudaFree(d_qc.p);
+        d_qp.p = d_ql.p = d_qc.p = nullptr;
+        cap = std::max<size_t>(nq, 4096);
+        FCK(cudaMalloc(&d_qp.p, cap * sizeof(unsigned long long)));
+        FCK(cudaMalloc(&d_ql.p, cap * sizeof(int)));
+        FCK(cudaMalloc(&d_qc.p, cap * sizeof(int)));
+      }
+      FCK(cudaMemcpy(d_qp.p, pre.data(), nq * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+      FCK(cudaMemcpy(d_ql.p, lev.data(), nq * sizeof(int), cudaMemcpyHostToDevice));
+      k_count_prefix<<<((int) nq + 127) / 128, 128>>>((int) nq, d_qp.as<unsigned long long>(), d_ql.as<int>(),
+                                                      d_key2.as<unsigned long long>(), ntot, d_qc.as<int>());
+      FCK(cudaGetLastError());
+      FCK(cudaMemcpy(cnt.data(), d_qc.p, nq * sizeof(int), cudaMemcpyDeviceToHost));
+      return 0;
+    };
     const float c0[3] = {(float) centre[0], (float) centre[1], (float) centre[2]};
-    tt.build(0, 0, c0, 0, 0);
+    const int st = tt.build(c0, counts);
+    if(st) return st;
   }
   std::vector<unsigned long long> leaf_start;
   std::vector<int> leaf_level;
@@ -770,26 +939,26 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cudaGetLastError());
 
   // probes in key order (SoA) and the key-order rank of each probe
-  std::vector<double> probes(3 * (size_t) np);
-  std::vector<int> rank(np);
-  for(int r = 0, t = 0; r < ntot; r++) {
-    const int id = order[r] - n;
-    if(id < 0) continue;
-    rank[id] = t;
-    for(int j = 0; j < 3; j++) probes[(size_t) j * np + t] = P[3 * ((size_t) n + id) + j];
-    t++;
-  }
-  DevBuf d_probes, d_res, d_rank, d_trig, d_out, d_counts;
+  DevBuf d_probes, d_res, d_rank, d_out, d_counts, d_flag2, d_before;
   FCK(cudaMalloc(&d_probes.p, 3 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_res.p, 4 * (size_t) np * sizeof(double)));
   FCK(cudaMalloc(&d_rank.p, (size_t) np * sizeof(int)));
-  FCK(cudaMalloc(&d_trig.p, sizeof(trig)));
   FCK(cudaMalloc(&d_out.p, 3 * (size_t) NN * sizeof(double)));
+  FCK(cudaMalloc(&d_flag2.p, (size_t) ntot * sizeof(int)));
+  FCK(cudaMalloc(&d_before.p, (size_t) ntot * sizeof(int)));
+  k_is_probe<<<(ntot + 255) / 256, 256>>>(ntot, n, d_idx2.as<int>(), d_flag2.as<int>());
+  {
+    size_t b = 0;
+    FCK(cub::DeviceScan::ExclusiveSum(nullptr, b, d_flag2.as<int>(), d_before.as<int>(), ntot));
+    DevBuf d_t3;
+    FCK(cudaMalloc(&d_t3.p, b));
+    FCK(cub::DeviceScan::ExclusiveSum(d_t3.p, b, d_flag2.as<int>(), d_before.as<int>(), ntot));
+  }
+  k_probe_order<<<(ntot + 255) / 256, 256>>>(ntot, n, np, d_idx2.as<int>(), d_before.as<int>(), d_pos.as<double>(),
+                                             d_probes.as<double>(), d_rank.as<int>());
+  FCK(cudaGetLastError());
   FCK(cudaMalloc(&d_counts.p, 2 * sizeof(unsigned long long)));
   FCK(cudaMemset(d_counts.p, 0, 2 * sizeof(unsigned long long)));
-  FCK(cudaMemcpy(d_probes.p, probes.data(), 3 * (size_t) np * sizeof(double), cudaMemcpyHostToDevice));
-  FCK(cudaMemcpy(d_rank.p, rank.data(), (size_t) np * sizeof(int), cudaMemcpyHostToDevice));
-  FCK(cudaMemcpy(d_trig.p, trig, sizeof(trig), cudaMemcpyHostToDevice));
 
   cudaEvent_t e0, e1;
   FCK(cudaEventCreate(&e0));
