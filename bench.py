@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
     ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
+    ap.add_argument("--serve-workers", type=int, default=4, help="concurrent jobs of the serving loop")
     return ap.parse_args()
 
 
@@ -238,7 +239,7 @@ def serving_requests(count, seed, scale):
     return out
 
 
-def measure_serving(count, mean_gap, scale, torch):
+def measure_serving(count, mean_gap, scale, torch, workers=4):
     """Poisson stream of model-construction jobs through the serving loop:
     admission by HBM budget, concurrent jobs on one GPU, per-job
     time-to-convergence (submit to done)."""
@@ -251,7 +252,7 @@ def measure_serving(count, mean_gap, scale, torch):
     free, total = torch.cuda.mem_get_info()
     budget = int(0.5 * free)
     schedule = dict(form=GALIC_FORM_FP32, max_iterations=2, reps_per_iteration=5, fraction_per_rep=0.001)
-    with Server(budget, workers=8) as srv:
+    with Server(budget, workers=workers) as srv:
         t0 = time.perf_counter()
         ids = []
         for k, m in enumerate(models):
@@ -271,7 +272,8 @@ def measure_serving(count, mean_gap, scale, torch):
                          "fraction_per_rep": 0.001, "reps": "fp32 orbits, fp64 merit"},
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "makespan_s": makespan, "orbit_steps": int(steps), "orbit_steps_per_s": steps / makespan,
-            "hbm_budget_bytes": budget, "peak_bytes": st["peak_bytes"], "peak_concurrent_jobs": st["peak_running"]}
+            "hbm_budget_bytes": budget, "peak_bytes": st["peak_bytes"], "peak_concurrent_jobs": st["peak_running"],
+            "workers": workers}
 
 
 def cpu_model():
@@ -520,7 +522,7 @@ def ours_arm(args, rank, world, local_rank):
         fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
-        serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch)
+        serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         cpu = None
