@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
     ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
-    ap.add_argument("--serve-workers", type=int, default=4, help="concurrent jobs of the serving loop")
+    ap.add_argument("--serve-workers", type=int, default=16, help="concurrent jobs of the serving loop")
     return ap.parse_args()
 
 
@@ -239,7 +239,7 @@ def serving_requests(count, seed, scale):
     return out
 
 
-def measure_serving(count, mean_gap, scale, torch, workers=4):
+def measure_serving(count, mean_gap, scale, torch, workers=16):
     """Poisson stream of model-construction jobs through the serving loop:
     admission by HBM budget, concurrent jobs on one GPU, per-job
     time-to-convergence (submit to done)."""

@@ -83,6 +83,22 @@ cudaError_t keep_pool_memory(int device)
 
 int stack_size(int L) { return ((1 << (2 + 2 * L)) - 1) / 3; }
 
+// pinned staging area of at least `bytes` (null on failure)
+char *stage(galic_ctx *ctx, size_t bytes)
+{
+  if(bytes <= ctx->stage_cap) return ctx->h_stage;
+  if(ctx->h_stage) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFreeHost(ctx->h_stage);
+  }
+  ctx->h_stage = nullptr;
+  ctx->stage_cap = 0;
+  const size_t cap = std::max<size_t>(bytes, 4096);
+  if(cudaMallocHost((void **) &ctx->h_stage, cap) != cudaSuccess) return nullptr;
+  ctx->stage_cap = cap;
+  return ctx->h_stage;
+}
+
 int check_params(const galic_params_t *p)
 {
   if(!p) return GALIC_ERR_INVALID_ARGUMENT;
@@ -359,7 +375,11 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx, ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
     if(ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
-  if(ctx->stream) cudaStreamDestroy(ctx->stream);
+  if(ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  if(ctx->h_stage) cudaFreeHost(ctx->h_stage);
   delete ctx;
 }
 
@@ -668,16 +688,21 @@ int enqueue_finish(galic_ctx *ctx, int *launches)
 int collect(galic_ctx *ctx, int launches, bool with_timing)
 {
   cudaStream_t s = ctx->stream;
-  int status = 0;
-  unsigned long long steps = 0;
-  CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(&steps, ctx->d_counters + 8, sizeof(steps), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(&ctx->last_max_egy_err, ctx->d_maxerr, sizeof(double), cudaMemcpyDeviceToHost, s));
+  char *h = stage(ctx, 32);
+  if(!h) return fail(ctx, GALIC_ERR_CUDA);
+  CK(cudaMemcpyAsync(h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h + 8, ctx->d_counters + 8, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h + 16, ctx->d_maxerr, sizeof(double), cudaMemcpyDeviceToHost, s));
   cudaEvent_t ev_end;
   CK(cudaEventCreate(&ev_end));
   CK(cudaEventRecord(ev_end, s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
+  int status;
+  unsigned long long steps;
+  std::memcpy(&status, h, sizeof(int));
+  std::memcpy(&steps, h + 8, sizeof(steps));
+  std::memcpy(&ctx->last_max_egy_err, h + 16, sizeof(double));
   if(with_timing) {
     float ms_total = 0, ms_orbit = 0;
     CK(cudaEventElapsedTime(&ms_total, ctx->ev[0], ev_end));
@@ -770,7 +795,14 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
   }
   int st = ensure_rep_scratch(ctx, count);
   if(st) return st;
-  CK(cudaMemcpyAsync(ctx->d_idx, idx, count * sizeof(int), cudaMemcpyHostToDevice, s));
+  // staging: idx, then status, per-orbit status and steps
+  const size_t off_st = ((size_t) count * sizeof(int) + 15) & ~(size_t) 15;
+  const size_t off_ost = off_st + 16;
+  const size_t off_steps = (off_ost + 2 * (size_t) count * sizeof(int) + 15) & ~(size_t) 15;
+  char *h = stage(ctx, off_steps + 2 * (size_t) count * sizeof(long long));
+  if(!h) return fail(ctx, GALIC_ERR_CUDA);
+  std::memcpy(h, idx, count * sizeof(int));
+  CK(cudaMemcpyAsync(ctx->d_idx, h, count * sizeof(int), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
   CK(cudaMemsetAsync(ctx->d_b_status, 0, 2 * (size_t) count * sizeof(int), s));
   RepArgs R;
@@ -824,15 +856,16 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
   b.with_egy = 1;
   ctx->last_launches = form == GALIC_FORM_FP32 ? launch_rep(ctx->dm, R, f, b, s, ctx->d_tab32, ctx->d_cellsize32)
                                                : launch_rep(ctx->dm, R, f, b, s);
-  int status = 0;
-  std::vector<int> ost(2 * count);
-  std::vector<long long> steps(2 * count);
-  CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(ost.data(), ctx->d_b_status, 2 * (size_t) count * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(steps.data(), ctx->d_b_steps, 2 * (size_t) count * sizeof(long long), cudaMemcpyDeviceToHost,
+  CK(cudaMemcpyAsync(h + off_st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h + off_ost, ctx->d_b_status, 2 * (size_t) count * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h + off_steps, ctx->d_b_steps, 2 * (size_t) count * sizeof(long long), cudaMemcpyDeviceToHost,
                      s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
+  int status;
+  std::memcpy(&status, h + off_st, sizeof(int));
+  const int *ost = (const int *) (h + off_ost);
+  const long long *steps = (const long long *) (h + off_steps);
   long long tot = 0;
   for(int k = 0; k < 2 * count; k++) {
     tot += steps[k];

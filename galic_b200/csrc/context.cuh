@@ -71,6 +71,10 @@ struct galic_ctx {
   unsigned generation = 0;
   // form of a galic_calc_all_shard awaiting galic_calc_all_finish, else -1
   int shard_form = -1;
+  // pinned staging for the small per-call transfers (asynchronous copies
+  // that do not go through the driver's shared pageable staging)
+  char *h_stage = nullptr;
+  size_t stage_cap = 0;
 };
 
 namespace galic_internal {
