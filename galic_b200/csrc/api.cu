@@ -879,8 +879,11 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
 extern "C" int galic_get_fit(galic_ctx *ctx, double *out)
 {
   if(!ctx || !out) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  char *h = stage(ctx, 4 * 7 * sizeof(double));
+  if(!h) return fail(ctx, GALIC_ERR_CUDA);
+  CK(cudaMemcpyAsync(h, ctx->d_fit, 4 * 7 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpyAsync(out, ctx->d_fit, 4 * 7 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  std::memcpy(out, h, 4 * 7 * sizeof(double));
   return fail(ctx, GALIC_OK);
 }
 
