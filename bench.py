@@ -69,6 +69,9 @@ def build_workload(scale, seed):
 def _cpu_worker(args):
     """Integrates orbits of one chunk with GALIC's own C (or the restatement)."""
     arrays, idx, seconds, kind = args
+    # GALIC's C prints its energy-drift warnings on stdout; this worker's copy
+    # goes to /dev/null so that the bench's stdout stays one JSON line
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     import oracle_lib

@@ -21,7 +21,7 @@ enum { NG_COMMITTED = 10 };
 #define GALIC_FP64_MIN_BLOCKS 3
 #endif
 #ifndef GALIC_FP32_MIN_BLOCKS
-#define GALIC_FP32_MIN_BLOCKS 5
+#define GALIC_FP32_MIN_BLOCKS 4
 #endif
 // target stacks per type: DGs_MassTarget, EGs_MassTarget, EGs_EgyTarget_{r,t,p,q}
 enum { T_DGM = 0, T_EGM = 1, T_R = 2, T_T = 3, T_P = 4, T_Q = 5, NT_TARGET = 6 };

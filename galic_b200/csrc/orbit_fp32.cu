@@ -4,6 +4,9 @@
 // Same algorithm as the FP64 form (orbit_fp64.cu) with these changes, all of
 // which only move results within the stated tolerance of the FP64 oracle:
 //  * positions, velocities, accelerations and the interpolation run in FP32;
+//    position and velocity are carried as compensated sums (Kahan 1965: an
+//    FP32 value plus an FP32 correction term), so the rounding of the many
+//    small kicks and drifts does not build up over an orbit span;
 //    the force grid is read from one "quad" table per particle type: for
 //    every cell the four corners' DPotDR, DPotDz and Vstream[type] (three
 //    float4, one 64-byte line), so a bilinear lookup is one cache line;
@@ -166,11 +169,10 @@ __device__ __forceinline__ Cell32 density_cell32(const Model32 &M, const float *
 // the four nodes of any cell have the four parities, so when the orbit moves
 // to a neighbouring cell the nodes both cells share stay in their slots
 // untouched, and only the slots whose node changes are flushed and cleared.
-// A deposit's corner c = 2 dz + dr of the cell lands in slot c ^ parity(cell).
+// A deposit's corner c = 2 dz + dr of the cell lands in slot c ^ (2 (iz & 1) + (iR & 1)).
 struct NodeAcc {
   int cur = -1, cur_iR = 0, cur_iz = 0;
   float a[4][5];
-  __device__ __forceinline__ int parity() const { return ((cur_iz & 1) << 1) | (cur_iR & 1); }
   // slot s of cell (iz, iR) holds node (iz + node_dz(s, iz), iR + node_dr(s, iR))
   __device__ __forceinline__ static int node_dz(int s, int iz) { return ((s >> 1) ^ iz) & 1; }
   __device__ __forceinline__ static int node_dr(int s, int iR) { return (s ^ iR) & 1; }
@@ -288,8 +290,20 @@ struct Sink32 : NodeAcc {
   }
 };
 
+// Kahan compensated summation (W. Kahan, "Further remarks on reducing
+// truncation errors", CACM 8(1), 1965): adds inc to the sum s whose exact
+// value is s - c; c collects what each rounding of s lost.
+__device__ __forceinline__ void comp_add(float &s, float &c, float inc)
+{
+  const float y = inc - c;
+  const float t = s + y;
+  c = __fsub_rn(__fsub_rn(t, s), y);  // explicit roundings: never contracted
+  s = t;
+}
+
 struct State32 {
   float x[3], v[3], a[3];
+  float xc[3], vc[3];  // compensation of x and v: the exact values are x - xc, v - vc
   double tall, timespan;
   int iR, iz;
   float fR, fz, radsign_prev;
@@ -309,6 +323,8 @@ __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const
   for(int i = 0; i < 3; i++) {
     s.x[i] = (float) xd[i];
     s.v[i] = (float) vd[i];
+    s.xc[i] = (float) ((double) s.x[i] - xd[i]);
+    s.vc[i] = (float) ((double) s.v[i] - vd[i]);
   }
   s.type = type;
   s.tovs = M.tovs[type];
@@ -354,13 +370,13 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   const float fdt = (float) dt;
   sink.add(s.iR, s.iz, hdt + s.pend, s.fR, s.fz, s.proj);
 #pragma unroll
-  for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+  for(int i = 0; i < 3; i++) comp_add(s.v[i], s.vc[i], hdt * s.a[i]);
 #pragma unroll
-  for(int i = 0; i < 3; i++) s.x[i] = fmaf(fdt, s.v[i], s.x[i]);
+  for(int i = 0; i < 3; i++) comp_add(s.x[i], s.xc[i], fdt * (s.v[i] - s.vc[i]));
   float vstr;
   accel32(M, s.type, s.x, s.a, &vstr);
 #pragma unroll
-  for(int i = 0; i < 3; i++) s.v[i] = fmaf(hdt, s.a[i], s.v[i]);
+  for(int i = 0; i < 3; i++) comp_add(s.v[i], s.vc[i], hdt * s.a[i]);
   Cell32 c = density_cell32(M, s.x);
   s.iR = c.iR;
   s.iz = c.iz;
@@ -720,7 +736,7 @@ Model32 make_model32(const DevModel &M64, const float4 *const quad[4], const flo
 struct Variant {
   int block, min_blocks;
 };
-constexpr Variant kVariants[] = {{128, 5}, {256, 2}, {128, 4}, {192, 3}, {256, 3}, {128, 6}};
+constexpr Variant kVariants[] = {{128, 4}, {256, 2}, {128, 5}, {192, 3}, {256, 3}, {128, 3}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <int V>
