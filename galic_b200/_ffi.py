@@ -102,6 +102,17 @@ class GalicJobResult(C.Structure):
     ]
 
 
+class GalicSampleParams(C.Structure):
+    """galic_sample_params_t."""
+    _fields_ = [(n, C.c_double) for n in ("Rmax", "Halo_A", "HaloStretch", "Disk_Z0", "Disk_H", "Bulge_A",
+                                          "BulgeStretch", "HaloBetaParameter", "BulgeBetaParameter")]
+
+
+class GalicStream(C.Structure):
+    """galic_stream_t."""
+    _fields_ = [("seed", C.c_uint64), ("a", C.c_uint32), ("b", C.c_uint32), ("position", C.c_uint64)]
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
@@ -174,6 +185,13 @@ SIGNATURES = [
     ("galic_force_grid_fill", C.c_int,
      [C.POINTER(GalicFillParams), C.c_int, PD, PD, PD, PD, PD, C.POINTER(GalicFillStats)]),
     ("galic_peano_hilbert_key", C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("galic_set_dispersion", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD]),
+    ("galic_sample_density_targets", C.c_int,
+     [VP, C.POINTER(GalicSampleParams), C.c_longlong, C.POINTER(GalicStream), C.c_int]),
+    ("galic_sample_energy_targets", C.c_int, [VP, C.POINTER(GalicSampleParams), C.c_longlong, C.POINTER(GalicStream)]),
+    ("galic_get_targets", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD, PD]),
+    ("galic_sample_positions", C.c_int,
+     [C.POINTER(GalicSampleParams), C.c_int, C.c_longlong, C.POINTER(GalicStream), PD]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),
     ("galic_density_geometry", C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
     ("galic_smooth_stack", None, [PD, C.c_int]),

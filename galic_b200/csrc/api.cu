@@ -27,7 +27,7 @@ const char *kStatusText[] = {"ok",
                              "no CUDA device",
                              "request exceeds the HBM budget",
                              "configuration not supported",
-                             "velocity proposal exceeded 100000 tries",
+                             "rejection loop exceeded its cap (velocity proposal: 100000 tries; sampling: nothing lands inside Rmax)",
                              "fixed-point response bin out of range",
                              "call out of order"};
 
@@ -361,6 +361,8 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   cudaStreamSynchronize(ctx->stream);
   dfree(ctx, ctx->d_fg_acc); dfree(ctx, ctx->d_fg_pot);
   for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_vstream[t]);
+  for(int t = 0; t < 4; t++)
+    for(int k = 0; k < 5; k++) dfree(ctx, ctx->d_disp[t][k]);
   dfree(ctx, ctx->d_cellsize); dfree(ctx, ctx->d_dist); dfree(ctx, ctx->d_targets); dfree(ctx, ctx->d_committed); dfree(ctx, ctx->d_stacks);
   dfree(ctx, ctx->d_fx); dfree(ctx, ctx->d_shift); dfree(ctx, ctx->d_fit); dfree(ctx, ctx->d_firstrun); dfree(ctx, ctx->d_counters);
   dfree(ctx, ctx->d_status); dfree(ctx, ctx->d_next); dfree(ctx, ctx->d_maxerr);

@@ -75,6 +75,15 @@ struct galic_ctx {
   // that do not go through the driver's shared pageable staging)
   char *h_stage = nullptr;
   size_t stage_cap = 0;
+  // Jeans tables of get_disp_rtp per type (galic_set_dispersion): FG_Disp_r,
+  // FG_DispZ, FG_DispPhi, FG_tilted_vR2_prime, FG_tilted_vz2_prime, and the
+  // largest magnitude of each (fixed-point range of the sampled energy maps)
+  double *d_disp[4][5] = {};
+  double disp_max[4][5] = {};
+  bool have_disp[4] = {false, false, false, false};
+  // target stacks written by the samplers: bit 0 DGs_MassTarget, bit 1 the
+  // five energy-grid stacks; both make the type's targets complete
+  unsigned target_parts[4] = {0, 0, 0, 0};
 };
 
 namespace galic_internal {

@@ -262,6 +262,43 @@ GM_HD double gm_cos(double x)
   }
 }
 
+/* ---------------------------------------------------------------- exp */
+/* Cody & Waite reduction x = k ln2 + r with k the integer nearest x/ln2
+ * (|r| <= ln2/2; ln2 split as in gm_log, so k*ln2_hi is exact), e^r by its
+ * Taylor series to degree 13 (truncation below 2^-57 relative), then the
+ * scaling by 2^k in two exact-or-once-rounded steps, so that subnormal
+ * results are rounded once. */
+GM_HD double gm_exp(double x)
+{
+  const double ln2_hi = 0x1.62e42fee00000p-1;
+  const double ln2_lo = 0x1.a39ef35793c76p-33;
+  const double inv_ln2 = 0x1.71547652b82fep+0;
+
+  if(gm_isnan(x)) return x;
+  if(x > 710.0) return GM_INF;
+  if(x < -746.0) return 0.0;
+  double k = gm_round(x * inv_ln2);
+  double r = (x - k * ln2_hi) - k * ln2_lo;
+  double p = 0x1.6124613a86d09p-33; /* 1/13! */
+  p = gm_fma(r, p, 0x1.1eed8eff8d898p-29);
+  p = gm_fma(r, p, 0x1.ae64567f544e4p-26);
+  p = gm_fma(r, p, 0x1.27e4fb7789f5cp-22);
+  p = gm_fma(r, p, 0x1.71de3a556c734p-19);
+  p = gm_fma(r, p, 0x1.a01a01a01a01ap-16);
+  p = gm_fma(r, p, 0x1.a01a01a01a01ap-13);
+  p = gm_fma(r, p, 0x1.6c16c16c16c17p-10);
+  p = gm_fma(r, p, 0x1.1111111111111p-7);
+  p = gm_fma(r, p, 0x1.5555555555555p-5);
+  p = gm_fma(r, p, 0x1.5555555555555p-3);
+  p = gm_fma(r, p, 0.5);
+  p = gm_fma(r, p, 1.0);
+  p = gm_fma(r, p, 1.0);
+  int ki = (int) k;        /* |k| <= 1077 */
+  int k1 = ki / 2, k2 = ki - k1;
+  p *= gm_from_bits((uint64_t) (k1 + 1023) << 52); /* exact */
+  return p * gm_from_bits((uint64_t) (k2 + 1023) << 52);
+}
+
 /* ---------------------------------------------------------------- acos */
 GM_HD double gm_acos(double x)
 {

@@ -85,6 +85,40 @@ GM_HD double grng_uniform(grng_t *g)
   return (double) bits * 0x1.0p-53;
 }
 
+/* Uniform number k of a stream: words 2(k&1), 2(k&1)+1 of block k>>1 give
+ * the k-th draw of grng_uniform, so any draw can be computed without the
+ * ones before it. */
+GM_HD double grng_uniform_at(uint64_t seed, uint32_t stream_a, uint32_t stream_b, uint64_t k)
+{
+  const uint32_t key[2] = {(uint32_t) seed, (uint32_t) (seed >> 32)};
+  const uint32_t ctr[4] = {(uint32_t) (k >> 1), (uint32_t) (k >> 33), stream_a, stream_b};
+  uint32_t out[4];
+  grng_philox(ctr, key, out);
+  const int w = (int) (k & 1) * 2;
+  uint64_t bits = (((uint64_t) out[w] << 32) | (uint64_t) out[w + 1]) >> 11;
+  return (double) bits * 0x1.0p-53;
+}
+
+/* index of the next uniform grng_uniform returns */
+GM_HD uint64_t grng_position(const grng_t *g)
+{
+  uint64_t blocks = ((uint64_t) g->ctr[1] << 32) | g->ctr[0];
+  return 2 * blocks - (uint64_t) (g->have / 2);
+}
+
+/* positions the stream so that the next grng_uniform returns draw k */
+GM_HD void grng_seek(grng_t *g, uint64_t k)
+{
+  g->ctr[0] = (uint32_t) (k >> 1);
+  g->ctr[1] = (uint32_t) (k >> 33);
+  g->have = 0;
+  if(k & 1) {
+    grng_philox(g->ctr, g->key, g->buf);
+    if(++g->ctr[0] == 0) ++g->ctr[1];
+    g->have = 2;
+  }
+}
+
 GM_HD double grng_gaussian(grng_t *g, double sigma)
 {
   double x, y, r2;

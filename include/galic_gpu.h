@@ -44,7 +44,8 @@ typedef enum {
   GALIC_ERR_NO_DEVICE = 4,        /* no CUDA device visible */
   GALIC_ERR_BUDGET = 5,           /* the request does not fit the HBM budget */
   GALIC_ERR_UNSUPPORTED = 6,      /* configuration the reference rejects with terminate() */
-  GALIC_ERR_REJECTION_CAP = 7,    /* velocity proposal loop exceeded 100000 tries (main.c:432) */
+  GALIC_ERR_REJECTION_CAP = 7,    /* velocity proposal loop exceeded 100000 tries (main.c:432), or a
+                                     sampler whose draws stopped landing inside Rmax */
   GALIC_ERR_OVERFLOW = 8,         /* a fixed-point response bin left its representable range */
   GALIC_ERR_STATE = 9             /* call out of order (e.g. fit requested before any response) */
 } galic_status;
@@ -349,6 +350,79 @@ int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const double *po
 /* peano_hilbert_key (peano.c:331-347) of the integer cell (x, y, z) with
  * `bits` bits per dimension (bits <= 21). */
 uint64_t galic_peano_hilbert_key(int x, int y, int z, int bits);
+
+/* ------------------------------------------------------- target sampling */
+
+/* Component shapes and limits read by the coordinate samplers and by
+ * get_disp_rtp (All.* of allvars.h:650-720). */
+typedef struct {
+  double Rmax;                  /* All.Rmax (grid.c:329-340) */
+  double Halo_A, HaloStretch;   /* halo.c:17-40 */
+  double Disk_Z0, Disk_H;       /* disk.c:17-50 */
+  double Bulge_A, BulgeStretch; /* bulge.c:15-37 */
+  double HaloBetaParameter, BulgeBetaParameter; /* get_beta_of_type, disp_fields.c:26-60 */
+} galic_sample_params_t;
+
+/* A position in a random stream.  GALIC draws every random number from one
+ * sequential generator (random_generator, init.c:25-27).  This library's
+ * stand-in is the Philox4x32-10 stream keyed by (seed, a, b) whose k-th
+ * uniform double can be computed without the ones before it, so the
+ * reference's sequential sampling loops are replayed in parallel and give
+ * the same samples.  `position` is the index of the next uniform; every call
+ * that draws advances it past the last uniform the reference loop would
+ * have consumed. */
+typedef struct {
+  uint64_t seed;
+  uint32_t a, b;
+  uint64_t position;
+} galic_stream_t;
+
+/* Jeans tables of one type read by get_disp_rtp (disp_fields.c:66-198,
+ * 375-398), each FG_Nbin^2 doubles laid out [iz * FG_Nbin + iR]
+ * (FG_Disp_r: only its first FG_Nbin entries are read, by spherical radius
+ * bin): FG_Disp_r, FG_DispZ, FG_DispPhi, FG_tilted_vR2_prime,
+ * FG_tilted_vz2_prime.  A table that the type's velocity structure does
+ * not read may be NULL (structure 0 and 1 read disp_r; 2 reads dispz and
+ * dispphi; 3 reads tilted_vr2, tilted_vz2 and dispphi).  FG_Vstream[type]
+ * comes from galic_set_vstream. */
+int galic_set_dispersion(galic_ctx *ctx, int type, const double *disp_r, const double *dispz, const double *dispphi,
+                         const double *tilted_vr2, const double *tilted_vz2);
+
+/* Replaces densitygrid_sample_targetresponse (grid.c:536-617) with one rank.
+ * For each type 1..3 with MType[type] > 0, in that order, draws coordinates
+ * from `stream` as the reference's loop does until ntarget of them lie
+ * inside Rmax (the reference's ntarget is SampleParticleCount / NTask + 1),
+ * bins them bilinearly into the density grid, scales by MType / ntarget,
+ * smooths the stack (grid.c:1247-1265) and stores it as the type's
+ * DGs_MassTarget.  renormalize != 0 also applies the recalibration that
+ * forcedensitygrid_calculate makes next (grid.c:862-880: the finest level
+ * times MType / its sum, coarser levels unchanged).  Bins are exact
+ * fixed-point sums (the reference sums in draw order; the two agree to
+ * ~1e-13 relative).  GALIC_ERR_REJECTION_CAP when the samples stop landing
+ * inside Rmax (the reference would loop for ever). */
+int galic_sample_density_targets(galic_ctx *ctx, const galic_sample_params_t *sp, long long ntarget,
+                                 galic_stream_t *stream, int renormalize);
+
+/* Replaces calc_energy_grid_mass_maps (grid.c:941-1076) with one rank: as
+ * above on the energy grid, each sample depositing its bilinear weights and
+ * the weights times get_disp_rtp's four dispersions; stores EGs_MassTarget
+ * and EGs_EgyTarget_{r,t,p,q} of every sampled type.  Needs
+ * galic_set_dispersion for each sampled type. */
+int galic_sample_energy_targets(galic_ctx *ctx, const galic_sample_params_t *sp, long long ntarget,
+                                galic_stream_t *stream);
+
+/* Copies the context's target stacks of one type (each Nstack doubles) to
+ * host arrays; a NULL array is skipped. */
+int galic_get_targets(galic_ctx *ctx, int type, double *dgs_mass, double *egs_mass, double *egs_r, double *egs_t,
+                      double *egs_p, double *egs_q);
+
+/* Replaces n calls of halo_get_fresh_coordinate (halo.c:17-40, type 1),
+ * disk_get_fresh_coordinate (disk.c:17-50, type 2) or
+ * bulge_get_fresh_coordinate (bulge.c:15-37, type 3): the mass-particle
+ * positions that forcedensitygrid_calculate draws (grid.c:659-678), on the
+ * current device.  pos: host array of 3n doubles. */
+int galic_sample_positions(const galic_sample_params_t *sp, int type, long long n, galic_stream_t *stream,
+                           double *pos);
 
 /* ---------------------------------------------------------- host helpers */
 

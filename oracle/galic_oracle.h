@@ -106,4 +106,13 @@ uint64_t orc_peano_key(int x, int y, int z, int bits);
 int orc_force_grid_fill(const galic_fill_params_t *fp, int n, const double *pos, const double *mass,
                         double *dpotdr, double *dpotdz, double *pot);
 
+/* set-up sampling (grid.c:536-617, 659-678, 941-1076), one type, one rank;
+ * oracle_sampling.c */
+void orc_sample_positions(const galic_sample_params_t *sp, int type, long long n, galic_stream_t *stream,
+                          int use_libm, double *pos);
+void orc_sample_density(const galic_params_t *p, const galic_sample_params_t *sp, int type, long long ntarget,
+                        galic_stream_t *stream, int use_libm, int renorm, double *stack);
+void orc_sample_energy(const galic_params_t *p, const galic_sample_params_t *sp, int type, long long ntarget,
+                       galic_stream_t *stream, int use_libm, const double *const *tab, double *stacks);
+
 #endif

@@ -376,3 +376,73 @@ int ref_force_fill(const char *outdir, const ref_fill_params *f, double *dpotdr,
 
 /* peano_hilbert_key (peano.c:331-347) */
 unsigned long long ref_peano_key(int x, int y, int z, int bits) { return peano_hilbert_key(x, y, z, bits); }
+
+/* ------------------------------------------------------- set-up sampling */
+
+/* selects the stream of the reference's random_generator and its position */
+void ref_rng_stream(unsigned long long seed, unsigned int a, unsigned int b, unsigned long long position)
+{
+  galic_shim_rng_stream(random_generator, seed, a, b);
+  galic_shim_rng_seek(random_generator, position);
+}
+unsigned long long ref_rng_position(void) { return galic_shim_rng_position(random_generator); }
+
+/* All.* that the samplers and get_disp_rtp read; SampleParticleCount =
+ * ntarget - 1 with one rank (grid.c:558, grid.c:974) */
+void ref_sample_setup(const galic_sample_params_t *sp, long long ntarget)
+{
+  All.Rmax = sp->Rmax;
+  All.Halo_A = sp->Halo_A;
+  All.HaloStretch = sp->HaloStretch;
+  All.Disk_Z0 = sp->Disk_Z0;
+  All.Disk_H = sp->Disk_H;
+  All.Bulge_A = sp->Bulge_A;
+  All.BulgeStretch = sp->BulgeStretch;
+  All.HaloBetaParameter = sp->HaloBetaParameter;
+  All.BulgeBetaParameter = sp->BulgeBetaParameter;
+  All.SampleParticleCount = (int) (ntarget - 1);
+}
+
+/* FG_Disp_r, FG_DispZ, FG_DispPhi, FG_tilted_vR2_prime, FG_tilted_vz2_prime
+ * of one type (FG_Ngrid doubles each; NULL leaves a table as it is) */
+void ref_set_dispersion(int type, const double *disp_r, const double *dispz, const double *dispphi,
+                        const double *tvr2, const double *tvz2)
+{
+  size_t b = FG_Ngrid * sizeof(double);
+  if(disp_r) memcpy(FG_Disp_r[type], disp_r, b);
+  if(dispz) memcpy(FG_DispZ[type], dispz, b);
+  if(dispphi) memcpy(FG_DispPhi[type], dispphi, b);
+  if(tvr2) memcpy(FG_tilted_vR2_prime[type], tvr2, b);
+  if(tvz2) memcpy(FG_tilted_vz2_prime[type], tvz2, b);
+}
+
+/* densitygrid_sample_targetresponse (grid.c:536-617) */
+void ref_sample_density(void) { densitygrid_sample_targetresponse(); }
+/* calc_energy_grid_mass_maps (grid.c:941-1076) */
+void ref_sample_energy(void) { calc_energy_grid_mass_maps(); }
+
+/* the target stacks of one type (Nstack doubles each) */
+void ref_get_targets(int type, double *dgs_mass, double *egs_mass, double *egs_r, double *egs_t, double *egs_p,
+                     double *egs_q)
+{
+  memcpy(dgs_mass, DGs_MassTarget[type], DG_Nstack * sizeof(double));
+  memcpy(egs_mass, EGs_MassTarget[type], EG_Nstack * sizeof(double));
+  memcpy(egs_r, EGs_EgyTarget_r[type], EG_Nstack * sizeof(double));
+  memcpy(egs_t, EGs_EgyTarget_t[type], EG_Nstack * sizeof(double));
+  memcpy(egs_p, EGs_EgyTarget_p[type], EG_Nstack * sizeof(double));
+  memcpy(egs_q, EGs_EgyTarget_q[type], EG_Nstack * sizeof(double));
+}
+
+/* n calls of the type's *_get_fresh_coordinate (halo.c:17, disk.c:17, bulge.c:15) */
+void ref_fresh_positions(int type, long long n, double *pos)
+{
+  long long i;
+  for(i = 0; i < n; i++) {
+    if(type == 1)
+      halo_get_fresh_coordinate(&pos[3 * i]);
+    else if(type == 2)
+      disk_get_fresh_coordinate(&pos[3 * i]);
+    else
+      bulge_get_fresh_coordinate(&pos[3 * i]);
+  }
+}

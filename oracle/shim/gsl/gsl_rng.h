@@ -15,4 +15,7 @@ void gsl_rng_set(const gsl_rng *r, unsigned long int seed);
 double gsl_rng_uniform(const gsl_rng *r);
 /* project extension: select the Philox stream (seed, a, b) for r */
 void galic_shim_rng_stream(gsl_rng *r, uint64_t seed, uint32_t a, uint32_t b);
+/* project extensions: move to / read the index of the next uniform */
+void galic_shim_rng_seek(gsl_rng *r, uint64_t position);
+uint64_t galic_shim_rng_position(const gsl_rng *r);
 #endif

@@ -32,6 +32,8 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *T)
 void gsl_rng_free(gsl_rng *r) { free(r); }
 void gsl_rng_set(const gsl_rng *r, unsigned long int seed) { grng_init(&((gsl_rng *) r)->g, seed, 0, 0); }
 void galic_shim_rng_stream(gsl_rng *r, uint64_t seed, uint32_t a, uint32_t b) { grng_init(&r->g, seed, a, b); }
+void galic_shim_rng_seek(gsl_rng *r, uint64_t position) { grng_seek(&r->g, position); }
+uint64_t galic_shim_rng_position(const gsl_rng *r) { return grng_position(&r->g); }
 double gsl_rng_uniform(const gsl_rng *r) { return grng_uniform(&((gsl_rng *) r)->g); }
 double gsl_ran_gaussian(const gsl_rng *r, double sigma) { return grng_gaussian(&((gsl_rng *) r)->g, sigma); }
 

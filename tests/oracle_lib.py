@@ -25,6 +25,8 @@ REF_SRC = "/root/reference/src"
 dptr, iptr = _ffi.dptr, _ffi.iptr
 PD, PI, VP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
 PP = C.POINTER(_ffi.GalicParams)
+PSP = C.POINTER(_ffi.GalicSampleParams)
+PST = C.POINTER(_ffi.GalicStream)
 
 
 def build_oracle():
@@ -77,6 +79,9 @@ def oracle_lib():
             "orc_density_geometry": (C.c_int, [C.c_int, C.c_double, C.c_double, PD, PD, PD]),
             "orc_peano_key": (C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_force_grid_fill": (C.c_int, [C.POINTER(_ffi.GalicFillParams), C.c_int, PD, PD, PD, PD, PD]),
+            "orc_sample_positions": (None, [PSP, C.c_int, C.c_longlong, PST, C.c_int, PD]),
+            "orc_sample_density": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.c_int, PD]),
+            "orc_sample_energy": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.POINTER(PD), PD]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -227,6 +232,84 @@ def reference_force_fill(params, rf, with_grid=True):
     return pos, mass, out[0], out[1], out[2]
 
 
+# ------------------------------------------------------------ set-up sampling
+# stream = (seed, a, b, position); tables = {type: (disp_r, dispz, dispphi,
+# tilted_vr2, tilted_vz2, vstream)} with None where a table is not read
+
+def _stream(st):
+    return _ffi.GalicStream(int(st[0]), int(st[1]), int(st[2]), int(st[3]))
+
+
+def _stack_size(L):
+    return ((1 << (2 + 2 * L)) - 1) // 3
+
+
+def oracle_positions(sp, ptype, n, stream, use_libm):
+    """orc_sample_positions: ([n, 3] positions, stream position after)."""
+    s = _stream(stream)
+    pos = np.zeros((n, 3))
+    oracle_lib().orc_sample_positions(C.byref(sp), ptype, n, C.byref(s), 1 if use_libm else 0, dptr(pos))
+    return pos, int(s.position)
+
+
+def oracle_density(params, sp, ptype, ntarget, stream, use_libm, renorm=False):
+    """orc_sample_density: (DGs_MassTarget stack, stream position after)."""
+    s = _stream(stream)
+    out = np.zeros(_stack_size(params.DG_MaxLevel))
+    oracle_lib().orc_sample_density(C.byref(params), C.byref(sp), ptype, ntarget, C.byref(s), 1 if use_libm else 0,
+                                    1 if renorm else 0, dptr(out))
+    return out, int(s.position)
+
+
+def oracle_energy(params, sp, ptype, ntarget, stream, use_libm, tab):
+    """orc_sample_energy: ([5, Nstack] mass, r, t, p, q stacks, stream position after)."""
+    s = _stream(stream)
+    Ns = _stack_size(params.EG_MaxLevel)
+    out = np.zeros((5, Ns))
+    keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab]
+    arr = (PD * 6)(*[dptr(a) if a is not None else PD() for a in keep])
+    oracle_lib().orc_sample_energy(C.byref(params), C.byref(sp), ptype, ntarget, C.byref(s), 1 if use_libm else 0,
+                                   arr, dptr(out))
+    return out, int(s.position)
+
+
+def reference_sampling(params, sp, ntarget, stream, kind, tables=None):
+    """GALIC's own densitygrid_sample_targetresponse (kind "density") or
+    calc_energy_grid_mass_maps (kind "energy") with one rank; returns
+    ({type: six target stacks}, stream position after).  Run it through
+    run_reference()."""
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    L.ref_sample_setup(C.byref(sp), int(ntarget))
+    keep = []
+    for t, tab in (tables or {}).items():
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab]
+        keep.append(arrs)
+        L.ref_set_dispersion(t, *[dptr(a) for a in arrs[:5]])
+        if arrs[5] is not None:
+            L.ref_set_vstream(t, dptr(arrs[5]))
+    L.ref_rng_stream(*[int(x) for x in stream])
+    (L.ref_sample_density if kind == "density" else L.ref_sample_energy)()
+    Ns = _stack_size(params.DG_MaxLevel)
+    out = {}
+    for t in (1, 2, 3):
+        st = [np.zeros(Ns) for _ in range(6)]
+        L.ref_get_targets(t, *[dptr(a) for a in st])
+        out[t] = st
+    return out, int(L.ref_rng_position())
+
+
+def reference_positions(params, sp, ptype, n, stream):
+    """n calls of GALIC's own *_get_fresh_coordinate: ([n, 3], stream position after)."""
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    L.ref_sample_setup(C.byref(sp), 1)
+    L.ref_rng_stream(*[int(x) for x in stream])
+    pos = np.zeros((n, 3))
+    L.ref_fresh_positions(int(ptype), int(n), dptr(pos))
+    return pos, int(L.ref_rng_position())
+
+
 def reference_peano_keys(xyz, bits):
     L = _ref_lib()
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
@@ -260,6 +343,14 @@ def _ref_lib():
         "ref_fill_positions": (None, [C.POINTER(RefFillParams), PD]),
         "ref_force_fill": (C.c_int, [C.c_char_p, C.POINTER(RefFillParams), PD, PD, PD]),
         "ref_peano_key": (C.c_ulonglong, [C.c_int, C.c_int, C.c_int, C.c_int]),
+        "ref_rng_stream": (None, [C.c_ulonglong, C.c_uint, C.c_uint, C.c_ulonglong]),
+        "ref_rng_position": (C.c_ulonglong, []),
+        "ref_sample_setup": (None, [PSP, C.c_longlong]),
+        "ref_set_dispersion": (None, [C.c_int, PD, PD, PD, PD, PD]),
+        "ref_sample_density": (None, []),
+        "ref_sample_energy": (None, []),
+        "ref_get_targets": (None, [C.c_int, PD, PD, PD, PD, PD, PD]),
+        "ref_fresh_positions": (None, [C.c_int, C.c_longlong, PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,6 +1,6 @@
 """The project's elementary functions (galic_b200/csrc/gmath.h) against glibc.
 
-gmath.h replaces log/atan2/sin/cos/acos on the orbit path so that the CUDA
+gmath.h replaces log/atan2/sin/cos/acos/exp on the orbit and sampling paths so that the CUDA
 kernels and the CPU restatement agree bit for bit; these tests bound its
 error against glibc over the argument ranges the path uses."""
 import ctypes as C
@@ -20,6 +20,7 @@ double t_atan2(double y, double x) { return gm_atan2(y, x); }
 double t_sin(double x) { return gm_sin(x); }
 double t_cos(double x) { return gm_cos(x); }
 double t_acos(double x) { return gm_acos(x); }
+double t_exp(double x) { return gm_exp(x); }
 '''
 
 
@@ -32,7 +33,7 @@ def gm(tmp_path_factory):
     subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I",
                     os.path.join(ROOT, "galic_b200", "csrc"), str(src), "-o", str(so)], check=True)
     L = C.CDLL(str(so))
-    for n, k in (("t_log", 1), ("t_atan2", 2), ("t_sin", 1), ("t_cos", 1), ("t_acos", 1)):
+    for n, k in (("t_log", 1), ("t_atan2", 2), ("t_sin", 1), ("t_cos", 1), ("t_acos", 1), ("t_exp", 1)):
         f = getattr(L, n)
         f.restype = C.c_double
         f.argtypes = [C.c_double] * k
@@ -78,3 +79,13 @@ def test_acos_within_two_ulp(gm):
     xs = np.concatenate([rng.uniform(-1, 1, 20000), [1.0, -1.0, 0.0, 1 - 2 ** -52, -1 + 2 ** -53]])
     assert max(ulps(gm.t_acos(x), math.acos(x)) for x in xs) <= 2.0
     assert math.isnan(gm.t_acos(1.5))
+
+
+def test_exp_within_one_ulp(gm):
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([rng.uniform(-700, 700, 20000), rng.uniform(-40, 0, 20000), rng.uniform(-1, 1, 5000),
+                         rng.uniform(-745, -708, 2000), [0.0, -0.0, 1.0, -1.0, 709.78, 1e-300, -1e-300]])
+    assert max(ulps(gm.t_exp(x), math.exp(x)) for x in xs) <= 1.0
+    assert gm.t_exp(0.0) == 1.0
+    assert gm.t_exp(-800.0) == 0.0 and math.isinf(gm.t_exp(800.0)) and math.isinf(gm.t_exp(709.9))
+    assert math.isnan(gm.t_exp(math.nan))
