@@ -174,6 +174,82 @@ def measure_fill(model, steps, cpu, fp64_peak):
     return res
 
 
+SAMPLE_COUNT = 100_000_000  # SampleParticleCount of every Model_*.param
+
+
+def sampling_inputs(model):
+    """Sampler shapes of the workload's components and seeded smooth Jeans
+    tables (the synthetic workload has no Jeans solution; the tables only set
+    the values the energy maps deposit, not the work)."""
+    from galic_b200 import sampling
+
+    comps = {c["kind"]: c for c in model.meta["components"]}
+    h, d = comps["halo"], comps.get("disk")
+    sp = sampling.sample_params(Rmax=model.meta["rmax"], Halo_A=h["scale"], Disk_Z0=d["z0"] if d else 0.0,
+                                Disk_H=d["scale"] if d else 0.0, HaloBetaParameter=h.get("beta", 0.0))
+    N = model.params.FG_Nbin
+    iR, iz = np.meshgrid(np.arange(N), np.arange(N))
+    rng = np.random.default_rng(17)
+    tables = {}
+    for t in (1, 2, 3):
+        if model.params.MType[t] > 0:
+            tables[t] = [np.ascontiguousarray(rng.uniform(1e3, 4e4) * np.exp(-iR / 60.0 - iz / 40.0) + 50.0)
+                         for _ in range(5)]
+    return sp, tables
+
+
+def _ref_sampling_timed(params, sp, ntarget, kind, tables):
+    """GALIC's own sampling function (one rank) on the host; its progress
+    output goes to /dev/null so that the bench's stdout stays one JSON line."""
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+
+    t = time.perf_counter()
+    oracle_lib.reference_sampling(params, sp, ntarget, (42, 0, 0, 0), kind, tables)
+    return time.perf_counter() - t
+
+
+def measure_sampling(model, ctx, steps, cpu):
+    """densitygrid_sample_targetresponse and calc_energy_grid_mass_maps
+    through the C ABI at SampleParticleCount = 1e8 (ntarget = 1e8 + 1 per
+    type, one rank): per call the windows of draws, the exact fixed-point
+    bins, the smoothing and the read-back of every target stack."""
+    from galic_b200 import sampling
+
+    sp, tables = sampling_inputs(model)
+    for t, tab in tables.items():
+        sampling.set_dispersion(ctx, t, *tab)
+    types = sorted(tables)
+    ntarget = SAMPLE_COUNT + 1
+    res = {"sample_count": SAMPLE_COUNT, "types": types, "tables": "seeded smooth synthetic Jeans tables"}
+    for kind, fn in (("density", sampling.sample_density_targets), ("energy", sampling.sample_energy_targets)):
+        fn(ctx, sp, 10000, sampling.Stream(42))
+        walls = []
+        for _ in range(max(steps, 1)):
+            s = sampling.Stream(42)
+            t = time.perf_counter()
+            fn(ctx, sp, ntarget, s)
+            for ty in types:
+                sampling.get_targets(ctx, ty)
+            walls.append(time.perf_counter() - t)
+        ms = statistics.mean(walls) * 1e3
+        res[kind] = {"ms_per_call_e2e": ms, "samples_per_s": len(types) * ntarget / (ms * 1e-3),
+                     "draws": s.position, "gpu_launches": ctx.last_kernel_launches()}
+        if cpu:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import oracle_lib
+
+            n_cpu = 1_000_001
+            sec = oracle_lib.run_reference(_ref_sampling_timed, model.params, sp, n_cpu, kind, tables)
+            cps = len(types) * n_cpu / sec
+            res[kind]["cpu_baseline"] = {"samples_per_s": cps, "cores": 1, "kind": "reference",
+                                         "sample": f"GALIC's own function, {n_cpu} samples per type, one rank",
+                                         "ms_per_call_extrapolated": len(types) * ntarget / cps * 1e3}
+            res[kind]["speedup_e2e_vs_cpu"] = res[kind]["samples_per_s"] / cps
+    return res
+
+
 def measure_ensemble(count, steps):
     """Batched ensemble: `count` Hernquist halos of uneven N advanced per
     iteration by one persistent FP32 launch replayed from a CUDA graph, tile
@@ -524,6 +600,7 @@ def ours_arm(args, rank, world, local_rank):
         kern_avg = sum(kern_ms) / len(kern_ms)
         fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
+        target_sampling = measure_sampling(model, ctx, args.steps, world == 1 and args.cpu_seconds > 0)
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
         serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
@@ -557,6 +634,7 @@ def ours_arm(args, rank, world, local_rank):
                           "unit": "orbit-steps/s"},
                 "cpu_baseline": cpu,
                 "force_grid_fill": fill,
+                "target_sampling": target_sampling,
                 "ensemble": ensemble,
                 "serving": serving,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,

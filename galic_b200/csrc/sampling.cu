@@ -107,6 +107,7 @@ struct WalkArgs {
   int shift[5];
   DispTab D;
   double *pos_out;  // MODE_POS: 3 doubles per kept sample, from rank 0
+  double disk_q_half;  // disk radius draws below it give R < 0.45 Rmax (quick_keep)
 };
 
 // ---------------------------------------------------------------- samplers
@@ -136,8 +137,9 @@ __device__ __forceinline__ bool disk_draw(const Shape &S, double q1, double q2, 
   double R = 1.0, Rold, f, f_;
   int it = 0;
   do {
-    f = (1 + R) * gm_exp(-R) + q2 - 1;
-    f_ = -R * gm_exp(-R);
+    const double e = gm_exp(-R);  // the reference evaluates exp(-R) twice: same value
+    f = (1 + R) * e + q2 - 1;
+    f_ = -R * e;
     Rold = R;
     R = R - f / f_;
   } while(gm_fabs(R - Rold) / R > 1e-7 && ++it < NEWTON_CAP);
@@ -277,6 +279,36 @@ __device__ __forceinline__ void deposit(const WalkArgs &a, const double *pos)
 
 // ---------------------------------------------------------------- the walk
 
+// The count pass only needs each sample's keep decision.  Where a cheap
+// bound settles it with a wide margin the coordinates are not evaluated:
+// 1 = kept, 0 = not kept, -1 = evaluate exactly.  Halo and bulge:
+// |pos|^2 = r^2 (sin^2 theta + cos^2 theta / stretch^2) with cos theta = 2u - 1,
+// and the grid.c test sqrt(x^2 + z^2) < Rmax follows from |pos| < Rmax (the
+// rounded sums are monotone).  Disk: below the radius draw q_half the Newton
+// radius is under 0.45 Rmax, and with |z| < 0.85 Rmax the point is inside.
+// The evaluated values differ from the bounds by a few ulp, far inside the
+// 1e-7 margins; a sample near a boundary takes the exact path.
+template <int TYPE>
+__device__ __forceinline__ int quick_keep(const WalkArgs &a, double d0, double d1, double d2)
+{
+  const Shape &S = a.S;
+  const double R2 = S.Rmax * S.Rmax;
+  if(TYPE == 2) {
+    if(!(d1 < a.disk_q_half)) return -1;
+    const double z = S.Disk_Z0 / 2 * gm_log(d0 / (1 - d0));
+    return gm_fabs(z) < 0.85 * S.Rmax ? 1 : -1;
+  }
+  const double s = (TYPE == 1) ? S.HaloStretch : S.BulgeStretch;
+  if(!(s >= 0.01 && s <= 100.0)) return -1;
+  if(TYPE == 3 && a.mode == MODE_POS) return 1;  // the radius was accepted when drawn
+  const double r = (TYPE == 1) ? (d0 > 0 ? S.Halo_A * (d0 + sqrt(d0)) / (1 - d0) : 0.0) : bulge_radius(S, d0);
+  const double c = d2 * 2 - 1;
+  const double E = r * r * ((1 - c * c) + c * c / (s * s));
+  if(E < R2 * (1 - 1e-7)) return 1;
+  if(TYPE == 1 && E > R2 * (1 + 1e-7)) return 0;
+  return -1;
+}
+
 template <int TYPE, int PASS>
 __global__ void __launch_bounds__(WALK_BLOCK) k_walk(const WalkArgs a)
 {
@@ -316,8 +348,15 @@ __global__ void __launch_bounds__(WALK_BLOCK) k_walk(const WalkArgs a)
     } else {
       st = 0;
       double pos[3];
-      bool keep = make_sample<TYPE>(a.S, u2, u1, u, pos);
-      if(keep && a.mode != MODE_POS) keep = sqrt(pos[0] * pos[0] + pos[2] * pos[2]) < a.S.Rmax;
+      int quick = -1;
+      if(PASS == PASS_COUNT) quick = quick_keep<TYPE>(a, u2, u1, u);
+      bool keep;
+      if(quick >= 0) {
+        keep = quick;
+      } else {
+        keep = make_sample<TYPE>(a.S, u2, u1, u, pos);
+        if(keep && a.mode != MODE_POS) keep = sqrt(pos[0] * pos[0] + pos[2] * pos[2]) < a.S.Rmax;
+      }
       if(keep) {
         if(PASS == PASS_EMIT) {
           const long long rank = base + kept;
@@ -446,6 +485,16 @@ cudaError_t walk(int type, int pass, const WalkArgs &a, cudaStream_t st)
   return launch_walk<3>(pass, a, st);
 }
 
+// The disk's radius draw q solves (1 + R) e^-R = 1 - q for R / Disk_H
+// (disk.c:25-36), increasing in q: q(R) = 1 - (1 + R) e^-R at R = 0.45 Rmax /
+// Disk_H bounds the draws whose radius is below 0.45 Rmax (0: no quick path).
+double disk_q_half(const Shape &S)
+{
+  if(!(S.Disk_H > 0) || !(S.Rmax > 0) || !std::isfinite(S.Rmax / S.Disk_H)) return 0.0;
+  const double R = 0.45 * S.Rmax / S.Disk_H;
+  return 1.0 - (1.0 + R) * std::exp(-R);
+}
+
 // Draws `ntarget` kept samples of one type from the stream, window by
 // window (see the top of this file).  a: mode, shape, deposit targets.
 // Returns GALIC_OK, GALIC_ERR_CUDA or GALIC_ERR_REJECTION_CAP.
@@ -469,6 +518,7 @@ int run_type(int type, long long ntarget, galic_stream_t *stream, WalkArgs a, Sc
   a.offsets = s.offsets;
   a.end = s.end;
   a.end_state = s.end_state;
+  a.disk_q_half = disk_q_half(a.S);
   while(remaining > 0) {
     double want = (double) remaining / rate * 1.02 + 64;
     long long nch = (long long) std::ceil(want / SAMPLES_PER_CHUNK);

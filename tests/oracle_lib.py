@@ -286,7 +286,7 @@ def reference_sampling(params, sp, ntarget, stream, kind, tables=None):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab]
         keep.append(arrs)
         L.ref_set_dispersion(t, *[dptr(a) for a in arrs[:5]])
-        if arrs[5] is not None:
+        if len(arrs) > 5 and arrs[5] is not None:
             L.ref_set_vstream(t, dptr(arrs[5]))
     L.ref_rng_stream(*[int(x) for x in stream])
     (L.ref_sample_density if kind == "density" else L.ref_sample_energy)()
