@@ -310,7 +310,7 @@ __device__ __forceinline__ int quick_keep(const WalkArgs &a, double d0, double d
 }
 
 template <int TYPE, int PASS>
-__global__ void __launch_bounds__(WALK_BLOCK) k_walk(const WalkArgs a)
+__global__ void __launch_bounds__(WALK_BLOCK) k_sample_walk(const WalkArgs a)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if(c >= a.nchunks) return;
@@ -472,9 +472,9 @@ template <int TYPE>
 cudaError_t launch_walk(int pass, const WalkArgs &a, cudaStream_t st)
 {
   const int grid = (a.nchunks + WALK_BLOCK - 1) / WALK_BLOCK;
-  if(pass == PASS_MAP) k_walk<TYPE, PASS_MAP><<<grid, WALK_BLOCK, 0, st>>>(a);
-  else if(pass == PASS_COUNT) k_walk<TYPE, PASS_COUNT><<<grid, WALK_BLOCK, 0, st>>>(a);
-  else k_walk<TYPE, PASS_EMIT><<<grid, WALK_BLOCK, 0, st>>>(a);
+  if(pass == PASS_MAP) k_sample_walk<TYPE, PASS_MAP><<<grid, WALK_BLOCK, 0, st>>>(a);
+  else if(pass == PASS_COUNT) k_sample_walk<TYPE, PASS_COUNT><<<grid, WALK_BLOCK, 0, st>>>(a);
+  else k_sample_walk<TYPE, PASS_EMIT><<<grid, WALK_BLOCK, 0, st>>>(a);
   return cudaGetLastError();
 }
 
