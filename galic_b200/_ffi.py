@@ -113,6 +113,21 @@ class GalicStream(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("a", C.c_uint32), ("b", C.c_uint32), ("position", C.c_uint64)]
 
 
+class GalicJeansParams(C.Structure):
+    """galic_jeans_params_t."""
+    _fields_ = [("StreamingVelocityParameter", D4), ("DispersionRoverZratio", D4)]
+
+
+class GalicJeansTables(C.Structure):
+    """galic_jeans_tables_t (pointers to FG_Nbin^2 doubles)."""
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in ("disp_r", "dispz", "dispphi", "vstream", "tilted_vz2",
+                                                      "tilted_vR2", "tilted_vz2_prime", "tilted_vR2_prime")]
+
+
+JEANS_TABLES = ("disp_r", "dispz", "dispphi", "vstream", "tilted_vz2", "tilted_vR2", "tilted_vz2_prime",
+                "tilted_vR2_prime")
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
@@ -190,6 +205,8 @@ SIGNATURES = [
      [VP, C.POINTER(GalicSampleParams), C.c_longlong, C.POINTER(GalicStream), C.c_int]),
     ("galic_sample_energy_targets", C.c_int, [VP, C.POINTER(GalicSampleParams), C.c_longlong, C.POINTER(GalicStream)]),
     ("galic_get_targets", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD, PD]),
+    ("galic_calculate_dispfield", C.c_int,
+     [VP, C.POINTER(GalicSampleParams), C.POINTER(GalicJeansParams), C.POINTER(GalicJeansTables)]),
     ("galic_sample_positions", C.c_int,
      [C.POINTER(GalicSampleParams), C.c_int, C.c_longlong, C.POINTER(GalicStream), PD]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),

@@ -424,6 +424,36 @@ int galic_get_targets(galic_ctx *ctx, int type, double *dgs_mass, double *egs_ma
 int galic_sample_positions(const galic_sample_params_t *sp, int type, long long n, galic_stream_t *stream,
                            double *pos);
 
+/* ------------------------------------------------------- Jeans solvers */
+
+/* Parameters of calculate_dispfield beyond galic_params_t and
+ * galic_sample_params_t, indexed by type 1..3. */
+typedef struct {
+  double StreamingVelocityParameter[4]; /* All.{Halo,Disk,Bulge}StreamingVelocityParameter (disp_fields.c:570-575) */
+  double DispersionRoverZratio[4];      /* All.{Halo,Disk,Bulge}DispersionRoverZratio (disp_fields.c:1051-1105) */
+} galic_jeans_params_t;
+
+/* The Jeans tables of one type, FG_Nbin^2 doubles each in [iz * FG_Nbin + iR]
+ * (FG_Disp_r: its first FG_Nbin entries, by radius bin); NULL skips a table. */
+typedef struct {
+  double *disp_r, *dispz, *dispphi, *vstream;
+  double *tilted_vz2, *tilted_vR2, *tilted_vz2_prime, *tilted_vR2_prime;
+} galic_jeans_tables_t;
+
+/* Replaces calculate_dispfield (disp_fields.c:502-1049): the spherical
+ * Jeans equation with anisotropy beta (FG_Disp_r), the axisymmetric
+ * f(E, Lz) solution (FG_DispZ, and FG_DispPhi / FG_Vstream) for every type
+ * with particles, and for velocity structure 3 the method-of-lines solution
+ * of the tilted (f(E, Lz, I3)) case (FG_tilted_*, and FG_DispPhi / FG_Vstream
+ * again, VER_1_1 form).  Reads the context's force grid (galic_set_force_grid)
+ * and the densities of halo.c / disk.c / bulge.c.  The results replace the
+ * context's FG_Vstream and Jeans tables, as galic_set_vstream and
+ * galic_set_dispersion would; out, when not NULL, is indexed by type (1..3)
+ * and receives copies.  GALIC_ERR_UNSUPPORTED for velocity structure 3 with
+ * a zero DispersionRoverZratio (the reference's terminate()). */
+int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_params_t *sp, const galic_jeans_params_t *jp,
+                              galic_jeans_tables_t *out);
+
 /* ---------------------------------------------------------- host helpers */
 
 /* Grid geometry of forcedensitygrid_create (grid.c:329-480): from Halo_A,

@@ -115,4 +115,10 @@ void orc_sample_density(const galic_params_t *p, const galic_sample_params_t *sp
 void orc_sample_energy(const galic_params_t *p, const galic_sample_params_t *sp, int type, long long ntarget,
                        galic_stream_t *stream, int use_libm, const double *const *tab, double *stacks);
 
+/* calculate_dispfield (disp_fields.c:502-1049); oracle_jeans.c.  out:
+ * [4][8][FG_Nbin^2] (disp_r, dispz, dispphi, vstream, tilted_vz2, tilted_vR2,
+ * tilted_vz2_prime, tilted_vR2_prime per type). */
+int orc_calculate_dispfield(orc_model *m, const galic_sample_params_t *sp, const galic_jeans_params_t *jp,
+                            double *out);
+
 #endif

@@ -446,3 +446,37 @@ void ref_fresh_positions(int type, long long n, double *pos)
       bulge_get_fresh_coordinate(&pos[3 * i]);
   }
 }
+
+/* ------------------------------------------------------- Jeans solvers */
+
+/* calculate_dispfield (disp_fields.c:502-1049) with the All.* it reads; its
+ * sigma/pde output files go to outdir */
+int ref_calculate_dispfield(const char *outdir, const galic_sample_params_t *sp, const galic_jeans_params_t *jp)
+{
+  ref_sample_setup(sp, 1);
+  All.HaloStreamingVelocityParameter = jp->StreamingVelocityParameter[1];
+  All.DiskStreamingVelocityParameter = jp->StreamingVelocityParameter[2];
+  All.BulgeStreamingVelocityParameter = jp->StreamingVelocityParameter[3];
+  All.HaloDispersionRoverZratio = jp->DispersionRoverZratio[1];
+  All.DiskDispersionRoverZratio = jp->DispersionRoverZratio[2];
+  All.BulgeDispersionRoverZratio = jp->DispersionRoverZratio[3];
+  if(strlen(outdir) >= sizeof(All.OutputDir)) return 1;
+  strcpy(All.OutputDir, outdir);
+  /* tables the function leaves untouched read as zero */
+  for(int t = 1; t <= 3; t++) {
+    double *tab[8] = {FG_Disp_r[t], FG_DispZ[t], FG_DispPhi[t], FG_Vstream[t],
+                      FG_tilted_vz2[t], FG_tilted_vR2[t], FG_tilted_vz2_prime[t], FG_tilted_vR2_prime[t]};
+    for(int k = 0; k < 8; k++) memset(tab[k], 0, FG_Ngrid * sizeof(double));
+  }
+  calculate_dispfield();
+  return 0;
+}
+
+/* the Jeans tables of one type: disp_r, dispz, dispphi, vstream, tilted_vz2,
+ * tilted_vR2, tilted_vz2_prime, tilted_vR2_prime (FG_Ngrid doubles each) */
+void ref_get_jeans(int type, double *out)
+{
+  double *src[8] = {FG_Disp_r[type], FG_DispZ[type], FG_DispPhi[type], FG_Vstream[type],
+                    FG_tilted_vz2[type], FG_tilted_vR2[type], FG_tilted_vz2_prime[type], FG_tilted_vR2_prime[type]};
+  for(int k = 0; k < 8; k++) memcpy(out + (size_t) k * FG_Ngrid, src[k], FG_Ngrid * sizeof(double));
+}

@@ -27,6 +27,7 @@ PD, PI, VP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
 PP = C.POINTER(_ffi.GalicParams)
 PSP = C.POINTER(_ffi.GalicSampleParams)
 PST = C.POINTER(_ffi.GalicStream)
+PJP = C.POINTER(_ffi.GalicJeansParams)
 
 
 def build_oracle():
@@ -80,6 +81,7 @@ def oracle_lib():
             "orc_peano_key": (C.c_uint64, [C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_force_grid_fill": (C.c_int, [C.POINTER(_ffi.GalicFillParams), C.c_int, PD, PD, PD, PD, PD]),
             "orc_sample_positions": (None, [PSP, C.c_int, C.c_longlong, PST, C.c_int, PD]),
+            "orc_calculate_dispfield": (C.c_int, [VP, PSP, PJP, PD]),
             "orc_sample_density": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.c_int, PD]),
             "orc_sample_energy": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.POINTER(PD), PD]),
         }
@@ -310,6 +312,36 @@ def reference_positions(params, sp, ptype, n, stream):
     return pos, int(L.ref_rng_position())
 
 
+def oracle_dispfield(m, sp, jp, use_libm):
+    """orc_calculate_dispfield on the model's force grid: (status, [4, 8, N, N] tables)."""
+    o = Oracle(m.params, use_libm=use_libm)
+    o.load_model(m, particles=False)
+    N = m.params.FG_Nbin
+    out = np.zeros((4, 8, N, N))
+    st = o.L.orc_calculate_dispfield(o.h, C.byref(sp), C.byref(jp), dptr(out))
+    return st, out
+
+
+def reference_dispfield(params, m_arrays, sp, jp):
+    """GALIC's own calculate_dispfield (one rank) on the force grid
+    m_arrays = (pot, dpotdr, dpotdz): [4, 8, N, N] tables of the types it
+    computes.  Run it through run_reference()."""
+    import tempfile
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    pot, dpotdr, dpotdz = [np.ascontiguousarray(a, dtype=np.float64) for a in m_arrays]
+    L.ref_set_force_grid(dptr(pot), dptr(dpotdr), dptr(dpotdz))
+    with tempfile.TemporaryDirectory() as d:
+        st = L.ref_calculate_dispfield(d.encode(), C.byref(sp), C.byref(jp))
+    if st != 0:
+        raise RuntimeError(f"ref_calculate_dispfield status {st}")
+    N = params.FG_Nbin
+    out = np.zeros((4, 8, N, N))
+    for t in (1, 2, 3):
+        L.ref_get_jeans(t, dptr(out[t]))
+    return out
+
+
 def reference_peano_keys(xyz, bits):
     L = _ref_lib()
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
@@ -351,6 +383,8 @@ def _ref_lib():
         "ref_sample_energy": (None, []),
         "ref_get_targets": (None, [C.c_int, PD, PD, PD, PD, PD, PD]),
         "ref_fresh_positions": (None, [C.c_int, C.c_longlong, PD]),
+        "ref_calculate_dispfield": (C.c_int, [C.c_char_p, PSP, PJP]),
+        "ref_get_jeans": (None, [C.c_int, PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
