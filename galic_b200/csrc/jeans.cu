@@ -16,11 +16,11 @@
 //    points of every z interval of every column (k_axi_points), then one
 //    thread per column sums the trapezoids in the reference's order
 //    (k_axi_march), then DispPhi / Vstream per grid point (k_axi_stream);
-//  * tilted f(E, Lz, I3) (disp_fields.c:733-1044): for a block of rows the
-//    coefficients of the 100 method-of-lines substeps (k_tilt_coef), then one
-//    CTA, a thread per column, steps the rows with the neighbour exchange in
-//    shared memory (k_tilt_march); then the tilted tables and the VER_1_1
-//    streaming velocity per grid point.
+//  * tilted f(E, Lz, I3) (disp_fields.c:733-1044): the coefficients of the
+//    100 method-of-lines substeps of every row (k_tilt_coef, 313 MB at
+//    N = 256), then one CTA, a thread per column, steps the rows with the
+//    neighbour exchange in shared memory (k_tilt_march); then the tilted
+//    tables and the VER_1_1 streaming velocity per grid point.
 // Every expression keeps the reference's operation order and the file is
 // built with --fmad=false, so the tables are bit-identical to the CPU
 // restatement with gmath.h's functions.  The grid radii
@@ -36,6 +36,8 @@
 #include "galic_gpu.h"
 #include "model.cuh"
 
+#include <cuda_pipeline.h>
+
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;  // M_PI
@@ -43,7 +45,6 @@ constexpr double MIN_DENSITY = 1e-25;           // allvars.h:201
 constexpr int SPH_STEPS = 50;                   // disp_fields.c:458
 constexpr int AXI_STEPS = 50;                   // disp_fields.c:429
 constexpr int TILT_STEPS = 100;                 // disp_fields.c:784
-constexpr int TILT_ROWS = 16;                   // rows per coefficient block
 constexpr int NTAB = 8;  // disp_r, dispz, dispphi, vstream, tilted_vz2, tilted_vR2, tilted_vz2_prime, tilted_vR2_prime
 
 struct JeansArgs {
@@ -177,22 +178,40 @@ __global__ void k_sph_coef(const JeansArgs J, SphCoef *coef)
   coef[t] = c;
 }
 
-__global__ void k_sph_march(const JeansArgs J, const SphCoef *coef)
+// One thread runs the recurrence; the other threads of the CTA stage the
+// next chunk of coefficients in shared memory meanwhile.
+constexpr int SPH_CHUNK = 256;
+
+__global__ void __launch_bounds__(256) k_sph_march(const JeansArgs J, const SphCoef *coef)
 {
-  if(threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ SphCoef buf[2][SPH_CHUNK];
+  const int total = (J.N + 1) * SPH_STEPS;
   double *disp_r = table(J, 0);
+  for(int t = threadIdx.x; t < SPH_CHUNK && t < total; t += blockDim.x) buf[0][t] = coef[t];
+  __syncthreads();
   double y = 0.0;
-  for(int m = 0; m <= J.N; m++) {
-    for(int i = 0; i < SPH_STEPS; i++) {
-      const SphCoef c = coef[m * SPH_STEPS + i];
-      if(c.flag == 2) {
-        double ypred = y + c.dr * (c.a0 - c.c0 * y);
-        y += c.dr * 0.5 * ((c.a0 - c.c0 * y) + (c.a1 - c.c1 * ypred));
-      } else if(c.flag == 1) {
-        y += c.dr * (c.a0 - c.c0 * y);
+  int b = 0;
+  for(int c0 = 0; c0 < total; c0 += SPH_CHUNK, b ^= 1) {
+    const int n1 = c0 + SPH_CHUNK;
+    if(threadIdx.x > 0) {
+      for(int t = threadIdx.x - 1; t < SPH_CHUNK && n1 + t < total; t += blockDim.x - 1) buf[b ^ 1][t] = coef[n1 + t];
+    } else {
+      for(int t = 0; t < SPH_CHUNK && c0 + t < total; t++) {
+        const SphCoef c = buf[b][t];
+        if(c.flag == 2) {
+          double ypred = y + c.dr * (c.a0 - c.c0 * y);
+          y += c.dr * 0.5 * ((c.a0 - c.c0 * y) + (c.a1 - c.c1 * ypred));
+        } else if(c.flag == 1) {
+          y += c.dr * (c.a0 - c.c0 * y);
+        }
+        const int g = c0 + t;
+        if((g + 1) % SPH_STEPS == 0) {
+          const int m = g / SPH_STEPS;
+          if(m >= 1) disp_r[J.N - m] = y;
+        }
       }
     }
-    if(m >= 1) disp_r[J.N - m] = y;
+    __syncthreads();
   }
 }
 
@@ -228,6 +247,7 @@ __global__ void k_axi_points(const JeansArgs J, double *Y)
   const int P = AXI_STEPS + 1;
   const long long total = (long long) J.N * (J.N + 1) * P;
   if(t >= total) return;
+  // Y[(j * (N + 1) + m) * P + i]: one column's points are contiguous
   const int i = (int) (t % P);
   const long long cm = t / P;
   const int m = (int) (cm % (J.N + 1));
@@ -255,9 +275,14 @@ __global__ void k_axi_march(const JeansArgs J, const double *Y)
     double zstart, zend;
     axi_interval(J, m, &zstart, &zend);
     double dz = (zend - zstart) / AXI_STEPS;
+    // the interval's 51 points are loaded together, then summed in order
     const double *y = Y + ((size_t) j * (N + 1) + m) * P;
+    double v[AXI_STEPS + 1];
+#pragma unroll
+    for(int i = 0; i <= AXI_STEPS; i++) v[i] = y[i];
     double sum = 0;
-    for(int i = 0; i < AXI_STEPS; i++) sum += 0.5 * (y[i] + y[i + 1]) * dz;
+#pragma unroll
+    for(int i = 0; i < AXI_STEPS; i++) sum += 0.5 * (v[i] + v[i + 1]) * dz;
     if(m == 0) {
       integ = sum;
     } else {
@@ -331,10 +356,12 @@ __global__ void k_axi_stream(const JeansArgs J)
 
 // ---------------------------------------------------------------- tilted
 
-struct TiltCoef {
+struct alignas(16) TiltCoef {
   double p, h1, h2, dR, hor;
   int nb;  // neighbour column of dqdR, -1: dqdR = 0
+  int pad;
 };
+static_assert(sizeof(TiltCoef) == 48, "three 16-byte copies per coefficient");
 
 // rows k in [k_lo, k_hi] (all < N - 1), substep st, column j
 // (disp_fields.c:775-835)
@@ -374,34 +401,63 @@ __global__ void k_tilt_coef(const JeansArgs J, int k_lo, int k_hi, TiltCoef *coe
   coef[t] = c;
 }
 
-// one CTA, a thread per column: the substeps of rows k_hi .. k_lo
-// (disp_fields.c:775-839); q holds the row above on entry in smem
-__global__ void k_tilt_march(const JeansArgs J, int k_lo, int k_hi, const TiltCoef *coef, double *FG_q)
+// one CTA, a thread per column (N <= blockDim.x): the substeps of rows
+// k_hi .. k_lo (disp_fields.c:775-839); FG_q holds the row above on entry.
+// Each thread streams its own coefficients D substeps ahead into a ring in
+// shared memory with asynchronous copies (only the thread that reads a slot
+// writes it, so no barrier guards the ring); the row alternates between two
+// shared buffers, one barrier per substep.
+template <int MAXT, int D>
+__global__ void __launch_bounds__(MAXT) k_tilt_march(const JeansArgs J, int k_lo, int k_hi, const TiltCoef *coef,
+                                                     double *FG_q)
 {
-  extern __shared__ double sh[];
-  const int N = J.N;
-  double *qprev = sh, *qnew = sh + N;
-  for(int j = threadIdx.x; j < N; j += blockDim.x) qprev[j] = FG_q[(size_t) (k_hi + 1) * N + j];
-  __syncthreads();
-  for(int k = k_hi; k >= k_lo; k--) {
-    const double dz = J.Rg[k] - J.Rg[k + 1];
-    const double step = dz / TILT_STEPS;
-    const TiltCoef *row = coef + (size_t) (k_hi - k) * TILT_STEPS * N;
-    for(int st = 0; st < TILT_STEPS; st++) {
-      for(int j = threadIdx.x; j < N; j += blockDim.x) {
-        const TiltCoef c = row[(size_t) st * N + j];
-        double dqdR;
-        if(c.nb < 0)
-          dqdR = 0;
-        else
-          dqdR = (c.h2 * qprev[c.nb] - c.h1 * qprev[j]) / (c.dR) + qprev[j] * c.hor;
-        qnew[j] = qprev[j] + (-c.p - dqdR) * step;
-      }
-      __syncthreads();
-      for(int j = threadIdx.x; j < N; j += blockDim.x) qprev[j] = qnew[j];
-      __syncthreads();
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int N = J.N, j = threadIdx.x;
+  const bool active = j < N;
+  TiltCoef *ring = reinterpret_cast<TiltCoef *>(smem);     // [D][N]
+  double *qb = reinterpret_cast<double *>(ring + (size_t) D * N);  // [2][N]
+  const int steps = (k_hi - k_lo + 1) * TILT_STEPS;
+  if(active) qb[j] = FG_q[(size_t) (k_hi + 1) * N + j];
+#pragma unroll
+  for(int u = 0; u < D; u++) {
+    if(active && u < steps) {
+      const char *src = reinterpret_cast<const char *>(coef + (size_t) u * N + j);
+      char *dst = reinterpret_cast<char *>(ring + (size_t) u * N + j);
+      __pipeline_memcpy_async(dst, src, 16);
+      __pipeline_memcpy_async(dst + 16, src + 16, 16);
+      __pipeline_memcpy_async(dst + 32, src + 32, 16);
     }
-    for(int j = threadIdx.x; j < N; j += blockDim.x) FG_q[(size_t) k * N + j] = qprev[j];
+    __pipeline_commit();
+  }
+  __syncthreads();
+  int cur = 0;
+  double step = 0;
+  for(int g = 0; g < steps; g++) {
+    const int k = k_hi - g / TILT_STEPS, st = g - (g / TILT_STEPS) * TILT_STEPS;
+    if(st == 0) step = (J.Rg[k] - J.Rg[k + 1]) / TILT_STEPS;  // dz / nsteps
+    __pipeline_wait_prior(D - 1);  // this thread's copy of substep g has landed
+    const int slot = g % D;
+    if(active) {
+      const TiltCoef c = ring[(size_t) slot * N + j];
+      const double *qp = qb + cur * N;
+      double dqdR;
+      if(c.nb < 0)
+        dqdR = 0;
+      else
+        dqdR = (c.h2 * qp[c.nb] - c.h1 * qp[j]) / (c.dR) + qp[j] * c.hor;
+      qb[(cur ^ 1) * N + j] = qp[j] + (-c.p - dqdR) * step;
+      if(g + D < steps) {
+        const char *src = reinterpret_cast<const char *>(coef + (size_t) (g + D) * N + j);
+        char *dst = reinterpret_cast<char *>(ring + (size_t) slot * N + j);
+        __pipeline_memcpy_async(dst, src, 16);
+        __pipeline_memcpy_async(dst + 16, src + 16, 16);
+        __pipeline_memcpy_async(dst + 32, src + 32, 16);
+      }
+    }
+    __pipeline_commit();
+    __syncthreads();
+    cur ^= 1;
+    if(active && st == TILT_STEPS - 1) FG_q[(size_t) k * N + j] = qb[cur * N + j];
   }
 }
 
@@ -499,6 +555,25 @@ int jfail(galic_ctx *ctx, int st)
 
 inline int blocks(long long n, int b) { return (int) ((n + b - 1) / b); }
 
+size_t march_smem(int N, int D) { return (size_t) D * N * sizeof(TiltCoef) + 2 * (size_t) N * sizeof(double); }
+
+// the marches' shared-memory ceiling, once per device
+cudaError_t prepare_march()
+{
+  static bool done[256];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e || (dev >= 0 && dev < 256 && done[dev])) return e;
+  if((e = cudaFuncSetAttribute(k_tilt_march<512, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int) march_smem(512, 8))))
+    return e;
+  if((e = cudaFuncSetAttribute(k_tilt_march<1024, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int) march_smem(1024, 4))))
+    return e;
+  if(dev >= 0 && dev < 256) done[dev] = true;
+  return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_params_t *sp,
@@ -520,6 +595,9 @@ extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_para
   double *d_Rg = nullptr, *d_tab = nullptr, *d_Y = nullptr, *d_q = nullptr;
   SphCoef *d_sph = nullptr;
   TiltCoef *d_tilt = nullptr;
+  // rows of tilted coefficients per block: all of them within 512 MiB
+  const int tilt_rows =
+      (int) std::max<size_t>(1, std::min<size_t>(N - 1, (512ull << 20) / ((size_t) TILT_STEPS * N * sizeof(TiltCoef))));
   std::vector<double> Rg(2 * N + 3), h_tab;
   for(int j = 0; j < 2 * N + 3; j++) Rg[j] = p.FG_Rmin * (std::pow(p.FG_Fac, j) - 1.0);
   bool any_tilt = false;
@@ -542,7 +620,8 @@ extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_para
   JCK(cudaMallocAsync((void **) &d_Y, (size_t) N * (N + 1) * (AXI_STEPS + 1) * sizeof(double), s));
   if(any_tilt) {
     JCK(cudaMallocAsync((void **) &d_q, G * sizeof(double), s));
-    JCK(cudaMallocAsync((void **) &d_tilt, (size_t) TILT_ROWS * TILT_STEPS * N * sizeof(TiltCoef), s));
+    JCK(cudaMallocAsync((void **) &d_tilt, (size_t) tilt_rows * TILT_STEPS * N * sizeof(TiltCoef), s));
+    JCK(prepare_march());
   }
   JCK(cudaMemcpyAsync(d_Rg, Rg.data(), Rg.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   JCK(cudaMemsetAsync(d_tab, 0, 4 * NTAB * G * sizeof(double), s));
@@ -555,7 +634,7 @@ extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_para
     J.beta_a = (t == 1) ? p.Halo_A : p.Bulge_A;
     J.tab = d_tab + (size_t) t * NTAB * G;
     k_sph_coef<<<blocks((long long) (N + 1) * SPH_STEPS, 256), 256, 0, s>>>(J, d_sph);
-    k_sph_march<<<1, 32, 0, s>>>(J, d_sph);
+    k_sph_march<<<1, 256, 0, s>>>(J, d_sph);
     k_sph_divide<<<blocks(N, 256), 256, 0, s>>>(J);
     launches += 3;
     JCK(cudaGetLastError());
@@ -567,7 +646,7 @@ extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_para
     J.kpar = jp->StreamingVelocityParameter[t];
     J.tab = d_tab + (size_t) t * NTAB * G;
     k_axi_points<<<blocks((long long) N * (N + 1) * (AXI_STEPS + 1), 256), 256, 0, s>>>(J, d_Y);
-    k_axi_march<<<blocks(N, 64), 64, 0, s>>>(J, d_Y);
+    k_axi_march<<<blocks(N, 32), 32, 0, s>>>(J, d_Y);
     k_axi_stream<<<blocks((long long) G, 256), 256, 0, s>>>(J);
     launches += 3;
     JCK(cudaGetLastError());
@@ -582,12 +661,15 @@ extern "C" int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_para
     J.beta_a = (t == 1) ? p.Halo_A : p.Bulge_A;
     J.tab = d_tab + (size_t) t * NTAB * G;
     JCK(cudaMemsetAsync(d_q + (size_t) (N - 1) * N, 0, N * sizeof(double), s));  // the top row is 0
-    const int mthreads = std::min(1024, ((N + 31) / 32) * 32);
-    for(int k_hi = N - 2; k_hi >= 0; k_hi -= TILT_ROWS) {
-      const int k_lo = std::max(0, k_hi - TILT_ROWS + 1);
+    const int mthreads = ((N + 31) / 32) * 32;
+    for(int k_hi = N - 2; k_hi >= 0; k_hi -= tilt_rows) {
+      const int k_lo = std::max(0, k_hi - tilt_rows + 1);
       const long long n = (long long) (k_hi - k_lo + 1) * TILT_STEPS * N;
       k_tilt_coef<<<blocks(n, 256), 256, 0, s>>>(J, k_lo, k_hi, d_tilt);
-      k_tilt_march<<<1, mthreads, 2 * N * sizeof(double), s>>>(J, k_lo, k_hi, d_tilt, d_q);
+      if(mthreads <= 512)
+        k_tilt_march<512, 8><<<1, mthreads, march_smem(N, 8), s>>>(J, k_lo, k_hi, d_tilt, d_q);
+      else
+        k_tilt_march<1024, 4><<<1, mthreads, march_smem(N, 4), s>>>(J, k_lo, k_hi, d_tilt, d_q);
       launches += 2;
     }
     k_tilt_tables<<<blocks((long long) G, 256), 256, 0, s>>>(J, d_q);
