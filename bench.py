@@ -250,6 +250,60 @@ def measure_sampling(model, ctx, steps, cpu):
     return res
 
 
+def jeans_inputs(model):
+    """Jeans parameters of the workload: disk (velocity structure 3) with
+    DispersionRoverZratio 1.5 and streaming parameter 0.8; halo structure 0."""
+    from galic_b200 import jeans
+
+    sp, _ = sampling_inputs(model)
+    jp = jeans.jeans_params(streaming=(0.0, 0.0, 0.8, 0.0), r_over_z=(0.0, 1.5, 1.5, 1.5))
+    return sp, jp
+
+
+def _ref_jeans_timed(params, grid, sp, jp):
+    """GALIC's own calculate_dispfield (one rank) on the host, progress output to /dev/null."""
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+
+    t = time.perf_counter()
+    oracle_lib.reference_dispfield(params, grid, sp, jp)
+    return time.perf_counter() - t
+
+
+def measure_jeans(model, steps, cpu):
+    """calculate_dispfield through the C ABI on the workload's 256^2 force
+    grid (halo: spherical and f(E, Lz) tables; disk: also the tilted method
+    of lines), host copies of every table included, in a context of its own."""
+    from galic_b200 import Context, jeans
+
+    sp, jp = jeans_inputs(model)
+    with Context(model.params) as c:
+        c.load_model(model)
+        jeans.calculate_dispfield(c, sp, jp)
+        walls = []
+        for _ in range(max(steps, 1)):
+            t = time.perf_counter()
+            jeans.calculate_dispfield(c, sp, jp)
+            walls.append(time.perf_counter() - t)
+        launches = c.last_kernel_launches()
+    ms = statistics.mean(walls) * 1e3
+    res = {"ms_per_call_e2e": ms, "fg_nbin": model.params.FG_Nbin,
+           "velocity_structures": {t: model.params.TypeOfVelocityStructure[t] for t in (1, 2, 3)
+                                   if model.params.NType[t] > 0},
+           "parameters": "synthetic: disk DispersionRoverZratio 1.5, StreamingVelocityParameter 0.8",
+           "gpu_launches": launches}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+
+        sec = oracle_lib.run_reference(_ref_jeans_timed, model.params, (model.pot, model.dpotdr, model.dpotdz), sp, jp)
+        res["cpu_baseline"] = {"ms_per_call": sec * 1e3, "cores": 1, "kind": "reference",
+                               "sample": "GALIC's own calculate_dispfield, the whole call, one rank"}
+        res["speedup_e2e_vs_cpu"] = sec * 1e3 / ms
+    return res
+
+
 def measure_ensemble(count, steps):
     """Batched ensemble: `count` Hernquist halos of uneven N advanced per
     iteration by one persistent FP32 launch replayed from a CUDA graph, tile
@@ -601,6 +655,7 @@ def ours_arm(args, rank, world, local_rank):
         fill = measure_fill(model, args.steps, world == 1 and args.cpu_seconds > 0,
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
         target_sampling = measure_sampling(model, ctx, args.steps, world == 1 and args.cpu_seconds > 0)
+        jeans_solve = measure_jeans(model, args.steps, world == 1 and args.cpu_seconds > 0)
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
         serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
@@ -635,6 +690,7 @@ def ours_arm(args, rank, world, local_rank):
                 "cpu_baseline": cpu,
                 "force_grid_fill": fill,
                 "target_sampling": target_sampling,
+                "jeans": jeans_solve,
                 "ensemble": ensemble,
                 "serving": serving,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
