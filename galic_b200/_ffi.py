@@ -124,6 +124,12 @@ class GalicJeansTables(C.Structure):
                                                       "tilted_vR2", "tilted_vz2_prime", "tilted_vR2_prime")]
 
 
+class GalicParticlesOut(C.Structure):
+    """galic_particles_out_t."""
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in ("pos", "vel", "vel_theo", "mass", "vesc", "tint", "targets")] + \
+               [(n, C.POINTER(C.c_int)) for n in ("type", "id", "permutation")] + [("low_disp", I4 * 4)]
+
+
 JEANS_TABLES = ("disp_r", "dispz", "dispphi", "vstream", "tilted_vz2", "tilted_vR2", "tilted_vz2_prime",
                 "tilted_vR2_prime")
 
@@ -207,6 +213,8 @@ SIGNATURES = [
     ("galic_get_targets", C.c_int, [VP, C.c_int, PD, PD, PD, PD, PD, PD]),
     ("galic_calculate_dispfield", C.c_int,
      [VP, C.POINTER(GalicSampleParams), C.POINTER(GalicJeansParams), C.POINTER(GalicJeansTables)]),
+    ("galic_initialize_particles", C.c_int,
+     [VP, C.POINTER(GalicSampleParams), C.c_double, C.POINTER(GalicStream), C.POINTER(GalicParticlesOut)]),
     ("galic_sample_positions", C.c_int,
      [C.POINTER(GalicSampleParams), C.c_int, C.c_longlong, C.POINTER(GalicStream), PD]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),

@@ -30,9 +30,12 @@
  *  - sin/cos: Cody & Waite three-part reduction by pi/2 (heads with 33
  *           significant bits), Taylor polynomials on |r| <= pi/4.  Accurate
  *           for |x| < 2^20; the orbit path only uses |x| <= pi.
- *  - acos:  acos(x) = atan2(sqrt((1-x)(1+x)), x).
+ *  - acos:  acos(x) = atan2(sqrt((1-x)(1+x)), x); asin(x) = atan2(x, sqrt((1-x)(1+x))).
+ *  - exp:   Cody & Waite reduction by ln2 (same split as log), Taylor series
+ *           of degree 13, scaling by 2^k in two steps.
  * Measured against glibc over random arguments the error is within 1 ulp for
- * log, sin and cos and within 2 ulp for atan2 and acos (tests/test_gmath.py).
+ * log, exp, sin and cos and within 2 ulp for atan2, acos and asin
+ * (tests/test_gmath.py).
  */
 #ifndef GALIC_GMATH_H
 #define GALIC_GMATH_H
@@ -311,6 +314,21 @@ GM_HD double gm_acos(double x)
   double q = __builtin_sqrt(s);
 #endif
   return gm_atan2(q, x);
+}
+
+/* ---------------------------------------------------------------- asin */
+/* asin(x) = atan2(x, sqrt((1-x)(1+x))), the companion of gm_acos */
+GM_HD double gm_asin(double x)
+{
+  if(gm_isnan(x)) return x;
+  if(x > 1.0 || x < -1.0) return GM_NAN;
+  double s = (1.0 - x) * (1.0 + x);
+#ifdef __CUDA_ARCH__
+  double q = __dsqrt_rn(s);
+#else
+  double q = __builtin_sqrt(s);
+#endif
+  return gm_atan2(x, q);
 }
 
 #endif

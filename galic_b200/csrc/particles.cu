@@ -1,0 +1,495 @@
+// initialize_particles (set_particles.c:15-307) on the GPU.
+//
+// The reference draws every particle from one sequential stream: particle
+// n starts where particle n-1 stopped, and how many draws a particle takes
+// depends on its rejection loops (position inside Rmax, the Hernquist
+// velocity by von Neumann rejection, the Gaussian velocity below the escape
+// speed, Marsaglia's polar method).  The replay here finds every particle's
+// first draw in parallel:
+//  * k_len: for EVERY stream position o of a type's segment, the number of
+//    draws one particle initialisation takes when it starts at o
+//    (next[o] = o + len).  Any position starts a valid initialisation, so
+//    this is a fully parallel map, about 20 positions per particle;
+//  * k_lift: binary lifting of the successor function, J_k = J_(k-1) o J_(k-1)
+//    (J_0 = next); particle n starts at J applied n times to the segment
+//    start, read off the bits of n (k_starts);
+//  * k_final: each particle is initialised once more from its start, this
+//    time keeping its values; then one uniform per particle after the last
+//    draw and a radix sort give the permutation.
+// Two sinks close the successor function: R (the segment's positions ran
+// out: the segment is enlarged and the type redone) and R + 1 (a rejection
+// loop hit its cap of 10^6 tries).  Built with --fmad=false and gmath.h's
+// functions, so every particle is bit-identical to the CPU restatement.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "context.cuh"
+#include "galic_gpu.h"
+#include "grng.h"
+#include "model.cuh"
+#include "setup.cuh"
+
+namespace {
+
+constexpr int LOOP_CAP = 1000000;     // tries of every rejection loop
+constexpr uint32_t LEN_CAPPED = 0xffffffffu;
+constexpr int PROBE = 1 << 16;        // positions of the draws-per-particle estimate
+constexpr int PBLOCK = 128;
+
+struct PInit {
+  DevModel M;
+  Shape S;
+  DispTab D[4];
+  uint64_t seed;
+  uint32_t sa, sb;
+  double MaxVel, LowerDispLimit, TorbitFac;
+};
+
+struct POut {
+  double *pos, *vel, *vel_theo, *vesc, *tint, *targets;
+  int *counts;  // [4][4]
+};
+
+// halo_get_potential_from_radius (halo.c:69-73)
+__device__ __forceinline__ double halo_pot_r(const DevModel &M, double r) { return -M.G * M.Halo_Mass / (r + M.Halo_A); }
+
+// halo_f_q (halo.c:136-147): pow(x, 1.5) = x sqrt(x), pow(x, 2.5) = x x sqrt(x)
+__device__ double halo_f_q(const DevModel &M, double q)
+{
+  const double c = 2 * M.G * M.Halo_Mass / M.Halo_A;
+  double pre = (M.Halo_Mass / (M.Halo_A * M.Halo_A * M.Halo_A)) / (4 * kPi * kPi * kPi * (c * sqrt(c)));
+  const double u = 1 - q * q;
+  return pre * (3 * gm_asin(q) + q * sqrt(1 - q * q) * (1 - 2 * q * q) * (8 * q * q * q * q - 8 * q * q - 3)) /
+         (u * u * sqrt(u));
+}
+
+// halo_f (halo.c:151-157) with halo_E_to_q (halo.c:113-116)
+__device__ __forceinline__ double halo_f(const DevModel &M, double rad, double vel)
+{
+  double E = 0.5 * vel * vel + halo_pot_r(M, rad);
+  double q = sqrt(-E * M.Halo_A / (M.G * M.Halo_Mass));
+  return halo_f_q(M, q);
+}
+
+// one call of the type's *_get_fresh_coordinate from the stream g
+// (halo.c:17-40, disk.c:17-50, bulge.c:15-37); false when capped
+__device__ bool fresh_seq(const Shape &S, int type, grng_t &g, double *pos)
+{
+  if(type == 1 || type == 2) {
+    for(int it = 0; it < LOOP_CAP; it++) {
+      const double d0 = grng_uniform(&g), d1 = grng_uniform(&g), d2 = grng_uniform(&g);
+      if(type == 1 ? halo_draw(S, d0, d1, d2, pos) : disk_draw(S, d0, d1, d2, pos)) return true;
+    }
+    return false;
+  }
+  for(int it = 0; it < LOOP_CAP; it++) {
+    const double r = bulge_radius(S, grng_uniform(&g));
+    if(!(r > S.Rmax)) {
+      const double d1 = grng_uniform(&g), d2 = grng_uniform(&g);
+      bulge_place(S, r, d1, d2, pos);
+      return true;
+    }
+  }
+  return false;
+}
+
+// one iteration of initialize_particles' loop (set_particles.c:64-237) from
+// stream position `start`; returns the draws it took (LEN_CAPPED when a
+// rejection loop hit its cap).  With o != nullptr the particle's values are
+// stored at index n.
+__device__ uint32_t init_one(const PInit &P, int type, uint64_t start, const POut *o, int n)
+{
+  grng_t g;
+  grng_init(&g, P.seed, P.sa, P.sb);
+  grng_seek(&g, start);
+  const DevModel &M = P.M;
+  const LogConsts L = make_log_consts(M);
+  double pos[3];
+  if(!fresh_seq(P.S, type, g, pos)) return LEN_CAPPED;
+  // forcegrid_get_escape_speed (grid.c:115-120), the acceleration, Tint
+  const double vesc = sqrt(-2.0 * forcegrid_pot(M, L, pos));
+  double acc[3];
+  const FgCoord fc = fg_coord(M, L, pos);
+  forcegrid_acc(M, fc, pos, acc);
+  const double a = sqrt(acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2]);
+  const double r = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+  const double tint = P.TorbitFac * 2 * kPi * r / sqrt(r * a);
+  double vt[3] = {0, 0, 0};
+  if(type == 1) {
+    // halo_generate_v (halo.c:168-184) until below MaxVelInUnitsVesc Vesc
+    double vr = 0;
+    int outer = 0;
+    do {
+      if(++outer > LOOP_CAP) return LEN_CAPPED;
+      const double pot = halo_pot_r(M, r);
+      const double v_max = sqrt(-2 * pot);
+      const double f_max = v_max * v_max * halo_f(M, r, 0);
+      double v_guess = grng_uniform(&g) * v_max;
+      double x_aux = grng_uniform(&g) * f_max;
+      int it = 0;
+      while(x_aux > v_guess * v_guess * halo_f(M, r, v_guess)) {
+        if(++it > LOOP_CAP) return LEN_CAPPED;
+        v_guess = grng_uniform(&g) * v_max;
+        x_aux = grng_uniform(&g) * f_max;
+      }
+      vr = v_guess;
+    } while(vr >= P.MaxVel * vesc);
+    const double phi = grng_uniform(&g) * kPi * 2;
+    const double theta = gm_acos(grng_uniform(&g) * 2 - 1);
+    vt[0] = vr * gm_sin(theta) * gm_cos(phi);
+    vt[1] = vr * gm_sin(theta) * gm_sin(phi);
+    vt[2] = vr * gm_cos(theta);
+  }
+  const DispTab &D = P.D[type];
+  double d[4];
+  disp_rtp(D, pos, d);
+  int low[4];
+  for(int k = 0; k < 4; k++) {
+    low[k] = d[k] <= P.LowerDispLimit;
+    if(low[k]) d[k] = P.LowerDispLimit;
+  }
+  // get_vstream (disp_fields.c:118-132)
+  const double vstr = vstream_at(M, fc, type);
+  double V[3];
+  const double sigmaR = sqrt(d[0]), sigmaT = sqrt(d[1]), sigmaP = sqrt(d[2]);
+  if(D.tovs == 0 || D.tovs == 1 || D.tovs == 3) {
+    double v, vr, vphi, vtheta;
+    int it = 0;
+    do {
+      if(++it > LOOP_CAP) return LEN_CAPPED;
+      vr = grng_gaussian(&g, sigmaR);
+      vtheta = grng_gaussian(&g, sigmaT);
+      vphi = grng_gaussian(&g, sigmaP);
+      vphi += vstr;
+      v = sqrt(vr * vr + vphi * vphi + vtheta * vtheta);
+    } while(P.MaxVel * vesc < v);
+    if(o) {
+      const double phi = gm_atan2(pos[1], pos[0]);
+      const double theta = gm_acos(pos[2] / sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]));
+      const double st = gm_sin(theta), ct = gm_cos(theta), sp = gm_sin(phi), cp = gm_cos(phi);
+      const double er[3] = {st * cp, st * sp, ct};
+      const double ePhi[3] = {-sp, cp, 0};
+      const double eTheta[3] = {-ct * cp, -ct * sp, st};
+      for(int k = 0; k < 3; k++) V[k] = vr * er[k] + vphi * ePhi[k] + vtheta * eTheta[k];
+    }
+  } else {
+    double v, vR, vphi, vz;
+    int it = 0;
+    do {
+      if(++it > LOOP_CAP) return LEN_CAPPED;
+      vR = grng_gaussian(&g, sigmaR);
+      vz = grng_gaussian(&g, sigmaT);
+      vphi = grng_gaussian(&g, sigmaP);
+      vphi += vstr;
+      v = sqrt(vR * vR + vphi * vphi + vz * vz);
+    } while(v >= P.MaxVel * vesc);
+    if(o) {
+      const double phi = gm_atan2(pos[1], pos[0]);
+      const double sp = gm_sin(phi), cp = gm_cos(phi);
+      const double eR[3] = {cp, sp, 0};
+      const double ePhi[3] = {-sp, cp, 0};
+      const double eZ[3] = {0, 0, 1};
+      for(int k = 0; k < 3; k++) V[k] = vR * eR[k] + vphi * ePhi[k] + vz * eZ[k];
+    }
+  }
+  const uint64_t len = grng_position(&g) - start;
+  if(o) {
+    for(int k = 0; k < 3; k++) {
+      o->pos[3 * n + k] = pos[k];
+      o->vel[3 * n + k] = V[k];
+      o->vel_theo[3 * n + k] = vt[k];
+    }
+    o->vesc[n] = vesc;
+    o->tint[n] = tint;
+    for(int k = 0; k < 4; k++) {
+      o->targets[4 * n + k] = d[k];
+      if(low[k]) atomicAdd(&o->counts[4 * type + k], 1);
+    }
+  }
+  return len >= LEN_CAPPED ? LEN_CAPPED : (uint32_t) len;
+}
+
+// J_0 over positions [0, R) of the segment starting at `base`; R and R + 1 are
+// the overflow and capped sinks
+__global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, int type, uint64_t base, uint32_t R, uint32_t *next)
+{
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if(o >= R + 2) return;
+  if(o >= R) {
+    next[o] = o;
+    return;
+  }
+  const uint32_t len = init_one(P, type, base + o, nullptr, 0);
+  const uint64_t e = (uint64_t) o + len;
+  next[o] = (len == LEN_CAPPED) ? R + 1 : (e < R ? (uint32_t) e : R);
+}
+
+__global__ void k_lift(const uint32_t *J, uint32_t *J2, uint32_t n)
+{
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if(o < n) J2[o] = J[J[o]];
+}
+
+// start of particle i of the segment (i <= count; i = count is the end)
+__global__ void k_starts(const uint32_t *J, size_t stride, int levels, int count, uint32_t *starts)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i > count) return;
+  uint32_t o = 0;
+  for(int k = 0; k < levels; k++)
+    if((i >> k) & 1) o = J[(size_t) k * stride + o];
+  starts[i] = o;
+}
+
+__global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, int type, uint64_t base, const uint32_t *starts,
+                                                  int count, int n0, POut o)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= count) return;
+  init_one(P, type, base + starts[i], &o, n0 + i);
+}
+
+// permutation[].rnd (set_particles.c:298-301): the bits of a uniform in [0, 1)
+// order like the value
+__global__ void k_perm_keys(uint64_t seed, uint32_t sa, uint32_t sb, uint64_t first, int n, unsigned long long *keys,
+                            int *vals)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  keys[i] = gm_bits(grng_uniform_at(seed, sa, sb, first + (uint64_t) i));
+  vals[i] = i;
+}
+
+#define PCK(call)                                                                             \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if(e_ != cudaSuccess) {                                                                   \
+      fprintf(stderr, "galic_cuda: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                      \
+      rc = GALIC_ERR_CUDA;                                                                    \
+      goto done;                                                                              \
+    }                                                                                         \
+  } while(0)
+
+int pfail(galic_ctx *ctx, int st)
+{
+  if(ctx) ctx->status = st;
+  return st;
+}
+
+inline unsigned gblocks(long long n, int b) { return (unsigned) ((n + b - 1) / b); }
+
+}  // namespace
+
+extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_params_t *sp, double TorbitFac,
+                                          galic_stream_t *stream, galic_particles_out_t *out)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(!sp || !stream) return pfail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  const galic_params_t &p = ctx->prm;
+  const int nt[4] = {0, p.NType[1], p.NType[2], p.NType[3]};
+  const long long Nll = (long long) nt[1] + nt[2] + nt[3];
+  if(nt[1] < 0 || nt[2] < 0 || nt[3] < 0 || Nll < 1 || Nll > (1ll << 28)) return pfail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  const int N = (int) Nll;
+  if(!ctx->have_fg) return pfail(ctx, GALIC_ERR_STATE);
+  for(int t = 1; t <= 3; t++)
+    if(nt[t] > 0 && (!ctx->have_disp[t] || !ctx->d_vstream[t] || ctx->h_vstream[t].empty()))
+      return pfail(ctx, GALIC_ERR_STATE);
+  if(cudaSetDevice(ctx->device)) return pfail(ctx, GALIC_ERR_CUDA);
+  cudaStream_t s = ctx->stream;
+  int rc = GALIC_OK, launches = 0;
+  double *d_f = nullptr;  // pos, vel, vel_theo (3N each), vesc, tint (N each), targets (4N)
+  int *d_counts = nullptr, *d_vals = nullptr, *d_vals2 = nullptr;
+  uint32_t *d_J = nullptr, *d_starts = nullptr;
+  unsigned long long *d_keys = nullptr, *d_keys2 = nullptr;
+  void *d_tmp = nullptr;
+  size_t J_cap = 0;
+  std::vector<double> h_f;
+  std::vector<int> h_counts(16), h_perm;
+  uint64_t pos = stream->position;
+  PInit P{};
+  POut O{};
+  P.M = ctx->dm;
+  P.S.Rmax = sp->Rmax;
+  P.S.Halo_A = sp->Halo_A;
+  P.S.HaloStretch = sp->HaloStretch;
+  P.S.Disk_Z0 = sp->Disk_Z0;
+  P.S.Disk_H = sp->Disk_H;
+  P.S.Bulge_A = sp->Bulge_A;
+  P.S.BulgeStretch = sp->BulgeStretch;
+  P.seed = stream->seed;
+  P.sa = stream->a;
+  P.sb = stream->b;
+  P.MaxVel = p.MaxVelInUnitsVesc;
+  P.LowerDispLimit = p.LowerDispLimit;
+  P.TorbitFac = TorbitFac;
+  for(int t = 1; t <= 3; t++) {
+    DispTab &D = P.D[t];
+    D.disp_r = ctx->d_disp[t][0];
+    D.dispz = ctx->d_disp[t][1];
+    D.dispphi = ctx->d_disp[t][2];
+    D.tvr2 = ctx->d_disp[t][3];
+    D.tvz2 = ctx->d_disp[t][4];
+    D.vstream = ctx->d_vstream[t];
+    D.tovs = p.TypeOfVelocityStructure[t];
+    D.beta = (t == 1) ? sp->HaloBetaParameter : (t == 3 ? sp->BulgeBetaParameter : 0.0);
+    D.beta_a = (t == 1) ? p.Halo_A : p.Bulge_A;
+    D.FG_Rmin = p.FG_Rmin;
+    D.lfg = gm_log(p.FG_Fac);
+    D.FG_Nbin = p.FG_Nbin;
+  }
+  PCK(cudaMallocAsync((void **) &d_f, (size_t) 15 * N * sizeof(double), s));
+  PCK(cudaMallocAsync((void **) &d_counts, 16 * sizeof(int), s));
+  PCK(cudaMemsetAsync(d_f, 0, (size_t) 15 * N * sizeof(double), s));
+  PCK(cudaMemsetAsync(d_counts, 0, 16 * sizeof(int), s));
+  O.pos = d_f;
+  O.vel = d_f + 3 * (size_t) N;
+  O.vel_theo = d_f + 6 * (size_t) N;
+  O.vesc = d_f + 9 * (size_t) N;
+  O.tint = d_f + 10 * (size_t) N;
+  O.targets = d_f + 11 * (size_t) N;
+  O.counts = d_counts;
+  {
+    int n0 = 0;
+    for(int t = 1; t <= 3 && rc == GALIC_OK; n0 += nt[t], t++) {
+      if(nt[t] == 0) continue;
+      // draws per particle, from the lengths at the segment's first positions
+      uint32_t R = PROBE;
+      std::vector<uint32_t> probe(PROBE + 2);
+      if(J_cap < (size_t) R + 2) {
+        if(d_J) cudaFreeAsync(d_J, s);
+        J_cap = (size_t) R + 2;
+        PCK(cudaMallocAsync((void **) &d_J, J_cap * sizeof(uint32_t), s));
+      }
+      k_len<<<gblocks(R + 2, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, R, d_J);
+      launches++;
+      PCK(cudaGetLastError());
+      PCK(cudaMemcpyAsync(probe.data(), d_J, (R + 2) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      PCK(cudaStreamSynchronize(s));
+      double sum = 0;
+      long long valid = 0;
+      for(uint32_t o = 0; o < R; o++)
+        if(probe[o] < R && probe[o] > o) {
+          sum += probe[o] - o;
+          valid++;
+        }
+      if(valid < PROBE / 2) {  // most starts end in a capped loop
+        rc = GALIC_ERR_REJECTION_CAP;
+        break;
+      }
+      double per = sum / valid;
+      for(int attempt = 0;; attempt++) {
+        const double want = (double) nt[t] * per * (1.15 + 0.5 * attempt) + 4096;
+        if(want > 4.0e9) {
+          rc = GALIC_ERR_UNSUPPORTED;
+          break;
+        }
+        R = (uint32_t) want;
+        int levels = 1;
+        while((1ll << levels) <= nt[t]) levels++;
+        const size_t stride = (size_t) R + 2;
+        if(stride * levels * sizeof(uint32_t) > (32ull << 30)) {  // the lifting tables' budget
+          rc = GALIC_ERR_UNSUPPORTED;
+          break;
+        }
+        if(J_cap < stride * levels) {
+          cudaFreeAsync(d_J, s);
+          J_cap = stride * levels;
+          PCK(cudaMallocAsync((void **) &d_J, J_cap * sizeof(uint32_t), s));
+        }
+        k_len<<<gblocks(stride, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, R, d_J);
+        for(int k = 1; k < levels; k++)
+          k_lift<<<gblocks(stride, 256), 256, 0, s>>>(d_J + (k - 1) * stride, d_J + k * stride, (uint32_t) stride);
+        if(d_starts) cudaFreeAsync(d_starts, s);
+        PCK(cudaMallocAsync((void **) &d_starts, ((size_t) nt[t] + 1) * sizeof(uint32_t), s));
+        k_starts<<<gblocks((long long) nt[t] + 1, 256), 256, 0, s>>>(d_J, stride, levels, nt[t], d_starts);
+        launches += levels + 1;
+        PCK(cudaGetLastError());
+        uint32_t end = 0;
+        PCK(cudaMemcpyAsync(&end, d_starts + nt[t], sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        PCK(cudaStreamSynchronize(s));
+        if(end == R + 1) {
+          rc = GALIC_ERR_REJECTION_CAP;
+          break;
+        }
+        if(end == R) continue;  // the segment was too short: enlarge it
+        k_final<<<gblocks(nt[t], PBLOCK), PBLOCK, 0, s>>>(P, t, pos, d_starts, nt[t], n0, O);
+        launches++;
+        PCK(cudaGetLastError());
+        pos += end;
+        break;
+      }
+    }
+  }
+  if(rc != GALIC_OK) goto done;
+  h_f.resize((size_t) 15 * N);
+  PCK(cudaMemcpyAsync(h_f.data(), d_f, h_f.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PCK(cudaMemcpyAsync(h_counts.data(), d_counts, 16 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  PCK(cudaStreamSynchronize(s));
+  for(int t = 1; t <= 3; t++)
+    for(int k = 0; k < 4; k++)
+      if(nt[t] > 0 && (double) h_counts[4 * t + k] / nt[t] > 0.05) rc = GALIC_ERR_UNSUPPORTED;
+  if(rc == GALIC_OK) {
+    // the permutation (set_particles.c:298-303)
+    size_t tb = 0;
+    PCK(cudaMallocAsync((void **) &d_keys, (size_t) N * sizeof(unsigned long long), s));
+    PCK(cudaMallocAsync((void **) &d_keys2, (size_t) N * sizeof(unsigned long long), s));
+    PCK(cudaMallocAsync((void **) &d_vals, (size_t) N * sizeof(int), s));
+    PCK(cudaMallocAsync((void **) &d_vals2, (size_t) N * sizeof(int), s));
+    k_perm_keys<<<gblocks(N, 256), 256, 0, s>>>(P.seed, P.sa, P.sb, pos, N, d_keys, d_vals);
+    PCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_keys, d_keys2, d_vals, d_vals2, N, 0, 64, s));
+    PCK(cudaMallocAsync(&d_tmp, std::max<size_t>(tb, 16), s));
+    PCK(cub::DeviceRadixSort::SortPairs(d_tmp, tb, d_keys, d_keys2, d_vals, d_vals2, N, 0, 64, s));
+    launches += 2;
+    h_perm.resize(N);
+    PCK(cudaMemcpyAsync(h_perm.data(), d_vals2, (size_t) N * sizeof(int), cudaMemcpyDeviceToHost, s));
+    PCK(cudaStreamSynchronize(s));
+    pos += (uint64_t) N;
+  }
+done:
+  for(void *q : {(void *) d_f, (void *) d_counts, (void *) d_vals, (void *) d_vals2, (void *) d_J, (void *) d_starts,
+                 (void *) d_keys, (void *) d_keys2, d_tmp})
+    if(q) cudaFreeAsync(q, s);
+  cudaStreamSynchronize(s);
+  ctx->last_launches = launches;
+  if(rc != GALIC_OK && rc != GALIC_ERR_UNSUPPORTED) return pfail(ctx, rc);
+  // host arrays in P order
+  std::vector<double> mass(N), tintv(N);
+  std::vector<int> type(N), id(N);
+  {
+    const double tm[4] = {0, p.Halo_Mass, p.Disk_Mass, p.Bulge_Mass};
+    int n = 0;
+    for(int t = 1; t <= 3; t++)
+      for(int i = 0; i < nt[t]; i++, n++) {
+        type[n] = t;
+        mass[n] = tm[t] / nt[t];
+        id[n] = n + 1;
+      }
+  }
+  const double *F = h_f.data();
+  if(out) {
+    double *dst[6] = {out->pos, out->vel, out->vel_theo, out->vesc, out->tint, out->targets};
+    const size_t off[6] = {0, 3, 6, 9, 10, 11}, len[6] = {3, 3, 3, 1, 1, 4};
+    for(int k = 0; k < 6; k++)
+      if(dst[k]) std::copy(F + off[k] * N, F + (off[k] + len[k]) * N, dst[k]);
+    if(out->mass) std::copy(mass.begin(), mass.end(), out->mass);
+    if(out->type) std::copy(type.begin(), type.end(), out->type);
+    if(out->id) std::copy(id.begin(), id.end(), out->id);
+    if(out->permutation && rc == GALIC_OK) std::copy(h_perm.begin(), h_perm.end(), out->permutation);
+    for(int t = 0; t < 4; t++)
+      for(int k = 0; k < 4; k++) out->low_disp[t][k] = h_counts[4 * t + k];
+  }
+  if(rc != GALIC_OK) return pfail(ctx, rc);
+  // the particles become the context's
+  rc = galic_set_particles(ctx, N, F, F + 3 * (size_t) N, mass.data(), F + 10 * (size_t) N, F + 9 * (size_t) N,
+                           type.data(), F + 11 * (size_t) N);
+  if(rc != GALIC_OK) return rc;
+  ctx->last_launches = launches;
+  stream->position = pos;
+  return pfail(ctx, GALIC_OK);
+}

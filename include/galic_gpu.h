@@ -454,6 +454,44 @@ typedef struct {
 int galic_calculate_dispfield(galic_ctx *ctx, const galic_sample_params_t *sp, const galic_jeans_params_t *jp,
                               galic_jeans_tables_t *out);
 
+/* ------------------------------------------------- particle initialisation */
+
+/* The particle state initialize_particles writes (P[], allvars.h:844-868, and
+ * permutation[], allvars.h:525-530), host arrays of NumPart entries (times 3
+ * or 4 where noted), in P order; a NULL array is skipped. */
+typedef struct {
+  double *pos;       /* 3n: P[].Pos */
+  double *vel;       /* 3n: P[].Vel */
+  double *vel_theo;  /* 3n: P[].VelTheo (halo particles; 0 for the others) */
+  double *mass;      /* n: P[].Mass */
+  double *vesc;      /* n: P[].Vesc */
+  double *tint;      /* n: P[].Tint */
+  double *targets;   /* 4n: P[].vr2_target, vt2_target, vp2_target, vq2_target */
+  int *type;         /* n: P[].Type */
+  int *id;           /* n: P[].ID */
+  int *permutation;  /* n: permutation[].index after the sort (set_particles.c:298-303) */
+  int low_disp[4][4]; /* per type: particles whose r, t, p, q dispersion was raised to LowerDispLimit */
+} galic_particles_out_t;
+
+/* Replaces initialize_particles (set_particles.c:15-307) with one rank:
+ * NType[t] particles of each type in P order (halo, disk, bulge), each with
+ * its position (the type's *_get_fresh_coordinate), Vesc and Tint
+ * (TorbitFac), for halo particles VelTheo from the Hernquist distribution
+ * function (halo.c:168-184), the Jeans dispersion targets (get_disp_rtp,
+ * raised to LowerDispLimit) and a velocity from three Gaussians redrawn while
+ * faster than MaxVelInUnitsVesc Vesc; then one uniform per particle and the
+ * permutation sorted by it.  The draws are those the reference's sequential
+ * loop takes from `stream`, which comes back advanced past them.  Needs the
+ * force grid and, per type with particles, FG_Vstream and the Jeans tables
+ * (galic_set_vstream + galic_set_dispersion, or galic_calculate_dispfield).
+ * The particles become the context's, as after galic_set_particles.
+ * GALIC_ERR_UNSUPPORTED when more than 5 % of a type had a dispersion raised
+ * to LowerDispLimit (the reference's endrun(), set_particles.c:261-282);
+ * GALIC_ERR_REJECTION_CAP when a rejection loop on the draws' path ran past
+ * 10^6 tries (where the reference would keep drawing). */
+int galic_initialize_particles(galic_ctx *ctx, const galic_sample_params_t *sp, double TorbitFac,
+                               galic_stream_t *stream, galic_particles_out_t *out);
+
 /* ---------------------------------------------------------- host helpers */
 
 /* Grid geometry of forcedensitygrid_create (grid.c:329-480): from Halo_A,

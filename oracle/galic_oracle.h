@@ -121,4 +121,12 @@ void orc_sample_energy(const galic_params_t *p, const galic_sample_params_t *sp,
 int orc_calculate_dispfield(orc_model *m, const galic_sample_params_t *sp, const galic_jeans_params_t *jp,
                             double *out);
 
+/* initialize_particles (set_particles.c:15-307), one rank; oracle_particles.c.
+ * tab[t] = {FG_Disp_r, FG_DispZ, FG_DispPhi, FG_tilted_vR2_prime,
+ * FG_tilted_vz2_prime, FG_Vstream} of type t. */
+int orc_initialize_particles(orc_model *m, const galic_sample_params_t *sp, double TorbitFac,
+                             const double *const *const *tab, galic_stream_t *stream, int use_libm, double *pos,
+                             double *vel, double *vel_theo, double *mass, double *vesc, double *tint,
+                             double *targets, int *type, int *id, int *perm, int *counts);
+
 #endif

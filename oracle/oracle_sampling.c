@@ -23,8 +23,7 @@
 #include <string.h>
 
 #include "galic_oracle.h"
-#include "../galic_b200/csrc/gmath.h"
-#include "../galic_b200/csrc/grng.h"
+#include "oracle_internal.h"
 
 typedef struct {
   int use_libm;
@@ -99,6 +98,12 @@ static void bulge_fresh(const smath *m, const galic_sample_params_t *sp, grng_t 
 }
 
 /* the dispatch of grid.c:563-568 */
+static void fresh(const smath *m, const galic_sample_params_t *sp, int type, grng_t *g, double *pos);
+void orc_fresh(int use_libm, const galic_sample_params_t *sp, int type, grng_t *g, double *pos)
+{
+  smath m = {use_libm};
+  fresh(&m, sp, type, g, pos);
+}
 static void fresh(const smath *m, const galic_sample_params_t *sp, int type, grng_t *g, double *pos)
 {
   if(type == 1)
@@ -279,6 +284,19 @@ static double beta_of(const galic_sample_params_t *sp, int type, const double *p
 
 /* get_disp_rtp (disp_fields.c:66-115); tab: disp_r, dispz, dispphi,
  * tilted_vr2, tilted_vz2, vstream */
+static void disp_rtp(const smath *m, const galic_params_t *p, const galic_sample_params_t *sp, int type,
+                     const double *const *tab, const double *pos, double *dr, double *dt, double *dp, double *dq);
+void orc_disp_rtp(int use_libm, const galic_params_t *p, const galic_sample_params_t *sp, int type,
+                  const double *const *tab, const double *pos, double *d)
+{
+  smath m = {use_libm};
+  disp_rtp(&m, p, sp, type, tab, pos, &d[0], &d[1], &d[2], &d[3]);
+}
+double orc_vstream_tab(int use_libm, const galic_params_t *p, const double *vstream, const double *pos)
+{
+  smath m = {use_libm};
+  return fg_interp(&m, p, vstream, pos);
+}
 static void disp_rtp(const smath *m, const galic_params_t *p, const galic_sample_params_t *sp, int type,
                      const double *const *tab, const double *pos, double *dr, double *dt, double *dp, double *dq)
 {

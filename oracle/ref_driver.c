@@ -480,3 +480,40 @@ void ref_get_jeans(int type, double *out)
                     FG_tilted_vz2[type], FG_tilted_vR2[type], FG_tilted_vz2_prime[type], FG_tilted_vR2_prime[type]};
   for(int k = 0; k < 8; k++) memcpy(out + (size_t) k * FG_Ngrid, src[k], FG_Ngrid * sizeof(double));
 }
+
+/* ------------------------------------------------------- particle initialisation */
+
+/* initialize_particles (set_particles.c:15-307) with TorbitFac and the
+ * sampler shapes; its fit_*.txt files go to outdir.  Returns NumPart. */
+int ref_initialize_particles(const char *outdir, const galic_sample_params_t *sp, double TorbitFac)
+{
+  ref_sample_setup(sp, 1);
+  All.TorbitFac = TorbitFac;
+  if(strlen(outdir) >= sizeof(All.OutputDir)) return -1;
+  strcpy(All.OutputDir, outdir);
+  initialize_particles();
+  return NumPart;
+}
+
+/* P[] and permutation[] after initialize_particles */
+void ref_get_init_particles(double *pos, double *vel, double *vel_theo, double *mass, double *vesc, double *tint,
+                            double *targets, int *type, int *id, int *perm)
+{
+  for(int n = 0; n < NumPart; n++) {
+    for(int k = 0; k < 3; k++) {
+      pos[3 * n + k] = P[n].Pos[k];
+      vel[3 * n + k] = P[n].Vel[k];
+      vel_theo[3 * n + k] = P[n].VelTheo[k];
+    }
+    mass[n] = P[n].Mass;
+    vesc[n] = P[n].Vesc;
+    tint[n] = P[n].Tint;
+    targets[4 * n] = P[n].vr2_target;
+    targets[4 * n + 1] = P[n].vt2_target;
+    targets[4 * n + 2] = P[n].vp2_target;
+    targets[4 * n + 3] = P[n].vq2_target;
+    type[n] = P[n].Type;
+    id[n] = (int) P[n].ID;
+    perm[n] = permutation[n].index;
+  }
+}

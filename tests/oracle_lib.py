@@ -82,6 +82,8 @@ def oracle_lib():
             "orc_force_grid_fill": (C.c_int, [C.POINTER(_ffi.GalicFillParams), C.c_int, PD, PD, PD, PD, PD]),
             "orc_sample_positions": (None, [PSP, C.c_int, C.c_longlong, PST, C.c_int, PD]),
             "orc_calculate_dispfield": (C.c_int, [VP, PSP, PJP, PD]),
+            "orc_initialize_particles": (C.c_int, [VP, PSP, C.c_double, C.POINTER(C.POINTER(PD)), PST, C.c_int,
+                                                   PD, PD, PD, PD, PD, PD, PD, PI, PI, PI, PI]),
             "orc_sample_density": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.c_int, PD]),
             "orc_sample_energy": (None, [PP, PSP, C.c_int, C.c_longlong, PST, C.c_int, C.POINTER(PD), PD]),
         }
@@ -342,6 +344,65 @@ def reference_dispfield(params, m_arrays, sp, jp):
     return out
 
 
+PARTICLE_FIELDS = (("pos", 3, np.float64), ("vel", 3, np.float64), ("vel_theo", 3, np.float64),
+                   ("mass", 1, np.float64), ("vesc", 1, np.float64), ("tint", 1, np.float64),
+                   ("targets", 4, np.float64), ("type", 1, np.int32), ("id", 1, np.int32), ("perm", 1, np.int32))
+
+
+def _particle_arrays(n):
+    return {k: np.zeros((n, w) if w > 1 else n, dtype=dt) for k, w, dt in PARTICLE_FIELDS}
+
+
+def _ptr(a):
+    return dptr(a) if a.dtype == np.float64 else iptr(a)
+
+
+def oracle_particles(m, sp, torbit_fac, tables, stream, use_libm):
+    """orc_initialize_particles on the model's force grid; tables = {type:
+    (FG_Disp_r, FG_DispZ, FG_DispPhi, FG_tilted_vR2_prime, FG_tilted_vz2_prime,
+    FG_Vstream)}.  Returns (status, {field: array}, low-dispersion counts [4, 4],
+    stream position after)."""
+    o = Oracle(m.params, use_libm=use_libm)
+    o.load_model(m, particles=False)
+    n = sum(m.params.NType[t] for t in (1, 2, 3))
+    out = _particle_arrays(n)
+    keep = {t: [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab] for t, tab in tables.items()}
+    rows = (C.POINTER(PD) * 4)()
+    inner = {}
+    for t in (1, 2, 3):
+        if t in keep:
+            inner[t] = (PD * 6)(*[dptr(a) for a in keep[t]])
+            rows[t] = C.cast(inner[t], C.POINTER(PD))
+    counts = np.zeros((4, 4), dtype=np.int32)
+    s = _stream(stream)
+    st = o.L.orc_initialize_particles(o.h, C.byref(sp), float(torbit_fac), rows, C.byref(s), 1 if use_libm else 0,
+                                      *[_ptr(out[k]) for k, _, _ in PARTICLE_FIELDS], iptr(counts))
+    return st, out, counts, int(s.position)
+
+
+def reference_particles(params, grid, sp, torbit_fac, tables, stream):
+    """GALIC's own initialize_particles (one rank) with the force grid
+    grid = (pot, dpotdr, dpotdz) and tables as for oracle_particles: returns
+    ({field: array}, stream position after).  Run it through run_reference()."""
+    import tempfile
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    pot, dpotdr, dpotdz = [np.ascontiguousarray(a, dtype=np.float64) for a in grid]
+    L.ref_set_force_grid(dptr(pot), dptr(dpotdr), dptr(dpotdz))
+    keep = []
+    for t, tab in tables.items():
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab]
+        keep.append(arrs)
+        L.ref_set_dispersion(t, dptr(arrs[0]), dptr(arrs[1]), dptr(arrs[2]), dptr(arrs[3]), dptr(arrs[4]))
+        L.ref_set_vstream(t, dptr(arrs[5]))
+    L.ref_rng_stream(*[int(x) for x in stream])
+    with tempfile.TemporaryDirectory() as d:
+        n = L.ref_initialize_particles(d.encode(), C.byref(sp), float(torbit_fac))
+    out = _particle_arrays(n)
+    L.ref_get_init_particles(*[_ptr(out[k]) for k, _, _ in PARTICLE_FIELDS])
+    return out, int(L.ref_rng_position())
+
+
 def reference_peano_keys(xyz, bits):
     L = _ref_lib()
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
@@ -385,6 +446,8 @@ def _ref_lib():
         "ref_fresh_positions": (None, [C.c_int, C.c_longlong, PD]),
         "ref_calculate_dispfield": (C.c_int, [C.c_char_p, PSP, PJP]),
         "ref_get_jeans": (None, [C.c_int, PD]),
+        "ref_initialize_particles": (C.c_int, [C.c_char_p, PSP, C.c_double]),
+        "ref_get_init_particles": (None, [PD, PD, PD, PD, PD, PD, PD, PI, PI, PI]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

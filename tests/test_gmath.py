@@ -1,6 +1,6 @@
 """The project's elementary functions (galic_b200/csrc/gmath.h) against glibc.
 
-gmath.h replaces log/atan2/sin/cos/acos/exp on the orbit and sampling paths so that the CUDA
+gmath.h replaces log/atan2/sin/cos/acos/asin/exp on the orbit, sampling and set-up paths so that the CUDA
 kernels and the CPU restatement agree bit for bit; these tests bound its
 error against glibc over the argument ranges the path uses."""
 import ctypes as C
@@ -21,6 +21,7 @@ double t_sin(double x) { return gm_sin(x); }
 double t_cos(double x) { return gm_cos(x); }
 double t_acos(double x) { return gm_acos(x); }
 double t_exp(double x) { return gm_exp(x); }
+double t_asin(double x) { return gm_asin(x); }
 '''
 
 
@@ -33,7 +34,7 @@ def gm(tmp_path_factory):
     subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I",
                     os.path.join(ROOT, "galic_b200", "csrc"), str(src), "-o", str(so)], check=True)
     L = C.CDLL(str(so))
-    for n, k in (("t_log", 1), ("t_atan2", 2), ("t_sin", 1), ("t_cos", 1), ("t_acos", 1), ("t_exp", 1)):
+    for n, k in (("t_log", 1), ("t_atan2", 2), ("t_sin", 1), ("t_cos", 1), ("t_acos", 1), ("t_exp", 1), ("t_asin", 1)):
         f = getattr(L, n)
         f.restype = C.c_double
         f.argtypes = [C.c_double] * k
@@ -89,3 +90,10 @@ def test_exp_within_one_ulp(gm):
     assert gm.t_exp(0.0) == 1.0
     assert gm.t_exp(-800.0) == 0.0 and math.isinf(gm.t_exp(800.0)) and math.isinf(gm.t_exp(709.9))
     assert math.isnan(gm.t_exp(math.nan))
+
+
+def test_asin_within_two_ulp(gm):
+    rng = np.random.default_rng(6)
+    xs = np.concatenate([rng.uniform(-1, 1, 20000), rng.uniform(-1e-3, 1e-3, 2000), [1.0, -1.0, 0.0, -0.0, 1 - 2 ** -52]])
+    assert max(ulps(gm.t_asin(x), math.asin(x)) for x in xs) <= 2.0
+    assert math.isnan(gm.t_asin(1.5))
