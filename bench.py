@@ -305,6 +305,61 @@ def measure_jeans(model, steps, cpu):
     return res
 
 
+TORBIT_FAC = 5.0  # TorbitFac of the synthetic workload (integration time in orbital periods)
+
+
+def _ref_particles_timed(params, grid, sp, tables, nscale):
+    """GALIC's own initialize_particles (one rank) on the host for NType x
+    nscale particles, progress output to /dev/null; seconds per particle."""
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+
+    p = params.copy()
+    for t in (1, 2, 3):
+        p.NType[t] = max(int(p.NType[t] * nscale), 1 if p.NType[t] else 0)
+    t = time.perf_counter()
+    oracle_lib.reference_particles(p, grid, sp, TORBIT_FAC, tables, (42, 0, 0, 0))
+    return (time.perf_counter() - t) / sum(p.NType[t] for t in (1, 2, 3))
+
+
+def measure_particles(model, steps, cpu):
+    """initialize_particles through the C ABI for the workload's 1.2e6
+    particles (Jeans tables from galic_calculate_dispfield), every particle
+    array and the permutation copied out, in a context of its own."""
+    from galic_b200 import Context, jeans, particles, sampling
+
+    sp, jp = jeans_inputs(model)
+    with Context(model.params) as c:
+        c.load_model(model)
+        J = jeans.calculate_dispfield(c, sp, jp)
+        particles.initialize_particles(c, sp, TORBIT_FAC, sampling.Stream(42))
+        walls = []
+        for _ in range(max(steps, 1)):
+            s = sampling.Stream(42)
+            t = time.perf_counter()
+            particles.initialize_particles(c, sp, TORBIT_FAC, s)
+            walls.append(time.perf_counter() - t)
+        launches = c.last_kernel_launches()
+    n = sum(int(model.params.NType[t]) for t in (1, 2, 3))
+    ms = statistics.mean(walls) * 1e3
+    res = {"particles": n, "draws": s.position, "ms_per_call_e2e": ms, "particles_per_s": n / (ms * 1e-3),
+           "gpu_launches": launches}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+
+        tables = {t: (J[t]["disp_r"], J[t]["dispz"], J[t]["dispphi"], J[t]["tilted_vR2_prime"],
+                      J[t]["tilted_vz2_prime"], J[t]["vstream"]) for t in J}
+        per = oracle_lib.run_reference(_ref_particles_timed, model.params, (model.pot, model.dpotdr, model.dpotdz),
+                                       sp, tables, 0.02)
+        res["cpu_baseline"] = {"particles_per_s": 1.0 / per, "cores": 1, "kind": "reference",
+                               "sample": "GALIC's own initialize_particles for 2 % of the particle counts, one rank",
+                               "ms_per_call_extrapolated": per * n * 1e3}
+        res["speedup_e2e_vs_cpu"] = per * n * 1e3 / ms
+    return res
+
+
 def measure_ensemble(count, steps):
     """Batched ensemble: `count` Hernquist halos of uneven N advanced per
     iteration by one persistent FP32 launch replayed from a CUDA graph, tile
@@ -657,6 +712,7 @@ def ours_arm(args, rank, world, local_rank):
                             peak if form == GALIC_FORM_FP64 else measured_fp64_peak(torch))
         target_sampling = measure_sampling(model, ctx, args.steps, world == 1 and args.cpu_seconds > 0)
         jeans_solve = measure_jeans(model, args.steps, world == 1 and args.cpu_seconds > 0)
+        init_particles = measure_particles(model, args.steps, world == 1 and args.cpu_seconds > 0)
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
         serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
@@ -692,6 +748,7 @@ def ours_arm(args, rank, world, local_rank):
                 "force_grid_fill": fill,
                 "target_sampling": target_sampling,
                 "jeans": jeans_solve,
+                "particle_init": init_particles,
                 "ensemble": ensemble,
                 "serving": serving,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,

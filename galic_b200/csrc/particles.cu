@@ -16,6 +16,8 @@
 //  * k_final: each particle is initialised once more from its start, this
 //    time keeping its values; then one uniform per particle after the last
 //    draw and a radix sort give the permutation.
+// The halo's velocity rejection loop has a long tail near the centre; its
+// draw pairs are tested 32 at a time by a whole warp (halo_velocity_warp).
 // Two sinks close the successor function: R (the segment's positions ran
 // out: the segment is enlarged and the type redone) and R + 1 (a rejection
 // loop hit its cap of 10^6 tries).  Built with --fmad=false and gmath.h's
@@ -98,53 +100,106 @@ __device__ bool fresh_seq(const Shape &S, int type, grng_t &g, double *pos)
   return false;
 }
 
+// The halo's velocity draw (halo.c:168-184 inside set_particles.c:92-99),
+// warp-cooperative.  For the particle of lane L (radius r, stream position w)
+// halo_generate_v tests draw pairs (w, w+1), (w+2, w+3), ... until the first
+// accepted one, and set_particles.c repeats that while the speed is not below
+// MaxVelInUnitsVesc Vesc.  Near the centre the acceptance is small and the
+// number of pairs has a long tail; here the 32 lanes test 32 consecutive
+// pairs of one particle at once and a ballot picks the first accepted pair,
+// which is the sequential loop's result.  Every lane of the warp calls it;
+// need: this lane has a draw to make.  Returns false when capped.
+__device__ bool halo_velocity_warp(const PInit &P, bool need, double r, double vesc, uint64_t &w, double &vr_out)
+{
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const DevModel &M = P.M;
+  bool ok = true;
+  unsigned pending = __ballot_sync(FULL, need);
+  while(pending) {
+    const int L = __ffs(pending) - 1;
+    const double rL = __shfl_sync(FULL, r, L), vescL = __shfl_sync(FULL, vesc, L);
+    uint64_t wpos = __shfl_sync(FULL, (unsigned long long) w, L);
+    double vr = 0;
+    bool capped = false;
+    long long tries = 0;  // pairs tested for this particle, over all of its draws
+    do {
+      const double pot = halo_pot_r(M, rL);
+      const double v_max = sqrt(-2 * pot);
+      const double f_max = v_max * v_max * halo_f(M, rL, 0);
+      for(long long base = 0;; base += 32) {
+        const uint64_t j = wpos + 2 * (uint64_t) (base + lane);
+        const double v_guess = grng_uniform_at(P.seed, P.sa, P.sb, j) * v_max;
+        const double x_aux = grng_uniform_at(P.seed, P.sa, P.sb, j + 1) * f_max;
+        const bool accept = !(x_aux > v_guess * v_guess * halo_f(M, rL, v_guess));
+        const unsigned mask = __ballot_sync(FULL, accept);
+        if(mask) {
+          const int first = __ffs(mask) - 1;
+          vr = __shfl_sync(FULL, v_guess, first);
+          wpos += 2 * (uint64_t) (base + first + 1);
+          break;
+        }
+        tries += 32;
+        if(tries >= LOOP_CAP) {
+          capped = true;
+          break;
+        }
+      }
+    } while(!capped && vr >= P.MaxVel * vescL);
+    if(lane == L) {
+      w = wpos;
+      vr_out = vr;
+      ok = !capped;
+    }
+    pending &= pending - 1;
+  }
+  return ok;
+}
+
 // one iteration of initialize_particles' loop (set_particles.c:64-237) from
-// stream position `start`; returns the draws it took (LEN_CAPPED when a
-// rejection loop hit its cap).  With o != nullptr the particle's values are
-// stored at index n.
-__device__ uint32_t init_one(const PInit &P, int type, uint64_t start, const POut *o, int n)
+// stream position `start`, called by all 32 lanes of a warp together
+// (active: the lane has a particle).  Returns the draws it took (LEN_CAPPED
+// when a rejection loop hit its cap).  With o != nullptr the particle's
+// values are stored at index n.
+__device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool active, const POut *o, int n)
 {
   grng_t g;
   grng_init(&g, P.seed, P.sa, P.sb);
   grng_seek(&g, start);
   const DevModel &M = P.M;
   const LogConsts L = make_log_consts(M);
-  double pos[3];
-  if(!fresh_seq(P.S, type, g, pos)) return LEN_CAPPED;
-  // forcegrid_get_escape_speed (grid.c:115-120), the acceleration, Tint
-  const double vesc = sqrt(-2.0 * forcegrid_pot(M, L, pos));
-  double acc[3];
-  const FgCoord fc = fg_coord(M, L, pos);
-  forcegrid_acc(M, fc, pos, acc);
-  const double a = sqrt(acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2]);
-  const double r = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
-  const double tint = P.TorbitFac * 2 * kPi * r / sqrt(r * a);
-  double vt[3] = {0, 0, 0};
-  if(type == 1) {
-    // halo_generate_v (halo.c:168-184) until below MaxVelInUnitsVesc Vesc
-    double vr = 0;
-    int outer = 0;
-    do {
-      if(++outer > LOOP_CAP) return LEN_CAPPED;
-      const double pot = halo_pot_r(M, r);
-      const double v_max = sqrt(-2 * pot);
-      const double f_max = v_max * v_max * halo_f(M, r, 0);
-      double v_guess = grng_uniform(&g) * v_max;
-      double x_aux = grng_uniform(&g) * f_max;
-      int it = 0;
-      while(x_aux > v_guess * v_guess * halo_f(M, r, v_guess)) {
-        if(++it > LOOP_CAP) return LEN_CAPPED;
-        v_guess = grng_uniform(&g) * v_max;
-        x_aux = grng_uniform(&g) * f_max;
-      }
-      vr = v_guess;
-    } while(vr >= P.MaxVel * vesc);
-    const double phi = grng_uniform(&g) * kPi * 2;
-    const double theta = gm_acos(grng_uniform(&g) * 2 - 1);
-    vt[0] = vr * gm_sin(theta) * gm_cos(phi);
-    vt[1] = vr * gm_sin(theta) * gm_sin(phi);
-    vt[2] = vr * gm_cos(theta);
+  double pos[3] = {0, 0, 0};
+  bool ok = active && fresh_seq(P.S, type, g, pos);
+  double vesc = 0, tint = 0, r = 0;
+  FgCoord fc{};
+  if(ok) {
+    // forcegrid_get_escape_speed (grid.c:115-120), the acceleration, Tint
+    vesc = sqrt(-2.0 * forcegrid_pot(M, L, pos));
+    double acc[3];
+    fc = fg_coord(M, L, pos);
+    forcegrid_acc(M, fc, pos, acc);
+    const double a = sqrt(acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2]);
+    r = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+    tint = P.TorbitFac * 2 * kPi * r / sqrt(r * a);
   }
+  double vt[3] = {0, 0, 0};
+  if(type == 1) {  // uniform over the launch: every lane takes this branch
+    uint64_t w = grng_position(&g);
+    double vr = 0;
+    const bool vok = halo_velocity_warp(P, ok, r, vesc, w, vr);
+    if(ok) {
+      ok = vok;
+      grng_seek(&g, w);
+    }
+    if(ok) {
+      const double phi = grng_uniform(&g) * kPi * 2;
+      const double theta = gm_acos(grng_uniform(&g) * 2 - 1);
+      vt[0] = vr * gm_sin(theta) * gm_cos(phi);
+      vt[1] = vr * gm_sin(theta) * gm_sin(phi);
+      vt[2] = vr * gm_cos(theta);
+    }
+  }
+  if(!ok) return LEN_CAPPED;
   const DispTab &D = P.D[type];
   double d[4];
   disp_rtp(D, pos, d);
@@ -216,15 +271,17 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, const POu
 
 // J_0 over positions [0, R) of the segment starting at `base`; R and R + 1 are
 // the overflow and capped sinks
+// (whole warps run init_one together: lanes past R only keep the others company)
 __global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, int type, uint64_t base, uint32_t R, uint32_t *next)
 {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = o < R;
+  const uint32_t len = init_one(P, type, base + (active ? o : 0), active, nullptr, 0);
   if(o >= R + 2) return;
-  if(o >= R) {
+  if(!active) {
     next[o] = o;
     return;
   }
-  const uint32_t len = init_one(P, type, base + o, nullptr, 0);
   const uint64_t e = (uint64_t) o + len;
   next[o] = (len == LEN_CAPPED) ? R + 1 : (e < R ? (uint32_t) e : R);
 }
@@ -250,8 +307,8 @@ __global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, int type, uint6
                                                   int count, int n0, POut o)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if(i >= count) return;
-  init_one(P, type, base + starts[i], &o, n0 + i);
+  const bool active = i < count;
+  init_one(P, type, base + (active ? starts[i] : 0), active, &o, n0 + (active ? i : 0));
 }
 
 // permutation[].rnd (set_particles.c:298-301): the bits of a uniform in [0, 1)
