@@ -215,6 +215,11 @@ SIGNATURES = [
      [VP, C.POINTER(GalicSampleParams), C.POINTER(GalicJeansParams), C.POINTER(GalicJeansTables)]),
     ("galic_initialize_particles", C.c_int,
      [VP, C.POINTER(GalicSampleParams), C.c_double, C.POINTER(GalicStream), C.POINTER(GalicParticlesOut)]),
+    ("galic_get_params", C.c_int, [VP, C.POINTER(GalicParams)]),
+    ("galic_write_snapshot", C.c_int, [C.c_char_p, C.c_int, C.c_int, PD, PD, PD, PD, PI, PI, PD]),
+    ("galic_write_forcefield", C.c_int, [C.c_char_p, C.POINTER(GalicParams), PD, PD, PD]),
+    ("galic_write_density_field", C.c_int, [C.c_char_p, C.POINTER(GalicParams), C.c_int, PD, PD, PD, PD]),
+    ("galic_output_density_field", C.c_int, [VP, C.c_char_p, C.c_int]),
     ("galic_sample_positions", C.c_int,
      [C.POINTER(GalicSampleParams), C.c_int, C.c_longlong, C.POINTER(GalicStream), PD]),
     ("galic_grid_geometry", C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, PD]),

@@ -259,6 +259,13 @@ extern "C" const char *galic_status_string(int status)
   return kStatusText[status];
 }
 
+extern "C" int galic_get_params(const galic_ctx *ctx, galic_params_t *out)
+{
+  if(!ctx || !out) return GALIC_ERR_INVALID_ARGUMENT;
+  *out = ctx->prm;
+  return GALIC_OK;
+}
+
 extern "C" int galic_last_status(const galic_ctx *ctx) { return ctx ? ctx->status : GALIC_ERR_INVALID_ARGUMENT; }
 
 extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)

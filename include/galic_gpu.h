@@ -94,6 +94,8 @@ typedef struct galic_ctx galic_ctx;
 int galic_ctx_create(const galic_params_t *prm, galic_ctx **out);
 void galic_ctx_destroy(galic_ctx *ctx);
 int galic_last_status(const galic_ctx *ctx);
+/* copy of the parameters the context was created with */
+int galic_get_params(const galic_ctx *ctx, galic_params_t *out);
 /* human-readable text of a status code */
 const char *galic_status_string(int status);
 
@@ -491,6 +493,39 @@ typedef struct {
  * 10^6 tries (where the reference would keep drawing). */
 int galic_initialize_particles(galic_ctx *ctx, const galic_sample_params_t *sp, double TorbitFac,
                                galic_stream_t *stream, galic_particles_out_t *out);
+
+/* ---------------------------------------------------------- output files */
+
+/* Replaces write_file (io.c:906-1243) as output_particles calls it with one
+ * rank and NumFilesPerSnapshot = 1 (io.c:460-540): a Gadget snapshot of
+ * SnapFormat 1 or 2, the header followed by the blocks POS, VEL, ID, MASS
+ * (types with mass_table[t] == 0; mass_table NULL: all zero, as GALIC never
+ * sets All.MassTable) and VELT in single precision, particles grouped by type
+ * in their order.  Host arrays as galic_particles_out_t holds them.  The
+ * reference names the file OutputDir + OutputFile + "_%03d" (io.c:513). */
+int galic_write_snapshot(const char *fname, int snap_format, int n, const double *pos, const double *vel,
+                         const double *vel_theo, const double *mass, const int *id, const int *type,
+                         const double *mass_table);
+/* forcefield.dat (grid.c:789-823): FG_Nbin, FG_DPotDR, FG_DPotDz, FG_Pot, the
+ * analytic halo's potential derivatives and potential at the grid points
+ * (grid.c:766-786), and the points' R and z. */
+int galic_write_forcefield(const char *fname, const galic_params_t *prm, const double *dpotdr, const double *dpotdz,
+                           const double *pot);
+/* densfield_<type>_<num>.dat of one type (io.c:36-460, without the optional
+ * gnuplot output): the DG target stack level by level, the variable-
+ * resolution (calc_smoothed_stack, grid.c:1217-1243) target and response,
+ * the fine response, the DG and EG cell centres, and the variable-resolution
+ * target and response of the energy-grid mass, r, t, p, q.  dgs_target: the
+ * DG target stack; egs_targets: 5 EG target stacks (mass, r, t, p, q);
+ * dg_mass_loc: the committed time-averaged DG mass grid; eg_loc: 5 committed
+ * instantaneous EG grids (mass, r, t, p, q), which become the response stacks
+ * as calc_global_fit builds them (main.c:259-289). */
+int galic_write_density_field(const char *fname, const galic_params_t *prm, int type, const double *dgs_target,
+                              const double *egs_targets, const double *dg_mass_loc, const double *eg_loc);
+/* Replaces output_density_field (io.c:36-460) for dump number num: writes
+ * outdir/densfield_<type>_<num>.dat for every type with particles from the
+ * context's targets and committed grids. */
+int galic_output_density_field(galic_ctx *ctx, const char *outdir, int num);
 
 /* ---------------------------------------------------------- host helpers */
 

@@ -517,3 +517,27 @@ void ref_get_init_particles(double *pos, double *vel, double *vel_theo, double *
     perm[n] = permutation[n].index;
   }
 }
+
+/* ------------------------------------------------------- output files */
+
+/* output_particles (io.c:460-540) for dump 0 with one file of SnapFormat fmt:
+ * writes prefix + "snap_000" (OutputDir is used as a prefix, io.c:513) */
+void ref_output_particles(const char *prefix, int fmt)
+{
+  All.SnapFormat = fmt;
+  All.NumFilesPerSnapshot = 1;
+  All.NumFilesWrittenInParallel = 1;
+  All.StepsBetweenDump = 1;
+  All.BufferSize = 100;
+  strcpy(All.OutputDir, prefix);
+  strcpy(All.OutputFile, "snap");
+  output_particles(0);
+}
+
+/* output_density_field (io.c:36-460) for dump 0: outdir/densfield_<type>_000.dat */
+void ref_output_density_field(const char *outdir)
+{
+  All.StepsBetweenDump = 1;
+  strcpy(All.OutputDir, outdir);
+  output_density_field(0);
+}

@@ -403,6 +403,76 @@ def reference_particles(params, grid, sp, torbit_fac, tables, stream):
     return out, int(L.ref_rng_position())
 
 
+# ------------------------------------------------------------ output files
+
+def reference_snapshot(params, grid, sp, torbit_fac, tables, stream, fmt):
+    """GALIC's own initialize_particles, then output_particles with SnapFormat
+    fmt: ({field: array} of the particles, the snapshot file's bytes).  Run it
+    through run_reference()."""
+    import tempfile
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    pot, dpotdr, dpotdz = [np.ascontiguousarray(a, dtype=np.float64) for a in grid]
+    L.ref_set_force_grid(dptr(pot), dptr(dpotdr), dptr(dpotdz))
+    keep = []
+    for t, tab in tables.items():
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in tab]
+        keep.append(arrs)
+        L.ref_set_dispersion(t, dptr(arrs[0]), dptr(arrs[1]), dptr(arrs[2]), dptr(arrs[3]), dptr(arrs[4]))
+        L.ref_set_vstream(t, dptr(arrs[5]))
+    L.ref_rng_stream(*[int(x) for x in stream])
+    with tempfile.TemporaryDirectory() as d:
+        n = L.ref_initialize_particles(d.encode(), C.byref(sp), float(torbit_fac))
+        out = _particle_arrays(n)
+        L.ref_get_init_particles(*[_ptr(out[k]) for k, _, _ in PARTICLE_FIELDS])
+        L.ref_output_particles((d + "/").encode(), int(fmt))
+        with open(os.path.join(d, "snap_000"), "rb") as f:
+            data = f.read()
+    return out, data
+
+
+def reference_density_field(m):
+    """GALIC's own calc_all_response_fields on the model, then
+    output_density_field: {type: (file bytes, six target stacks, the committed
+    grids MASS_S, MASS_I, R_I, T_I, P_I, Q_I)}.  Run it through run_reference()."""
+    import tempfile
+    r = Reference(m.params)
+    r.load_model(m)
+    r.calc_all()
+    res = {}
+    with tempfile.TemporaryDirectory() as d:
+        r.L.ref_output_density_field(d.encode())
+        for t in (1, 2, 3):
+            if m.params.NType[t] == 0:
+                continue
+            with open(os.path.join(d, f"densfield_{t}_000.dat"), "rb") as f:
+                data = f.read()
+            st = [np.zeros(r.nstack) for _ in range(6)]
+            r.L.ref_get_targets(t, *[dptr(a) for a in st])
+            locs = [r.response(t, w) for w in (_ffi.GRID_MASS_S, _ffi.GRID_MASS_I, _ffi.GRID_R_I, _ffi.GRID_T_I,
+                                               _ffi.GRID_P_I, _ffi.GRID_Q_I)]
+            res[t] = (data, st, locs)
+    return res
+
+
+def reference_forcefield(params, rf):
+    """GALIC's own forcedensitygrid_calculate (one rank): (FG_DPotDR, FG_DPotDz,
+    FG_Pot, the bytes of the forcefield.dat it writes).  Run it through
+    run_reference()."""
+    import tempfile
+    L = _ref_lib()
+    L.ref_setup(C.byref(params))
+    N = params.FG_Nbin
+    out = [np.zeros((N, N)) for _ in range(3)]
+    with tempfile.TemporaryDirectory() as d:
+        st = L.ref_force_fill(d.encode(), C.byref(rf), *[dptr(a) for a in out])
+        if st != 0:
+            raise RuntimeError(f"ref_force_fill status {st}")
+        with open(os.path.join(d, "forcefield.dat"), "rb") as f:
+            data = f.read()
+    return out[0], out[1], out[2], data
+
+
 def reference_peano_keys(xyz, bits):
     L = _ref_lib()
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
@@ -447,6 +517,8 @@ def _ref_lib():
         "ref_calculate_dispfield": (C.c_int, [C.c_char_p, PSP, PJP]),
         "ref_get_jeans": (None, [C.c_int, PD]),
         "ref_initialize_particles": (C.c_int, [C.c_char_p, PSP, C.c_double]),
+        "ref_output_particles": (None, [C.c_char_p, C.c_int]),
+        "ref_output_density_field": (None, [C.c_char_p]),
         "ref_get_init_particles": (None, [PD, PD, PD, PD, PD, PD, PD, PI, PI, PI]),
     }
     for name, (res, args) in sig.items():
