@@ -3,6 +3,7 @@
 // functions.  Host code only; the kernels live in orbit_fp64.cu and
 // fit_fp64.cu.
 #include <cuda_runtime.h>
+#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -512,6 +513,126 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
   CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
   return fail(ctx, GALIC_OK);
 }
+
+namespace {
+
+// masses and types of particles stored type by type
+__global__ void k_particle_meta(int n, int n1, int n12, double m1, double m2, double m3, double *mass, int *type)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const int t = i < n1 ? 1 : (i < n12 ? 2 : 3);
+  type[i] = t;
+  mass[i] = t == 1 ? m1 : (t == 2 ? m2 : m3);
+}
+
+// r^2 as it orders (non-negative doubles order like their bits)
+__global__ void k_radius_keys(int n, const double *pos, unsigned long long *key, int *idx)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const double *p = pos + 3 * (size_t) i;
+  const double r2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+  key[i] = (unsigned long long) __double_as_longlong(r2);
+  idx[i] = i;
+}
+
+__global__ void k_type_keys(int n, int n1, int n12, const int *idx, int *key)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const int j = idx[i];
+  key[i] = j < n1 ? 1 : (j < n12 ? 2 : 3);
+}
+
+// the orbit order of galic_set_particles (by type, then by radius, ties in
+// index order) for particles stored type by type: a stable radix sort by
+// r^2, then a stable one by type
+cudaError_t order_by_type_radius(galic_ctx *ctx, const int nt[4])
+{
+  const int n = ctx->n;
+  cudaStream_t s = ctx->stream;
+  const unsigned g = (unsigned) ((n + 255) / 256);
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  int *i0 = nullptr, *i1 = nullptr, *t0 = nullptr, *t1 = nullptr;
+  void *tmp = nullptr;
+  size_t tb = 0, tb2 = 0, tbx;
+  cudaError_t e = cudaMallocAsync((void **) &k0, 2 * (size_t) n * sizeof(unsigned long long), s);
+  if(e == cudaSuccess) e = cudaMallocAsync((void **) &i0, 4 * (size_t) n * sizeof(int), s);
+  if(e == cudaSuccess) {
+    k1 = k0 + n;
+    i1 = i0 + n;
+    t0 = i1 + n;
+    t1 = t0 + n;
+    e = cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, i0, i1, n, 0, 64, s);
+  }
+  if(e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb2, t0, t1, i1, ctx->d_order, n, 0, 2, s);
+  if(e == cudaSuccess) e = cudaMallocAsync(&tmp, std::max<size_t>(std::max(tb, tb2), 16), s);
+  if(e == cudaSuccess) {
+    k_radius_keys<<<g, 256, 0, s>>>(n, ctx->d_pos, k0, i0);
+    tbx = std::max(tb, tb2);
+    e = cub::DeviceRadixSort::SortPairs(tmp, tbx, k0, k1, i0, i1, n, 0, 64, s);
+  }
+  if(e == cudaSuccess) {
+    k_type_keys<<<g, 256, 0, s>>>(n, nt[1], nt[1] + nt[2], i1, t0);
+    tbx = std::max(tb, tb2);
+    e = cub::DeviceRadixSort::SortPairs(tmp, tbx, t0, t1, i1, ctx->d_order, n, 0, 2, s);
+  }
+  if(e == cudaSuccess) e = cudaGetLastError();
+  for(void *q : {(void *) k0, (void *) i0, tmp})
+    if(q) cudaFreeAsync(q, s);
+  return e;
+}
+
+}  // namespace
+
+namespace galic_internal {
+
+// installs particles whose arrays are on the device, stored type by type
+// (nt[t] particles of type t, masses tmass[t] / nt[t]), as galic_set_particles
+// does from the host
+int set_particles_device(galic_ctx *ctx, const int nt[4], const double tmass[4], const double *pos,
+                         const double *vel, const double *tint, const double *vesc, const double *targets)
+{
+  const int n = nt[1] + nt[2] + nt[3];
+  if(n <= 0) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  cudaStream_t s = ctx->stream;
+  ctx->generation++;
+  if(n != ctx->n) {
+    dfree(ctx, ctx->d_pos); dfree(ctx, ctx->d_vel); dfree(ctx, ctx->d_mass); dfree(ctx, ctx->d_tint); dfree(ctx, ctx->d_vesc);
+    dfree(ctx, ctx->d_ptargets); dfree(ctx, ctx->d_vdisp); dfree(ctx, ctx->d_type); dfree(ctx, ctx->d_orbits); dfree(ctx, ctx->d_order);
+    ctx->n = 0;
+    CK(dalloc(ctx, &ctx->d_order, n));
+    CK(dalloc(ctx, &ctx->d_pos, 3 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_vel, 3 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_mass, n));
+    CK(dalloc(ctx, &ctx->d_tint, n));
+    CK(dalloc(ctx, &ctx->d_vesc, n));
+    CK(dalloc(ctx, &ctx->d_ptargets, 4 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_vdisp, 4 * (size_t) n));
+    CK(dalloc(ctx, &ctx->d_type, n));
+    CK(dalloc(ctx, &ctx->d_orbits, n));
+    ctx->n = n;
+  }
+  const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(ctx->d_pos, pos, 3 * (size_t) n * sizeof(double), dd, s));
+  CK(cudaMemcpyAsync(ctx->d_vel, vel, 3 * (size_t) n * sizeof(double), dd, s));
+  CK(cudaMemcpyAsync(ctx->d_tint, tint, n * sizeof(double), dd, s));
+  CK(cudaMemcpyAsync(ctx->d_vesc, vesc, n * sizeof(double), dd, s));
+  CK(cudaMemcpyAsync(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), dd, s));
+  CK(cudaMemsetAsync(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double), s));
+  CK(cudaMemsetAsync(ctx->d_orbits, 0, n * sizeof(int), s));
+  k_particle_meta<<<(unsigned) ((n + 255) / 256), 256, 0, s>>>(n, nt[1], nt[1] + nt[2], nt[1] ? tmass[1] / nt[1] : 0.0,
+                                                                nt[2] ? tmass[2] / nt[2] : 0.0,
+                                                                nt[3] ? tmass[3] / nt[3] : 0.0, ctx->d_mass, ctx->d_type);
+  CK(cudaGetLastError());
+  CK(order_by_type_radius(ctx, nt));
+  ctx->have_response = false;
+  CK(cudaStreamSynchronize(s));
+  return fail(ctx, GALIC_OK);
+}
+
+}  // namespace galic_internal
 
 extern "C" int galic_get_particles(galic_ctx *ctx, double *vel, int *orbits, double *vdisp)
 {

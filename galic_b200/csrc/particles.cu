@@ -5,23 +5,28 @@
 // depends on its rejection loops (position inside Rmax, the Hernquist
 // velocity by von Neumann rejection, the Gaussian velocity below the escape
 // speed, Marsaglia's polar method).  The replay here finds every particle's
-// first draw in parallel:
-//  * k_len: for EVERY stream position o of a type's segment, the number of
-//    draws one particle initialisation takes when it starts at o
-//    (next[o] = o + len).  Any position starts a valid initialisation, so
-//    this is a fully parallel map, about 20 positions per particle;
-//  * k_lift: binary lifting of the successor function, J_k = J_(k-1) o J_(k-1)
-//    (J_0 = next); particle n starts at J applied n times to the segment
-//    start, read off the bits of n (k_starts);
+// first draw in parallel by speculative segment decoding:
+//  * k_len on the first 65536 positions of a type's draws gives the mean
+//    draws per particle, which sizes the segments (16 or 32 particles' worth
+//    of positions each, a multiple of 32);
+//  * k_seg_decode: one lane per segment initialises particles back to back
+//    from the segment's first position, marking each start in a bitmap;
+//  * k_seg_fix rounds: a segment whose entry (the largest exit before it) is
+//    not where its chain began re-decodes from the entry until it lands on a
+//    start it already has -- two chains that meet agree from there on, and
+//    they mostly meet within a few particles -- or leaves the segment, and
+//    then goes on into the next segments that no other lane walks this round;
+//  * k_seg_count, a scan and k_seg_extract turn the bitmap into the start of
+//    every particle;
 //  * k_final: each particle is initialised once more from its start, this
 //    time keeping its values; then one uniform per particle after the last
 //    draw and a radix sort give the permutation.
 // The halo's velocity rejection loop has a long tail near the centre; its
 // draw pairs are tested 32 at a time by a whole warp (halo_velocity_warp).
-// Two sinks close the successor function: R (the segment's positions ran
-// out: the segment is enlarged and the type redone) and R + 1 (a rejection
-// loop hit its cap of 10^6 tries).  Built with --fmad=false and gmath.h's
-// functions, so every particle is bit-identical to the CPU restatement.
+// A chain whose rejection loop hits its cap of 10^6 tries ends there; if
+// that happens before a type's last particle the call fails.  Built with
+// --fmad=false and gmath.h's functions, so every particle is bit-identical
+// to the CPU restatement.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -54,7 +59,7 @@ struct PInit {
 
 struct POut {
   double *pos, *vel, *vel_theo, *vesc, *tint, *targets;
-  int *counts;  // [4][4]
+  int *counts;  // [4][4] raised to LowerDispLimit, then [16] non-positive Tint
 };
 
 // halo_get_potential_from_radius (halo.c:69-73)
@@ -261,6 +266,7 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool acti
     }
     o->vesc[n] = vesc;
     o->tint[n] = tint;
+    if(!(tint > 0)) atomicAdd(&o->counts[16], 1);
     for(int k = 0; k < 4; k++) {
       o->targets[4 * n + k] = d[k];
       if(low[k]) atomicAdd(&o->counts[4 * type + k], 1);
@@ -269,9 +275,9 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool acti
   return len >= LEN_CAPPED ? LEN_CAPPED : (uint32_t) len;
 }
 
-// J_0 over positions [0, R) of the segment starting at `base`; R and R + 1 are
-// the overflow and capped sinks
-// (whole warps run init_one together: lanes past R only keep the others company)
+// the successor of every position o in [0, R) from `base`: next[o] = o + the
+// draws of a particle started at o, R when that is past R, R + 1 when a
+// rejection loop capped (whole warps run init_one together: lanes past R only keep the others company)
 __global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, int type, uint64_t base, uint32_t R, uint32_t *next)
 {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -286,24 +292,188 @@ __global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, int type, uint64_
   next[o] = (len == LEN_CAPPED) ? R + 1 : (e < R ? (uint32_t) e : R);
 }
 
-__global__ void k_lift(const uint32_t *J, uint32_t *J2, uint32_t n)
+// Segment decode.  The type's stream positions are cut into K segments of
+// Lseg positions (Lseg a multiple of 32, a few particles' worth); bit q of
+// the bitmap says that position q starts a particle of the chain recorded
+// for q's segment.  Each segment's chain starts at its entry x[c] and leaves
+// the segment at its exit cx[c] (the first start at or past the segment's
+// end; POS_CAPPED when a rejection loop hit its cap).  One lane owns each
+// segment and the segment's bitmap words.
+constexpr uint64_t POS_CAPPED = ~0ull;
+
+struct Segs {
+  uint64_t Lseg;
+  uint32_t K, W;   // segments; bitmap words per segment (Lseg / 32)
+  uint32_t *bits;  // K * W
+  uint64_t *x, *cx;
+};
+
+// clears positions [lo, hi) of the segment that starts at a (a multiple of 32)
+__device__ void clear_bits(uint32_t *w, uint64_t a, uint64_t lo, uint64_t hi)
 {
-  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
-  if(o < n) J2[o] = J[J[o]];
+  for(uint64_t q = lo; q < hi;) {
+    const uint32_t k = (uint32_t) ((q - a) >> 5), b = (uint32_t) (q & 31);
+    const uint64_t wend = a + ((uint64_t) k + 1) * 32;
+    const uint32_t nb = (uint32_t) ((hi < wend ? hi : wend) - q);  // 1 .. 32 - b
+    w[k] &= ~(nb == 32 ? 0xffffffffu : ((1u << nb) - 1) << b);
+    q += nb;
+  }
 }
 
-// start of particle i of the segment (i <= count; i = count is the end)
-__global__ void k_starts(const uint32_t *J, size_t stride, int levels, int count, uint32_t *starts)
+__device__ __forceinline__ bool bit_at(const uint32_t *w, uint64_t a, uint64_t q)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if(i > count) return;
-  uint32_t o = 0;
-  for(int k = 0; k < levels; k++)
-    if((i >> k) & 1) o = J[(size_t) k * stride + o];
-  starts[i] = o;
+  return (w[(q - a) >> 5] >> (q & 31)) & 1u;
 }
 
-__global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, int type, uint64_t base, const uint32_t *starts,
+// every segment decoded from its own first position (whole warps run
+// init_one together: lanes past K only keep the others company)
+__global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, int type, uint64_t base, const Segs S,
+                                                       uint64_t *exit)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = c < S.K;
+  const uint64_t a = (uint64_t) c * S.Lseg, end = a + S.Lseg;
+  uint32_t *w = S.bits + (size_t) (valid ? c : 0) * S.W;
+  uint64_t q = a;
+  bool work = valid;
+  while(__any_sync(0xffffffffu, work)) {
+    const uint32_t len = init_one(P, type, base + (work ? q : 0), work, nullptr, 0);
+    if(work) {
+      w[(q - a) >> 5] |= 1u << (q & 31);
+      if(len == LEN_CAPPED || len == 0) {
+        q = POS_CAPPED;
+        work = false;
+      } else {
+        q += len;
+        work = q < end;
+      }
+    }
+  }
+  if(valid) {
+    S.x[c] = a;
+    S.cx[c] = q;
+    exit[c] = q;
+  }
+}
+
+struct MaxU64 {
+  __device__ __forceinline__ uint64_t operator()(uint64_t u, uint64_t v) const { return u > v ? u : v; }
+};
+
+// before a resynchronisation round: a segment's entry is the largest exit
+// before it (exits never decrease along the true chain, and one long particle
+// can span many segments); flag[c]: the entry differs from the one the
+// segment's chain was decoded from, so the segment is walked this round
+__global__ void k_seg_prep(const Segs S, const uint64_t *pmax, const uint64_t *exit_in, uint64_t *exit_out,
+                           uint8_t *flag)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if(c >= S.K) return;
+  const uint64_t e = c ? pmax[c - 1] : 0;
+  flag[c] = e != POS_CAPPED && e != S.x[c];
+  exit_out[c] = exit_in[c];
+}
+
+// one resynchronisation round: each flagged segment re-decodes from its
+// entry until it lands on a start of its recorded chain (the chains agree
+// from there on) or leaves the segment; positions it steps over lose their
+// bits.  A walk that leaves with a new exit goes on into the next segment
+// when that one is not flagged (so no two lanes touch one segment), as the
+// next round would.  After round r segments 0 .. r are exact; the rounds end
+// when no exit changes.
+__global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, int type, uint64_t base, const Segs S,
+                                                    const uint64_t *pmax, const uint8_t *flag,
+                                                    const uint64_t *exit_in, uint64_t *exit_out, int *changed)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  bool work = c < S.K && flag[c];
+  uint32_t d = c;
+  uint64_t a = (uint64_t) d * S.Lseg, end = a + S.Lseg;
+  uint32_t *w = S.bits + (size_t) (work ? d : 0) * S.W;
+  uint64_t q = work ? pmax[c - 1] : 0;  // flag[0] is never set
+  if(work) {
+    S.x[d] = q;
+    clear_bits(w, a, a, q < end ? q : end);
+  }
+  while(__any_sync(0xffffffffu, work)) {
+    bool step = false;
+    if(work) {
+      const bool left = q >= end;
+      if(left || bit_at(w, a, q)) {  // left the segment, or joined the recorded chain
+        const uint64_t out = left ? q : S.cx[d];
+        S.cx[d] = out;
+        exit_out[d] = out;
+        work = false;
+        if(out != exit_in[d]) {
+          *changed = 1;
+          if(d + 1 < S.K && !flag[d + 1]) {  // go on into the next segment
+            d++;
+            a = end;
+            end = a + S.Lseg;
+            w = S.bits + (size_t) d * S.W;
+            S.x[d] = q;
+            clear_bits(w, a, a, q < end ? q : end);
+            work = true;
+          }
+        }
+      } else {
+        step = true;
+      }
+    }
+    const uint32_t len = init_one(P, type, base + (step ? q : 0), step, nullptr, 0);
+    if(step) {
+      w[(q - a) >> 5] |= 1u << (q & 31);
+      if(len == LEN_CAPPED || len == 0) {
+        clear_bits(w, a, q + 1, end);
+        S.cx[d] = POS_CAPPED;
+        exit_out[d] = POS_CAPPED;
+        if(exit_in[d] != POS_CAPPED) *changed = 1;
+        work = false;
+      } else {
+        const uint64_t n = q + len;
+        clear_bits(w, a, q + 1, n < end ? n : end);
+        q = n;
+      }
+    }
+  }
+}
+
+// the first segment whose chain caps (every later one is cut off)
+__global__ void k_seg_first_cap(const uint64_t *exit, uint32_t K, unsigned *first)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if(c < K && exit[c] == POS_CAPPED) atomicMin(first, c);
+}
+
+// starts per segment up to the first capped one; cnt[K] = 0 closes the scan
+__global__ void k_seg_count(const Segs S, const unsigned *first, uint64_t *cnt)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if(c > S.K) return;
+  uint64_t n = 0;
+  if(c < S.K && c <= *first) {
+    const uint32_t *w = S.bits + (size_t) c * S.W;
+    for(uint32_t k = 0; k < S.W; k++) n += __popc(w[k]);
+  }
+  cnt[c] = n;
+}
+
+// start of particle i (i <= count; i = count is where the type's draws end)
+__global__ void k_seg_extract(const Segs S, const unsigned *first, const uint64_t *off, int count,
+                              uint64_t *starts)
+{
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if(c >= S.K || c > *first) return;
+  uint64_t r = off[c];
+  if(r > (uint64_t) count) return;
+  const uint32_t *w = S.bits + (size_t) c * S.W;
+  const uint64_t a = (uint64_t) c * S.Lseg;
+  for(uint32_t k = 0; k < S.W && r <= (uint64_t) count; k++)
+    for(uint32_t m = w[k]; m && r <= (uint64_t) count; m &= m - 1)
+      starts[r++] = a + 32ull * k + (uint64_t) (__ffs(m) - 1);
+}
+
+__global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, int type, uint64_t base, const uint64_t *starts,
                                                   int count, int n0, POut o)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -350,6 +520,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
   if(!sp || !stream) return pfail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   const galic_params_t &p = ctx->prm;
   const int nt[4] = {0, p.NType[1], p.NType[2], p.NType[3]};
+  const double tmass[4] = {0, p.Halo_Mass, p.Disk_Mass, p.Bulge_Mass};
   const long long Nll = (long long) nt[1] + nt[2] + nt[3];
   if(nt[1] < 0 || nt[2] < 0 || nt[3] < 0 || Nll < 1 || Nll > (1ll << 28)) return pfail(ctx, GALIC_ERR_INVALID_ARGUMENT);
   const int N = (int) Nll;
@@ -362,12 +533,13 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
   int rc = GALIC_OK, launches = 0;
   double *d_f = nullptr;  // pos, vel, vel_theo (3N each), vesc, tint (N each), targets (4N)
   int *d_counts = nullptr, *d_vals = nullptr, *d_vals2 = nullptr;
-  uint32_t *d_J = nullptr, *d_starts = nullptr;
+  uint32_t *d_J = nullptr;
+  uint64_t *d_starts = nullptr;  // inside d_seg
+  char *d_seg = nullptr;
   unsigned long long *d_keys = nullptr, *d_keys2 = nullptr;
   void *d_tmp = nullptr;
-  size_t J_cap = 0;
-  std::vector<double> h_f;
-  std::vector<int> h_counts(16), h_perm;
+  size_t J_cap = 0, seg_cap = 0;
+  std::vector<int> h_counts(17);
   uint64_t pos = stream->position;
   PInit P{};
   POut O{};
@@ -401,9 +573,9 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     D.FG_Nbin = p.FG_Nbin;
   }
   PCK(cudaMallocAsync((void **) &d_f, (size_t) 15 * N * sizeof(double), s));
-  PCK(cudaMallocAsync((void **) &d_counts, 16 * sizeof(int), s));
+  PCK(cudaMallocAsync((void **) &d_counts, 17 * sizeof(int), s));
   PCK(cudaMemsetAsync(d_f, 0, (size_t) 15 * N * sizeof(double), s));
-  PCK(cudaMemsetAsync(d_counts, 0, 16 * sizeof(int), s));
+  PCK(cudaMemsetAsync(d_counts, 0, 17 * sizeof(int), s));
   O.pos = d_f;
   O.vel = d_f + 3 * (size_t) N;
   O.vel_theo = d_f + 6 * (size_t) N;
@@ -439,42 +611,109 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         rc = GALIC_ERR_REJECTION_CAP;
         break;
       }
-      double per = sum / valid;
+      const double per = sum / valid;
+      // particles per segment: enough segments to fill the GPU with lanes,
+      // few enough rounds (two chains usually meet within a few particles,
+      // but the spread of the halo's lengths gives a long tail)
+      const int seg_particles = (t == 2) ? 32 : 16;
+      const uint64_t Lseg = ((uint64_t) (per * seg_particles) + 31) / 32 * 32;
       for(int attempt = 0;; attempt++) {
-        const double want = (double) nt[t] * per * (1.15 + 0.5 * attempt) + 4096;
-        if(want > 4.0e9) {
+        const double want = ((double) nt[t] + 1) * per * (1.05 + 0.25 * attempt);
+        const double Kd = want / (double) Lseg + 2;
+        if(Kd > 2.0e9 || Kd * (double) Lseg / 8 > (double) (8ull << 30)) {  // the bitmap's budget
           rc = GALIC_ERR_UNSUPPORTED;
           break;
         }
-        R = (uint32_t) want;
-        int levels = 1;
-        while((1ll << levels) <= nt[t]) levels++;
-        const size_t stride = (size_t) R + 2;
-        if(stride * levels * sizeof(uint32_t) > (32ull << 30)) {  // the lifting tables' budget
-          rc = GALIC_ERR_UNSUPPORTED;
-          break;
+        Segs G{};
+        G.Lseg = Lseg;
+        G.K = (uint32_t) Kd;
+        G.W = (uint32_t) (Lseg / 32);
+        const size_t K = G.K;
+        size_t tb = 0, tb2 = 0;
+        PCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (uint64_t *) nullptr, (uint64_t *) nullptr, K + 1, s));
+        PCK(cub::DeviceScan::InclusiveScan(nullptr, tb2, (uint64_t *) nullptr, (uint64_t *) nullptr, MaxU64(), K, s));
+        tb = std::max(tb, tb2);
+        const auto al = [](size_t n) { return (n + 255) / 256 * 256; };
+        const size_t sz_bits = al(K * G.W * sizeof(uint32_t)), sz_k = al(K * sizeof(uint64_t)),
+                     sz_k1 = al((K + 1) * sizeof(uint64_t)), sz_st = al(((size_t) nt[t] + 1) * sizeof(uint64_t));
+        const size_t need = sz_bits + 5 * sz_k + al(K) + 2 * sz_k1 + 256 + al(tb) + sz_st;
+        if(seg_cap < need) {
+          if(d_seg) cudaFreeAsync(d_seg, s);
+          d_seg = nullptr;
+          seg_cap = need;
+          PCK(cudaMallocAsync((void **) &d_seg, seg_cap, s));
         }
-        if(J_cap < stride * levels) {
-          cudaFreeAsync(d_J, s);
-          J_cap = stride * levels;
-          PCK(cudaMallocAsync((void **) &d_J, J_cap * sizeof(uint32_t), s));
-        }
-        k_len<<<gblocks(stride, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, R, d_J);
-        for(int k = 1; k < levels; k++)
-          k_lift<<<gblocks(stride, 256), 256, 0, s>>>(d_J + (k - 1) * stride, d_J + k * stride, (uint32_t) stride);
-        if(d_starts) cudaFreeAsync(d_starts, s);
-        PCK(cudaMallocAsync((void **) &d_starts, ((size_t) nt[t] + 1) * sizeof(uint32_t), s));
-        k_starts<<<gblocks((long long) nt[t] + 1, 256), 256, 0, s>>>(d_J, stride, levels, nt[t], d_starts);
-        launches += levels + 1;
+        char *cur = d_seg;
+        G.bits = (uint32_t *) cur, cur += sz_bits;
+        G.x = (uint64_t *) cur, cur += sz_k;
+        G.cx = (uint64_t *) cur, cur += sz_k;
+        uint64_t *ex[2] = {(uint64_t *) cur, (uint64_t *) (cur + sz_k)};
+        cur += 2 * sz_k;
+        uint64_t *d_pmax = (uint64_t *) cur;
+        cur += sz_k;
+        uint8_t *d_flag = (uint8_t *) cur;
+        cur += al(K);
+        uint64_t *d_cnt = (uint64_t *) cur, *d_off = (uint64_t *) (cur + sz_k1);
+        cur += 2 * sz_k1;
+        unsigned *d_first = (unsigned *) cur;
+        int *d_changed = (int *) (cur + 128);
+        cur += 256;
+        void *d_scan = cur;
+        cur += al(tb);
+        d_starts = (uint64_t *) cur;
+        PCK(cudaMemsetAsync(G.bits, 0, sz_bits, s));
+        k_seg_decode<<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, G, ex[0]);
+        launches++;
         PCK(cudaGetLastError());
-        uint32_t end = 0;
-        PCK(cudaMemcpyAsync(&end, d_starts + nt[t], sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        PCK(cudaStreamSynchronize(s));
-        if(end == R + 1) {
-          rc = GALIC_ERR_REJECTION_CAP;
+        int fin = -1;
+        for(size_t r = 1; r <= K + 1; r++) {  // segment r - 1 is exact after round r - 1
+          int h_changed = 0;
+          const uint64_t *in = ex[(r - 1) & 1];
+          uint64_t *out_ = ex[r & 1];
+          size_t tbr = tb;
+          PCK(cub::DeviceScan::InclusiveScan(d_scan, tbr, in, d_pmax, MaxU64(), K, s));
+          k_seg_prep<<<gblocks((long long) K, 256), 256, 0, s>>>(G, d_pmax, in, out_, d_flag);
+          PCK(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
+          k_seg_fix<<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, G, d_pmax, d_flag, in, out_,
+                                                                      d_changed);
+          launches += 3;
+          PCK(cudaGetLastError());
+          PCK(cudaMemcpyAsync(&h_changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, s));
+          PCK(cudaStreamSynchronize(s));
+          if(!h_changed) {
+            fin = (int) (r & 1);
+            break;
+          }
+        }
+        if(fin < 0) {  // cannot happen: round r fixes segment r for good
+          rc = GALIC_ERR_CUDA;
           break;
         }
-        if(end == R) continue;  // the segment was too short: enlarge it
+        PCK(cudaMemsetAsync(d_first, 0xff, sizeof(unsigned), s));
+        k_seg_first_cap<<<gblocks((long long) K, 256), 256, 0, s>>>(ex[fin], G.K, d_first);
+        k_seg_count<<<gblocks((long long) K + 1, 256), 256, 0, s>>>(G, d_first, d_cnt);
+        size_t tbe = tb;
+        PCK(cub::DeviceScan::ExclusiveSum(d_scan, tbe, d_cnt, d_off, K + 1, s));
+        launches += 3;
+        PCK(cudaGetLastError());
+        uint64_t total = 0;
+        unsigned first = 0;
+        PCK(cudaMemcpyAsync(&total, d_off + K, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        PCK(cudaMemcpyAsync(&first, d_first, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        PCK(cudaStreamSynchronize(s));
+        if(total < (uint64_t) nt[t] + 1) {
+          if(first < G.K) {  // the chain caps before its last particle ends
+            rc = GALIC_ERR_REJECTION_CAP;
+            break;
+          }
+          continue;  // the segments were too few: enlarge them
+        }
+        k_seg_extract<<<gblocks((long long) K, 256), 256, 0, s>>>(G, d_first, d_off, nt[t], d_starts);
+        launches++;
+        PCK(cudaGetLastError());
+        uint64_t end = 0;
+        PCK(cudaMemcpyAsync(&end, d_starts + nt[t], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        PCK(cudaStreamSynchronize(s));
         k_final<<<gblocks(nt[t], PBLOCK), PBLOCK, 0, s>>>(P, t, pos, d_starts, nt[t], n0, O);
         launches++;
         PCK(cudaGetLastError());
@@ -484,13 +723,12 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     }
   }
   if(rc != GALIC_OK) goto done;
-  h_f.resize((size_t) 15 * N);
-  PCK(cudaMemcpyAsync(h_f.data(), d_f, h_f.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  PCK(cudaMemcpyAsync(h_counts.data(), d_counts, 16 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  PCK(cudaMemcpyAsync(h_counts.data(), d_counts, 17 * sizeof(int), cudaMemcpyDeviceToHost, s));
   PCK(cudaStreamSynchronize(s));
   for(int t = 1; t <= 3; t++)
     for(int k = 0; k < 4; k++)
       if(nt[t] > 0 && (double) h_counts[4 * t + k] / nt[t] > 0.05) rc = GALIC_ERR_UNSUPPORTED;
+  if(rc == GALIC_OK && h_counts[16]) rc = GALIC_ERR_INVALID_ARGUMENT;  // galic_set_particles' tint check
   if(rc == GALIC_OK) {
     // the permutation (set_particles.c:298-303)
     size_t tb = 0;
@@ -503,50 +741,40 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     PCK(cudaMallocAsync(&d_tmp, std::max<size_t>(tb, 16), s));
     PCK(cub::DeviceRadixSort::SortPairs(d_tmp, tb, d_keys, d_keys2, d_vals, d_vals2, N, 0, 64, s));
     launches += 2;
-    h_perm.resize(N);
-    PCK(cudaMemcpyAsync(h_perm.data(), d_vals2, (size_t) N * sizeof(int), cudaMemcpyDeviceToHost, s));
-    PCK(cudaStreamSynchronize(s));
-    pos += (uint64_t) N;
+    if(out && out->permutation)
+      PCK(cudaMemcpyAsync(out->permutation, d_vals2, (size_t) N * sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
+  if(out && (rc == GALIC_OK || rc == GALIC_ERR_UNSUPPORTED)) {
+    // the particles straight into the caller's arrays; masses, types and IDs
+    // by type (set_particles.c:38-62)
+    double *dst[6] = {out->pos, out->vel, out->vel_theo, out->vesc, out->tint, out->targets};
+    const size_t off[6] = {0, 3, 6, 9, 10, 11}, len[6] = {3, 3, 3, 1, 1, 4};
+    for(int k = 0; k < 6; k++)
+      if(dst[k])
+        PCK(cudaMemcpyAsync(dst[k], d_f + off[k] * N, len[k] * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    for(int t = 1, n = 0; t <= 3; t++)
+      for(int i = 0; i < nt[t]; i++, n++) {
+        if(out->mass) out->mass[n] = tmass[t] / nt[t];
+        if(out->type) out->type[n] = t;
+        if(out->id) out->id[n] = n + 1;
+      }
+    for(int t = 0; t < 4; t++)
+      for(int k = 0; k < 4; k++) out->low_disp[t][k] = h_counts[4 * t + k];
+  }
+  PCK(cudaStreamSynchronize(s));
+  if(rc == GALIC_OK) {
+    // the particles become the context's
+    rc = galic_internal::set_particles_device(ctx, nt, tmass, d_f, d_f + 3 * (size_t) N, d_f + 10 * (size_t) N, d_f + 9 * (size_t) N,
+                              d_f + 11 * (size_t) N);
+    if(rc == GALIC_OK) pos += (uint64_t) N;
   }
 done:
-  for(void *q : {(void *) d_f, (void *) d_counts, (void *) d_vals, (void *) d_vals2, (void *) d_J, (void *) d_starts,
+  for(void *q : {(void *) d_f, (void *) d_counts, (void *) d_vals, (void *) d_vals2, (void *) d_J, (void *) d_seg,
                  (void *) d_keys, (void *) d_keys2, d_tmp})
     if(q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
   ctx->last_launches = launches;
-  if(rc != GALIC_OK && rc != GALIC_ERR_UNSUPPORTED) return pfail(ctx, rc);
-  // host arrays in P order
-  std::vector<double> mass(N), tintv(N);
-  std::vector<int> type(N), id(N);
-  {
-    const double tm[4] = {0, p.Halo_Mass, p.Disk_Mass, p.Bulge_Mass};
-    int n = 0;
-    for(int t = 1; t <= 3; t++)
-      for(int i = 0; i < nt[t]; i++, n++) {
-        type[n] = t;
-        mass[n] = tm[t] / nt[t];
-        id[n] = n + 1;
-      }
-  }
-  const double *F = h_f.data();
-  if(out) {
-    double *dst[6] = {out->pos, out->vel, out->vel_theo, out->vesc, out->tint, out->targets};
-    const size_t off[6] = {0, 3, 6, 9, 10, 11}, len[6] = {3, 3, 3, 1, 1, 4};
-    for(int k = 0; k < 6; k++)
-      if(dst[k]) std::copy(F + off[k] * N, F + (off[k] + len[k]) * N, dst[k]);
-    if(out->mass) std::copy(mass.begin(), mass.end(), out->mass);
-    if(out->type) std::copy(type.begin(), type.end(), out->type);
-    if(out->id) std::copy(id.begin(), id.end(), out->id);
-    if(out->permutation && rc == GALIC_OK) std::copy(h_perm.begin(), h_perm.end(), out->permutation);
-    for(int t = 0; t < 4; t++)
-      for(int k = 0; k < 4; k++) out->low_disp[t][k] = h_counts[4 * t + k];
-  }
   if(rc != GALIC_OK) return pfail(ctx, rc);
-  // the particles become the context's
-  rc = galic_set_particles(ctx, N, F, F + 3 * (size_t) N, mass.data(), F + 10 * (size_t) N, F + 9 * (size_t) N,
-                           type.data(), F + 11 * (size_t) N);
-  if(rc != GALIC_OK) return rc;
-  ctx->last_launches = launches;
   stream->position = pos;
   return pfail(ctx, GALIC_OK);
 }

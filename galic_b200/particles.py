@@ -22,7 +22,7 @@ FIELDS = (("pos", 3, np.float64), ("vel", 3, np.float64), ("vel_theo", 3, np.flo
 def initialize_particles(ctx, sp, torbit_fac, stream):
     """Runs the initialisation; returns ({field: array}, low-dispersion counts [4, 4])."""
     n = sum(int(ctx.params.NType[t]) for t in (1, 2, 3))
-    arrs = {k: np.zeros((n, w) if w > 1 else n, dtype=dt) for k, w, dt in FIELDS}
+    arrs = {k: np.empty((n, w) if w > 1 else n, dtype=dt) for k, w, dt in FIELDS}  # the call fills every one
     out = _ffi.GalicParticlesOut()
     for k, _, dt in FIELDS:
         setattr(out, k, _ffi.dptr(arrs[k]) if dt == np.float64 else _ffi.iptr(arrs[k]))

@@ -90,7 +90,8 @@ def _gpu_particles(m, sp, tf, tables, stream):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tovs,n", [((1, 3, 2), (400, 200, 100)), ((0, 2, 1), (3000, 1000, 500))])
+@pytest.mark.parametrize("tovs,n", [((1, 3, 2), (400, 200, 100)), ((0, 2, 1), (3000, 1000, 500)),
+                                    ((1, 3, 2), (60000, 20000, 8000))])
 def test_gpu_bit_identical(tovs, n):
     m = particle_model(tovs=tovs, n=n)
     sp, _, tables, tf = setup_inputs(m)
@@ -103,6 +104,38 @@ def test_gpu_bit_identical(tovs, n):
         assert np.array_equal(got[k], ref[k]), k
     assert np.array_equal(got["permutation"], ref["perm"])
     assert np.all(np.isfinite(fit))
+
+
+@pytest.mark.gpu
+def test_gpu_installed_particles_match_upload():
+    """The particles the initialisation leaves in the context (installed on
+    the device, orbit order sorted there) give the same response fields,
+    fit and per-particle results as the same arrays uploaded through
+    galic_set_particles."""
+    from galic_b200 import particles, sampling
+    from galic_b200.context import Context
+    m = particle_model(n=(3000, 1000, 500))
+    sp, _, tables, tf = setup_inputs(m)
+    res = []
+    for upload in (False, True):
+        with Context(m.params) as ctx:
+            ctx.load_model(m)
+            for t, tab in tables.items():
+                sampling.set_dispersion(ctx, t, *tab[:5])
+                ctx.lib.galic_set_vstream(ctx.h, t, _ffi.dptr(np.ascontiguousarray(tab[5], dtype=np.float64).ravel()))
+            out, _ = particles.initialize_particles(ctx, sp, tf, sampling.Stream(42, 0, 0, 7))
+            if upload:
+                ctx.set_particles(out["pos"], out["vel"], out["mass"], out["tint"], out["vesc"], out["type"],
+                                  out["targets"])
+            ctx.calc_all_response_fields()
+            grids = [ctx.response(t, w) for t in (1, 2, 3) for w in range(2)]
+            res.append((grids, ctx.fit(), ctx.particles()))
+    (g0, f0, p0), (g1, f1, p1) = res
+    for a, b in zip(g0, g1):
+        assert np.array_equal(a, b)
+    assert np.array_equal(f0, f1)
+    for a, b in zip(p0, p1):
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.gpu
