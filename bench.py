@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
     ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
     ap.add_argument("--serve-workers", type=int, default=16, help="concurrent jobs of the serving loop")
+    ap.add_argument("--row", default="all", choices=["all", "fill", "sampling", "jeans", "particles"],
+                    help="one secondary measurement alone on this workload (a diagnostic line for profiling, "
+                         "not the bench line)")
     return ap.parse_args()
 
 
@@ -772,7 +775,31 @@ def main():
     if args.impl == "reference":
         reference_arm(args, rank, world)
         return
+    if args.row != "all":
+        row_alone(args)
+        return
     ours_arm(args, rank, world, local_rank)
+
+
+def row_alone(args):
+    """One secondary measurement on the workload, without its CPU baseline."""
+    import torch
+
+    from galic_b200 import Context
+
+    torch.cuda.set_device(0)
+    model = build_workload(args.scale, seed=2)
+    if args.row == "fill":
+        res = measure_fill(model, args.steps, False, measured_fp64_peak(torch))
+    elif args.row == "sampling":
+        with Context(model.params) as ctx:
+            ctx.load_model(model)
+            res = measure_sampling(model, ctx, args.steps, False)
+    elif args.row == "jeans":
+        res = measure_jeans(model, args.steps, False)
+    else:
+        res = measure_particles(model, args.steps, False)
+    print(json.dumps({"row": args.row, "steps": args.steps, **res}), flush=True)
 
 
 if __name__ == "__main__":

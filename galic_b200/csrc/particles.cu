@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "context.cuh"
@@ -85,21 +86,22 @@ __device__ __forceinline__ double halo_f(const DevModel &M, double rad, double v
 
 // one call of the type's *_get_fresh_coordinate from the stream g
 // (halo.c:17-40, disk.c:17-50, bulge.c:15-37); false when capped
-__device__ bool fresh_seq(const Shape &S, int type, grng_t &g, double *pos)
+template <int TYPE>
+__device__ bool fresh_seq(const Shape &S, grng_t &g, double *pos)
 {
-  if(type == 1 || type == 2) {
+  if constexpr(TYPE == 1 || TYPE == 2) {
     for(int it = 0; it < LOOP_CAP; it++) {
       const double d0 = grng_uniform(&g), d1 = grng_uniform(&g), d2 = grng_uniform(&g);
-      if(type == 1 ? halo_draw(S, d0, d1, d2, pos) : disk_draw(S, d0, d1, d2, pos)) return true;
+      if(TYPE == 1 ? halo_draw(S, d0, d1, d2, pos) : disk_draw(S, d0, d1, d2, pos)) return true;
     }
-    return false;
-  }
-  for(int it = 0; it < LOOP_CAP; it++) {
-    const double r = bulge_radius(S, grng_uniform(&g));
-    if(!(r > S.Rmax)) {
-      const double d1 = grng_uniform(&g), d2 = grng_uniform(&g);
-      bulge_place(S, r, d1, d2, pos);
-      return true;
+  } else {
+    for(int it = 0; it < LOOP_CAP; it++) {
+      const double r = bulge_radius(S, grng_uniform(&g));
+      if(!(r > S.Rmax)) {
+        const double d1 = grng_uniform(&g), d2 = grng_uniform(&g);
+        bulge_place(S, r, d1, d2, pos);
+        return true;
+      }
     }
   }
   return false;
@@ -161,20 +163,25 @@ __device__ bool halo_velocity_warp(const PInit &P, bool need, double r, double v
   return ok;
 }
 
-// one iteration of initialize_particles' loop (set_particles.c:64-237) from
-// stream position `start`, called by all 32 lanes of a warp together
-// (active: the lane has a particle).  Returns the draws it took (LEN_CAPPED
-// when a rejection loop hit its cap).  With o != nullptr the particle's
-// values are stored at index n.
-__device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool active, const POut *o, int n)
+// one iteration of initialize_particles' loop (set_particles.c:64-237) for a
+// particle of type TYPE from stream position `start`, called by all 32 lanes
+// of a warp together (active: the lane has a particle).  VS: the velocity
+// structure's frame, 0 spherical (TypeOfVelocityStructure 0, 1, 3) or 1
+// cylindrical (2); one launch has one type and one frame, so each kernel
+// carries only its own branches.  Returns the draws it took (LEN_CAPPED when
+// a rejection loop hit its cap).  With o != nullptr the particle's values are
+// stored at index n.
+template <int TYPE, int VS>
+__device__ uint32_t init_one(const PInit &P, uint64_t start, bool active, const POut *o, int n)
 {
+  constexpr int type = TYPE;
   grng_t g;
   grng_init(&g, P.seed, P.sa, P.sb);
   grng_seek(&g, start);
   const DevModel &M = P.M;
   const LogConsts L = make_log_consts(M);
   double pos[3] = {0, 0, 0};
-  bool ok = active && fresh_seq(P.S, type, g, pos);
+  bool ok = active && fresh_seq<TYPE>(P.S, g, pos);
   double vesc = 0, tint = 0, r = 0;
   FgCoord fc{};
   if(ok) {
@@ -188,7 +195,7 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool acti
     tint = P.TorbitFac * 2 * kPi * r / sqrt(r * a);
   }
   double vt[3] = {0, 0, 0};
-  if(type == 1) {  // uniform over the launch: every lane takes this branch
+  if constexpr(TYPE == 1) {
     uint64_t w = grng_position(&g);
     double vr = 0;
     const bool vok = halo_velocity_warp(P, ok, r, vesc, w, vr);
@@ -217,7 +224,7 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool acti
   const double vstr = vstream_at(M, fc, type);
   double V[3];
   const double sigmaR = sqrt(d[0]), sigmaT = sqrt(d[1]), sigmaP = sqrt(d[2]);
-  if(D.tovs == 0 || D.tovs == 1 || D.tovs == 3) {
+  if constexpr(VS == 0) {
     double v, vr, vphi, vtheta;
     int it = 0;
     do {
@@ -278,11 +285,12 @@ __device__ uint32_t init_one(const PInit &P, int type, uint64_t start, bool acti
 // the successor of every position o in [0, R) from `base`: next[o] = o + the
 // draws of a particle started at o, R when that is past R, R + 1 when a
 // rejection loop capped (whole warps run init_one together: lanes past R only keep the others company)
-__global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, int type, uint64_t base, uint32_t R, uint32_t *next)
+template <int TYPE, int VS>
+__global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, uint64_t base, uint32_t R, uint32_t *next)
 {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = o < R;
-  const uint32_t len = init_one(P, type, base + (active ? o : 0), active, nullptr, 0);
+  const uint32_t len = init_one<TYPE, VS>(P, base + (active ? o : 0), active, nullptr, 0);
   if(o >= R + 2) return;
   if(!active) {
     next[o] = o;
@@ -327,8 +335,8 @@ __device__ __forceinline__ bool bit_at(const uint32_t *w, uint64_t a, uint64_t q
 
 // every segment decoded from its own first position (whole warps run
 // init_one together: lanes past K only keep the others company)
-__global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, int type, uint64_t base, const Segs S,
-                                                       uint64_t *exit)
+template <int TYPE, int VS>
+__global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, uint64_t base, const Segs S, uint64_t *exit)
 {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = c < S.K;
@@ -337,7 +345,7 @@ __global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, int type, 
   uint64_t q = a;
   bool work = valid;
   while(__any_sync(0xffffffffu, work)) {
-    const uint32_t len = init_one(P, type, base + (work ? q : 0), work, nullptr, 0);
+    const uint32_t len = init_one<TYPE, VS>(P, base + (work ? q : 0), work, nullptr, 0);
     if(work) {
       w[(q - a) >> 5] |= 1u << (q & 31);
       if(len == LEN_CAPPED || len == 0) {
@@ -381,7 +389,8 @@ __global__ void k_seg_prep(const Segs S, const uint64_t *pmax, const uint64_t *e
 // when that one is not flagged (so no two lanes touch one segment), as the
 // next round would.  After round r segments 0 .. r are exact; the rounds end
 // when no exit changes.
-__global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, int type, uint64_t base, const Segs S,
+template <int TYPE, int VS>
+__global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, uint64_t base, const Segs S,
                                                     const uint64_t *pmax, const uint8_t *flag,
                                                     const uint64_t *exit_in, uint64_t *exit_out, int *changed)
 {
@@ -420,7 +429,7 @@ __global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, int type, uin
         step = true;
       }
     }
-    const uint32_t len = init_one(P, type, base + (step ? q : 0), step, nullptr, 0);
+    const uint32_t len = init_one<TYPE, VS>(P, base + (step ? q : 0), step, nullptr, 0);
     if(step) {
       w[(q - a) >> 5] |= 1u << (q & 31);
       if(len == LEN_CAPPED || len == 0) {
@@ -473,12 +482,30 @@ __global__ void k_seg_extract(const Segs S, const unsigned *first, const uint64_
       starts[r++] = a + 32ull * k + (uint64_t) (__ffs(m) - 1);
 }
 
-__global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, int type, uint64_t base, const uint64_t *starts,
-                                                  int count, int n0, POut o)
+// each particle once more from its start, keeping its values.  Thread j
+// takes the particle of length rank (j mod 32) * warps + j / 32 (ord: the
+// particles by length, longest first): the longest particles start first,
+// one to a warp, and no warp holds two of them.
+template <int TYPE, int VS>
+__global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, uint64_t base, const uint64_t *starts,
+                                                  const int *ord, int count, int n0, POut o)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int warps = (count + 31) / 32;
+  const long long rank = (long long) (j & 31) * warps + (j >> 5);
+  const bool active = j < warps * 32 && rank < count;
+  const int i = active ? ord[rank] : 0;
+  init_one<TYPE, VS>(P, base + (active ? starts[i] : 0), active, &o, n0 + i);
+}
+
+// particle lengths as sort keys (clamped to 32 bits) and their indices
+__global__ void k_len_keys(const uint64_t *starts, int count, uint32_t *key, int *idx)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = i < count;
-  init_one(P, type, base + (active ? starts[i] : 0), active, &o, n0 + (active ? i : 0));
+  if(i >= count) return;
+  const uint64_t len = starts[i + 1] - starts[i];
+  key[i] = len > 0xffffffffull ? 0xffffffffu : (uint32_t) len;
+  idx[i] = i;
 }
 
 // permutation[].rnd (set_particles.c:298-301): the bits of a uniform in [0, 1)
@@ -510,6 +537,23 @@ int pfail(galic_ctx *ctx, int st)
 }
 
 inline unsigned gblocks(long long n, int b) { return (unsigned) ((n + b - 1) / b); }
+
+// f(TYPE, VS) with the particle type (1-3) and the velocity frame (0, 1) as
+// compile-time constants
+template <class F>
+void with_kind(int type, int vs, F &&f)
+{
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  using I3 = std::integral_constant<int, 3>;
+  using V0 = std::integral_constant<int, 0>;
+  if(type == 1)
+    vs ? f(I1{}, I1{}) : f(I1{}, V0{});
+  else if(type == 2)
+    vs ? f(I2{}, I1{}) : f(I2{}, V0{});
+  else
+    vs ? f(I3{}, I1{}) : f(I3{}, V0{});
+}
 
 }  // namespace
 
@@ -587,6 +631,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     int n0 = 0;
     for(int t = 1; t <= 3 && rc == GALIC_OK; n0 += nt[t], t++) {
       if(nt[t] == 0) continue;
+      const int vs = p.TypeOfVelocityStructure[t] == 2 ? 1 : 0;
       // draws per particle, from the lengths at the segment's first positions
       uint32_t R = PROBE;
       std::vector<uint32_t> probe(PROBE + 2);
@@ -595,7 +640,9 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         J_cap = (size_t) R + 2;
         PCK(cudaMallocAsync((void **) &d_J, J_cap * sizeof(uint32_t), s));
       }
-      k_len<<<gblocks(R + 2, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, R, d_J);
+      with_kind(t, vs, [&](auto T, auto V) {
+        k_len<decltype(T)::value, decltype(V)::value><<<gblocks(R + 2, PBLOCK), PBLOCK, 0, s>>>(P, pos, R, d_J);
+      });
       launches++;
       PCK(cudaGetLastError());
       PCK(cudaMemcpyAsync(probe.data(), d_J, (R + 2) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -629,14 +676,17 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         G.K = (uint32_t) Kd;
         G.W = (uint32_t) (Lseg / 32);
         const size_t K = G.K;
-        size_t tb = 0, tb2 = 0;
+        size_t tb = 0, tb2 = 0, tb3 = 0;
         PCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (uint64_t *) nullptr, (uint64_t *) nullptr, K + 1, s));
         PCK(cub::DeviceScan::InclusiveScan(nullptr, tb2, (uint64_t *) nullptr, (uint64_t *) nullptr, MaxU64(), K, s));
-        tb = std::max(tb, tb2);
+        PCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb3, (uint32_t *) nullptr, (uint32_t *) nullptr,
+                                                      (int *) nullptr, (int *) nullptr, nt[t], 0, 32, s));
+        tb = std::max(std::max(tb, tb2), tb3);
         const auto al = [](size_t n) { return (n + 255) / 256 * 256; };
         const size_t sz_bits = al(K * G.W * sizeof(uint32_t)), sz_k = al(K * sizeof(uint64_t)),
-                     sz_k1 = al((K + 1) * sizeof(uint64_t)), sz_st = al(((size_t) nt[t] + 1) * sizeof(uint64_t));
-        const size_t need = sz_bits + 5 * sz_k + al(K) + 2 * sz_k1 + 256 + al(tb) + sz_st;
+                     sz_k1 = al((K + 1) * sizeof(uint64_t)), sz_st = al(((size_t) nt[t] + 1) * sizeof(uint64_t)),
+                     sz_n = al((size_t) nt[t] * sizeof(uint32_t));
+        const size_t need = sz_bits + 5 * sz_k + al(K) + 2 * sz_k1 + 256 + al(tb) + sz_st + 4 * sz_n;
         if(seg_cap < need) {
           if(d_seg) cudaFreeAsync(d_seg, s);
           d_seg = nullptr;
@@ -661,8 +711,14 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         void *d_scan = cur;
         cur += al(tb);
         d_starts = (uint64_t *) cur;
+        cur += sz_st;
+        uint32_t *d_lkey = (uint32_t *) cur, *d_lkey2 = (uint32_t *) (cur + sz_n);
+        int *d_lidx = (int *) (cur + 2 * sz_n), *d_ord = (int *) (cur + 3 * sz_n);
         PCK(cudaMemsetAsync(G.bits, 0, sz_bits, s));
-        k_seg_decode<<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, G, ex[0]);
+        with_kind(t, vs, [&](auto T, auto V) {
+          k_seg_decode<decltype(T)::value, decltype(V)::value>
+              <<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, pos, G, ex[0]);
+        });
         launches++;
         PCK(cudaGetLastError());
         int fin = -1;
@@ -674,8 +730,10 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
           PCK(cub::DeviceScan::InclusiveScan(d_scan, tbr, in, d_pmax, MaxU64(), K, s));
           k_seg_prep<<<gblocks((long long) K, 256), 256, 0, s>>>(G, d_pmax, in, out_, d_flag);
           PCK(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
-          k_seg_fix<<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, t, pos, G, d_pmax, d_flag, in, out_,
-                                                                      d_changed);
+          with_kind(t, vs, [&](auto T, auto V) {
+            k_seg_fix<decltype(T)::value, decltype(V)::value>
+                <<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, pos, G, d_pmax, d_flag, in, out_, d_changed);
+          });
           launches += 3;
           PCK(cudaGetLastError());
           PCK(cudaMemcpyAsync(&h_changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -692,8 +750,8 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         PCK(cudaMemsetAsync(d_first, 0xff, sizeof(unsigned), s));
         k_seg_first_cap<<<gblocks((long long) K, 256), 256, 0, s>>>(ex[fin], G.K, d_first);
         k_seg_count<<<gblocks((long long) K + 1, 256), 256, 0, s>>>(G, d_first, d_cnt);
-        size_t tbe = tb;
-        PCK(cub::DeviceScan::ExclusiveSum(d_scan, tbe, d_cnt, d_off, K + 1, s));
+        size_t tbx = tb;
+        PCK(cub::DeviceScan::ExclusiveSum(d_scan, tbx, d_cnt, d_off, K + 1, s));
         launches += 3;
         PCK(cudaGetLastError());
         uint64_t total = 0;
@@ -714,8 +772,14 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         uint64_t end = 0;
         PCK(cudaMemcpyAsync(&end, d_starts + nt[t], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         PCK(cudaStreamSynchronize(s));
-        k_final<<<gblocks(nt[t], PBLOCK), PBLOCK, 0, s>>>(P, t, pos, d_starts, nt[t], n0, O);
-        launches++;
+        k_len_keys<<<gblocks(nt[t], 256), 256, 0, s>>>(d_starts, nt[t], d_lkey, d_lidx);
+        tbx = tb;
+        PCK(cub::DeviceRadixSort::SortPairsDescending(d_scan, tbx, d_lkey, d_lkey2, d_lidx, d_ord, nt[t], 0, 32, s));
+        with_kind(t, vs, [&](auto T, auto V) {
+          k_final<decltype(T)::value, decltype(V)::value>
+              <<<gblocks(nt[t], PBLOCK), PBLOCK, 0, s>>>(P, pos, d_starts, d_ord, nt[t], n0, O);
+        });
+        launches += 3;
         PCK(cudaGetLastError());
         pos += end;
         break;
