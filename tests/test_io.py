@@ -29,13 +29,9 @@ def test_snapshot_matches_reference(fmt, tmp_path):
     sp, _, tables, tf = TP.setup_inputs(m)
     ref, data = oracle_lib.run_reference(oracle_lib.reference_snapshot, m.params, (m.pot, m.dpotdr, m.dpotdz), sp, tf,
                                          tables, (42, 0, 0, 3), fmt)
-    lib = _ffi.load_library()
-    fn = str(tmp_path / "snap_000")
-    arr = {k: np.ascontiguousarray(ref[k]) for k in ("pos", "vel", "vel_theo", "mass", "id", "type")}
-    st = lib.galic_write_snapshot(fn.encode(), fmt, len(arr["mass"]), _ffi.dptr(arr["pos"]), _ffi.dptr(arr["vel"]),
-                                  _ffi.dptr(arr["vel_theo"]), _ffi.dptr(arr["mass"]), _ffi.iptr(arr["id"]),
-                                  _ffi.iptr(arr["type"]), None)
-    assert st == 0
+    from galic_b200 import io
+    fn = io.output_particles(str(tmp_path) + "/", "snap", 0, ref, snap_format=fmt)
+    assert fn.endswith("snap_000")
     got = open(fn, "rb").read()
     assert len(got) == len(data) and got == data
 
@@ -47,11 +43,9 @@ def test_forcefield_matches_reference(tmp_path):
     p, rmax = case_params("hdb", 20)
     rf = oracle_lib.RefFillParams(0.1, 0.5, 3.0, 3.5, 0.7, rmax, 2, 600, 300, 100, 77)
     dpotdr, dpotdz, pot, data = oracle_lib.run_reference(oracle_lib.reference_forcefield, p, rf)
-    lib = _ffi.load_library()
+    from galic_b200 import io
     fn = str(tmp_path / "forcefield.dat")
-    st = lib.galic_write_forcefield(fn.encode(), C.byref(p), *[_ffi.dptr(np.ascontiguousarray(a))
-                                                               for a in (dpotdr, dpotdz, pot)])
-    assert st == 0
+    io.write_forcefield(fn, p, dpotdr, dpotdz, pot)
     assert open(fn, "rb").read() == data
 
 
@@ -95,7 +89,8 @@ def test_gpu_output_density_field(tmp_path):
     with Context(m.params) as ctx:
         ctx.load_model(m)
         ctx.calc_all_response_fields()
-        assert lib.galic_output_density_field(ctx.h, str(tmp_path).encode(), 7) == 0
+        from galic_b200 import io
+        io.output_density_field(ctx, tmp_path, 7)
         for t in (1, 2):
             tg = sampling.get_targets(ctx, t)
             loc = [ctx.response(t, w) for w in (_ffi.GRID_MASS_S, _ffi.GRID_MASS_I, _ffi.GRID_R_I, _ffi.GRID_T_I,
