@@ -40,45 +40,75 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
 }
 
 // FP32 variant.  A lane parks one record per grid node that leaves its
-// accumulators: the node's word index and its five sums already scaled by
-// value x 2^(shift-24) in FP32 (the orbit's mass/Tint and the field's
-// fixed-point scale are folded into one FP32 factor per field class when the
-// orbit starts).  The drain rounds each item to one
+// accumulators: the node's index and its five sums.  The drain scales them
+// by value x 2^(shift-24) in FP32 (the orbit's mass/Tint and the field's
+// fixed-point scale folded into one FP32 factor per field class when the
+// orbit starts, kept in the lane's queue header), rounds each item to one
 // signed 64-bit fixed-point word, X = round(scaled value), and adds it to the
 // high word of the bin (the low word stays zero, so fx_value reads it
 // unchanged).  shift - 24 is chosen so that no bin can overflow 2^62; the
 // FP32 rounding of the scaled value (2^-24 relative) is far inside the FP32
 // form's tolerance, and one atomic per value instead of two halves the L2
 // atomic traffic.
+// Each lane parks its node records in its own column of the warp's queue
+// (no reservation atomic); a lane parks at most 4 records per loop iteration
+// (one cell's nodes), so the warp drains before any lane could pass PER.
+// The drain compacts all lanes' records and every lane adds the five words of
+// one record at a time, so the global atomics run on full warps.  PER is
+// chosen per block size so that the queues fit the static shared memory.
+template <int PER_>
 struct WarpQueue32 {
-  int base[32 * 4];      // word of the node's mass field; field f is base + f * Ngrid
-  float val[32 * 4][5];  // the node's five sums, scaled to fixed point
-  int n;                 // records parked since the last drain
-  int gbase[32];         // per lane: first word of its orbit's grid set
-  float2 scale[32];      // per lane: {mass field, energy fields} fixed-point factors
+  static constexpr int PER = PER_;
+  int base[PER][32];      // the node's index in its grid (field f of the orbit's set: gbase + f * Ngrid + base)
+  float val[PER][5][32];  // the node's five sums
+  int off[32];            // drain: first compacted record of each lane
+  int gbase[32];          // per lane: first word of its orbit's grid set
+  float2 scale[32];       // per lane: {mass field, energy fields} fixed-point factors
 };
 
-// a lane reserves room for `count` node records; returns the first index
-__device__ __forceinline__ int queue32_reserve(WarpQueue32 &q, int count) { return atomicAdd(&q.n, count); }
+// records per lane of a block of BLOCK threads
+__host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 8 : (block <= 192 ? 7 : 5); }
 
-// all 32 lanes call this at the same point of the loop; each lane adds the
-// five words of one parked node record at a time
-__device__ __forceinline__ void warp_drain32(WarpQueue32 &q, FxWord *fx, int G)
+// true when some lane could not park another cell's nodes
+template <int PER>
+__device__ __forceinline__ bool queue32_due(int cnt)
 {
-  __syncwarp();
+  return __any_sync(0xffffffffu, cnt > PER - 4);
+}
+
+// all 32 lanes call this at the same point of the loop with their record
+// counts; cnt is 0 on return
+template <int PER>
+__device__ __forceinline__ void warp_drain32(WarpQueue32<PER> &q, FxWord *fx, int G, int &cnt)
+{
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int records = q.n;
-  for(int r = lane; r < records; r += 32) {
-    const int b = q.base[r];
+  int incl = cnt;
+#pragma unroll
+  for(int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if(lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(FULL, incl, 31);
+  q.off[lane] = incl - cnt;
+  __syncwarp();
+  for(int r = lane; r < total; r += 32) {
+    // the lane L whose records hold r: the last L with off[L] <= r
+    int L = 0;
+#pragma unroll
+    for(int step = 16; step; step >>= 1)
+      if(q.off[L + step] <= r) L += step;
+    const int k = r - q.off[L];
+    const int b = q.gbase[L] + q.base[k][L];
+    const float2 sc = q.scale[L];
 #pragma unroll
     for(int f = 0; f < 5; f++) {
-      const long long X = __float2ll_rn(q.val[r][f]);
+      const long long X = __float2ll_rn(q.val[k][f][L] * (f == 0 ? sc.x : sc.y));
       if(X) atomicAdd(&fx[b + f * G].hi, (unsigned long long) X);
     }
   }
   __syncwarp();
-  if(lane == 0) q.n = 0;
-  __syncwarp();
+  cnt = 0;
 }
 
 #endif

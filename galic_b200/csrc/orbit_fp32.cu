@@ -221,13 +221,13 @@ struct NodeAcc {
 };
 
 // Sink of the batched kernels: on a cell change the nonzero sums of the
-// leaving nodes are parked in the lane's slot of the warp queue as
-// (word index, scaled value) items, and the warp drains all parked slots
-// together (flush.cuh).
+// leaving nodes are parked in the warp queue as (word index, scaled value)
+// records, and the warp drains them together once enough wait (flush.cuh).
+template <int PER>
 struct Sink32 : NodeAcc {
-  WarpQueue32 *q;
+  WarpQueue32<PER> *q;
   int lane, Nb;
-  bool parked;
+  int cnt;  // records parked in this lane's queue column since the last drain
   // the orbit's first word (grid set x NG_COMMITTED x Ngrid) and the scale
   // factors mass/Tint x 2^(shift-24) of the mass and energy fields, kept in
   // the lane's queue header (read only when parking)
@@ -238,28 +238,26 @@ struct Sink32 : NodeAcc {
   }
   __device__ __forceinline__ void park_masked(const bool out[4])
   {
-    // a node with no mass has no deposit at all (every field is weight x ...)
+    // a node with no mass has no deposit at all (every field is weight x ...);
+    // the records keep the raw sums and the node's index in the grid, the
+    // drain adds the orbit's grid set and scale factors
     bool rec[4];
-    int n = 0;
+    int at[4], k = cnt;
 #pragma unroll
     for(int s = 0; s < 4; s++) {
       rec[s] = out[s] && a[s][0] != 0.f;
-      n += rec[s] ? 1 : 0;
+      at[s] = k;
+      k += rec[s] ? 1 : 0;
     }
-    if(n == 0) return;
-    int at = queue32_reserve(*q, n);
-    const int gbase = q->gbase[lane];
-    const float2 sc = q->scale[lane];
 #pragma unroll
     for(int s = 0; s < 4; s++) {
-      if(!rec[s]) continue;
-      q->base[at] = gbase + (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
-      q->val[at][0] = a[s][0] * sc.x;
+      if(rec[s]) {
+        q->base[at[s]][lane] = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
 #pragma unroll
-      for(int f = 1; f < 5; f++) q->val[at][f] = a[s][f] * sc.y;
-      at++;
+        for(int f = 0; f < 5; f++) q->val[at[s]][f][lane] = a[s][f];
+      }
     }
-    parked = true;
+    cnt = k;
   }
   __device__ __forceinline__ void park()
   {
@@ -314,7 +312,7 @@ struct State32 {
   int norbit, flag, type, tovs, steps, status;
 };
 
-enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
+enum { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2, LANE_LAST = 3, LANE_START = 4 };
 
 // orbit_response.c:172-206 in FP32: initial state of one orbit
 __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const double *xd, const double *vd,
@@ -353,7 +351,9 @@ __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const
 // The end-of-step deposit and the next step's start deposit sit at the same
 // position, cell and projections, so they are made as one deposit with the
 // two half-step weights added (the last one when the orbit ends).
-template <class Sink>
+// DEFER_LAST: the last half-step's deposit is left to the caller
+// (orbit32_last), so that one call parks at most one cell's nodes.
+template <class Sink, bool DEFER_LAST = false>
 __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink &sink)
 {
   // get_timestep (orbit_response.c:16-26)
@@ -406,8 +406,15 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
     s.status = ORBIT_STEP_CAP;
     return false;
   }
-  if(s.flag) sink.add(s.iR, s.iz, s.pend, s.fR, s.fz, s.proj);
+  if(!DEFER_LAST && s.flag) sink.add(s.iR, s.iz, s.pend, s.fR, s.fz, s.proj);
   return !s.flag;
+}
+
+// the deposit orbit32_step<Sink, true> left when the orbit ended normally
+template <class Sink>
+__device__ __forceinline__ void orbit32_last(const State32 &s, Sink &sink)
+{
+  sink.add(s.iR, s.iz, s.pend, s.fR, s.fz, s.proj);
 }
 
 // Particle arrays of one model
@@ -520,11 +527,11 @@ __device__ __forceinline__ LogConsts pot_logs(const DevModel &M)
 template <int BLOCK, class Src>
 __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
 {
-  __shared__ WarpQueue32 queues[BLOCK / 32];
+  constexpr int PER = queue32_per(BLOCK);
+  __shared__ WarpQueue32<PER> queues[BLOCK / 32];
   // values a lane needs only when an orbit starts or ends, out of registers
   __shared__ LaneAux aux_all[BLOCK];
   LaneAux &aux = aux_all[threadIdx.x];
-  if((threadIdx.x & 31) == 0) queues[threadIdx.x >> 5].n = 0;
   aux.p = -1;
   aux.stat_mi = 0;
   aux.steps = 0;
@@ -533,11 +540,11 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
   __syncwarp();
   const int G = S.model64(0).DG_Ngrid;
   State32 s;
-  Sink32 sink;
+  Sink32<PER> sink;
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
   sink.cur = -1;
-  sink.parked = false;
+  sink.cnt = 0;
   int mi = 0;
 
   auto begin = [&]() -> bool {
@@ -579,13 +586,17 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
 
   int state = begin() ? LANE_ACTIVE : LANE_DONE;
   for(;;) {
-    if(__any_sync(0xffffffffu, sink.parked)) {
-      warp_drain32(*sink.q, S.fx, G);
-      sink.parked = false;
-    }
-    if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
+    const bool all_done = !__any_sync(0xffffffffu, state != LANE_DONE);
+    // records carry the orbit's grid set and scale only through the lane's
+    // queue header, so a lane drains them before it starts the next orbit
+    if(queue32_due<PER>(sink.cnt) || __any_sync(0xffffffffu, (all_done || state == LANE_START) && sink.cnt > 0))
+      warp_drain32(*sink.q, S.fx, G, sink.cnt);
+    if(all_done) break;
     if(state == LANE_ACTIVE) {
-      if(!orbit32_step(S.model(mi), s, sink)) state = LANE_FINISH;
+      if(!orbit32_step<Sink32<PER>, true>(S.model(mi), s, sink)) state = s.status == ORBIT_OK ? LANE_LAST : LANE_FINISH;
+    } else if(state == LANE_LAST) {
+      orbit32_last(s, sink);
+      state = LANE_FINISH;
     } else if(state == LANE_FINISH) {
       sink.park();
       S.particles(mi).orbits[aux.p] = s.norbit;
@@ -600,6 +611,8 @@ __device__ __forceinline__ void calc_all_fp32_body(const Src &S)
         double e = fabs((E1 - aux.E0) / aux.E0);
         if(e > aux.err) aux.err = e;
       }
+      state = LANE_START;
+    } else if(state == LANE_START) {
       state = begin() ? LANE_ACTIVE : LANE_DONE;
     }
   }
