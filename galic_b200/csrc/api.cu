@@ -588,6 +588,8 @@ cudaError_t order_by_type_radius(galic_ctx *ctx, const int nt[4])
 
 namespace galic_internal {
 
+cudaError_t keep_device_pool(int device) { return keep_pool_memory(device); }
+
 // installs particles whose arrays are on the device, stored type by type
 // (nt[t] particles of type t, masses tmass[t] / nt[t]), as galic_set_particles
 // does from the host

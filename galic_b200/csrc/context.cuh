@@ -92,6 +92,8 @@ void set_shifts(galic_ctx *ctx, int *shift, int form);
 // FP32 force tables of the context, rebuilt after any table upload
 int ensure_tab32(galic_ctx *ctx);
 FitArgs make_fit_args(galic_ctx *ctx);
+// keeps the device's default memory pool mapped between calls (once per device)
+cudaError_t keep_device_pool(int device);
 // installs particles whose arrays are on the device, stored type by type
 int set_particles_device(galic_ctx *ctx, const int nt[4], const double tmass[4], const double *pos,
                          const double *vel, const double *tint, const double *vesc, const double *targets);

@@ -46,6 +46,7 @@
 #include <mutex>
 #include <vector>
 
+#include "context.cuh"
 #include "galic_gpu.h"
 
 namespace {
@@ -689,9 +690,21 @@ struct TopTree {
   }
 };
 
+// Scratch comes from the device's stream-ordered pool (kept mapped between
+// calls), allocated and released in the calling thread's default stream: a
+// fill allocates some thirty buffers, and plain cudaMalloc / cudaFree (which
+// synchronises the device) cost more than the walk.  The kernels run in the
+// legacy default stream, which orders itself with the per-thread stream.
+inline cudaError_t dmalloc(void **p, size_t bytes) { return cudaMallocAsync(p, bytes, cudaStreamPerThread); }
+inline void dfree_async(void *&p)
+{
+  if(p) cudaFreeAsync(p, cudaStreamPerThread);
+  p = nullptr;
+}
+
 struct DevBuf {
   void *p = nullptr;
-  ~DevBuf() { cudaFree(p); }
+  ~DevBuf() { dfree_async(p); }
   template <class T> T *as() { return static_cast<T *>(p); }
 };
 
@@ -744,15 +757,20 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     trig[s] = std::cos(phi);
     trig[kSections + s] = std::sin(phi);
   }
+  {
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess || galic_internal::keep_device_pool(dev) != cudaSuccess)
+      return GALIC_ERR_CUDA;
+  }
   if(!upload_tables()) {
     fprintf(stderr, "galic_cuda: Peano-Hilbert table upload failed\n");
     return GALIC_ERR_CUDA;
   }
   DevBuf d_pos, d_key, d_key2, d_idx, d_idx2, d_tmp, d_r1, d_z1, d_trig, d_part;
-  FCK(cudaMalloc(&d_pos.p, 3 * (size_t) ntot * sizeof(double)));
-  FCK(cudaMalloc(&d_r1.p, N * sizeof(double)));
-  FCK(cudaMalloc(&d_z1.p, N * sizeof(double)));
-  FCK(cudaMalloc(&d_trig.p, sizeof(trig)));
+  FCK(dmalloc(&d_pos.p, 3 * (size_t) ntot * sizeof(double)));
+  FCK(dmalloc(&d_r1.p, N * sizeof(double)));
+  FCK(dmalloc(&d_z1.p, N * sizeof(double)));
+  FCK(dmalloc(&d_trig.p, sizeof(trig)));
   FCK(cudaMemcpy(d_pos.p, pos, 3 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_r1.p, r1.data(), N * sizeof(double), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_z1.p, z1.data(), N * sizeof(double), cudaMemcpyHostToDevice));
@@ -762,7 +780,7 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cudaGetLastError());
   // domain_findExtent (domain_box.c:20-65)
   const int EB = 592;
-  FCK(cudaMalloc(&d_part.p, 6 * EB * sizeof(double)));
+  FCK(dmalloc(&d_part.p, 6 * EB * sizeof(double)));
   k_extent<<<EB, 256>>>(ntot, d_pos.as<double>(), d_part.as<double>());
   std::vector<double> part(6 * EB);
   FCK(cudaMemcpy(part.data(), d_part.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -785,10 +803,10 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   if(!(len > 0) || !std::isfinite(inv_len)) return GALIC_ERR_INVALID_ARGUMENT;
 
   // keys of all points and their stable key order (peano.c:63-104)
-  FCK(cudaMalloc(&d_key.p, (size_t) ntot * sizeof(unsigned long long)));
-  FCK(cudaMalloc(&d_key2.p, (size_t) ntot * sizeof(unsigned long long)));
-  FCK(cudaMalloc(&d_idx.p, (size_t) ntot * sizeof(int)));
-  FCK(cudaMalloc(&d_idx2.p, (size_t) ntot * sizeof(int)));
+  FCK(dmalloc(&d_key.p, (size_t) ntot * sizeof(unsigned long long)));
+  FCK(dmalloc(&d_key2.p, (size_t) ntot * sizeof(unsigned long long)));
+  FCK(dmalloc(&d_idx.p, (size_t) ntot * sizeof(int)));
+  FCK(dmalloc(&d_idx2.p, (size_t) ntot * sizeof(int)));
   k_keys<<<(ntot + 255) / 256, 256>>>(ntot, d_pos.as<double>(), corner[0], corner[1], corner[2], inv_len,
                                       d_key.as<unsigned long long>(), d_idx.as<int>());
   FCK(cudaGetLastError());
@@ -796,7 +814,7 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   FCK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_key.as<unsigned long long>(),
                                       d_key2.as<unsigned long long>(), d_idx.as<int>(), d_idx2.as<int>(), ntot, 0,
                                       3 * kBits));
-  FCK(cudaMalloc(&d_tmp.p, tmp_bytes));
+  FCK(dmalloc(&d_tmp.p, tmp_bytes));
   FCK(cub::DeviceRadixSort::SortPairs(d_tmp.p, tmp_bytes, d_key.as<unsigned long long>(),
                                       d_key2.as<unsigned long long>(), d_idx.as<int>(), d_idx2.as<int>(), ntot, 0,
                                       3 * kBits));
@@ -814,14 +832,14 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
                       std::vector<int> &cnt) -> int {
       const size_t nq = pre.size();
       if(nq > cap) {
-        cudaFree(d_qp.p);
-        cudaFree(d_ql.p);
-        cudaFree(d_qc.p);
+        dfree_async(d_qp.p);
+        dfree_async(d_ql.p);
+        dfree_async(d_qc.p);
         d_qp.p = d_ql.p = d_qc.p = nullptr;
         cap = std::max<size_t>(nq, 4096);
-        FCK(cudaMalloc(&d_qp.p, cap * sizeof(unsigned long long)));
-        FCK(cudaMalloc(&d_ql.p, cap * sizeof(int)));
-        FCK(cudaMalloc(&d_qc.p, cap * sizeof(int)));
+        FCK(dmalloc(&d_qp.p, cap * sizeof(unsigned long long)));
+        FCK(dmalloc(&d_ql.p, cap * sizeof(int)));
+        FCK(dmalloc(&d_qc.p, cap * sizeof(int)));
       }
       FCK(cudaMemcpy(d_qp.p, pre.data(), nq * sizeof(unsigned long long), cudaMemcpyHostToDevice));
       FCK(cudaMemcpy(d_ql.p, lev.data(), nq * sizeof(int), cudaMemcpyHostToDevice));
@@ -850,15 +868,15 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
   DevBuf d_mass, d_hi, d_lo, d_hi2, d_lo2, d_pidx, d_pidx2, d_pidx3, d_lstart, d_llevel, d_leaf_of, d_lolev, d_nitem,
       d_off, d_flag, d_loff0, d_loff1, d_lfirst, d_litem, d_lskip, d_tmp2;
   const int TB = 256, TG = (n + TB - 1) / TB;
-  FCK(cudaMalloc(&d_mass.p, (size_t) n * sizeof(double)));
+  FCK(dmalloc(&d_mass.p, (size_t) n * sizeof(double)));
   FCK(cudaMemcpy(d_mass.p, mass, (size_t) n * sizeof(double), cudaMemcpyHostToDevice));
-  for(DevBuf *b : {&d_hi, &d_lo, &d_hi2, &d_lo2}) FCK(cudaMalloc(&b->p, (size_t) n * sizeof(unsigned long long)));
+  for(DevBuf *b : {&d_hi, &d_lo, &d_hi2, &d_lo2}) FCK(dmalloc(&b->p, (size_t) n * sizeof(unsigned long long)));
   for(DevBuf *b : {&d_pidx, &d_pidx2, &d_pidx3, &d_leaf_of, &d_lolev, &d_nitem, &d_off})
-    FCK(cudaMalloc(&b->p, (size_t) n * sizeof(int)));
-  FCK(cudaMalloc(&d_lstart.p, nleaves * sizeof(unsigned long long)));
-  FCK(cudaMalloc(&d_llevel.p, nleaves * sizeof(int)));
-  for(DevBuf *b : {&d_loff0, &d_loff1, &d_lfirst, &d_litem, &d_lskip}) FCK(cudaMalloc(&b->p, nleaves * sizeof(int)));
-  FCK(cudaMalloc(&d_flag.p, sizeof(int)));
+    FCK(dmalloc(&b->p, (size_t) n * sizeof(int)));
+  FCK(dmalloc(&d_lstart.p, nleaves * sizeof(unsigned long long)));
+  FCK(dmalloc(&d_llevel.p, nleaves * sizeof(int)));
+  for(DevBuf *b : {&d_loff0, &d_loff1, &d_lfirst, &d_litem, &d_lskip}) FCK(dmalloc(&b->p, nleaves * sizeof(int)));
+  FCK(dmalloc(&d_flag.p, sizeof(int)));
   FCK(cudaMemset(d_flag.p, 0, sizeof(int)));
   FCK(cudaMemset(d_loff0.p, 0, nleaves * sizeof(int)));
   FCK(cudaMemset(d_loff1.p, 0, nleaves * sizeof(int)));
@@ -875,7 +893,7 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     FCK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_hi2.as<unsigned long long>(), d_hi.as<unsigned long long>(),
                                         d_pidx2.as<int>(), d_pidx3.as<int>(), n, 0, 3 * kBits));
     FCK(cub::DeviceScan::ExclusiveSum(nullptr, b3, d_nitem.as<int>(), d_off.as<int>(), n));
-    FCK(cudaMalloc(&d_tmp2.p, std::max(b1, std::max(b2, b3))));
+    FCK(dmalloc(&d_tmp2.p, std::max(b1, std::max(b2, b3))));
     size_t bb = b1;
     FCK(cub::DeviceRadixSort::SortPairs(d_tmp2.p, bb, d_lo.as<unsigned long long>(), d_lo2.as<unsigned long long>(),
                                         d_pidx.as<int>(), d_pidx2.as<int>(), n, 0, 3 * (kTreeLevels - kBits)));
@@ -921,9 +939,9 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
     at.push_back(c.item);
   }
   DevBuf d_items, d_top, d_at;
-  FCK(cudaMalloc(&d_items.p, (size_t) nitems * sizeof(FillItem)));
-  FCK(cudaMalloc(&d_top.p, top_items.size() * sizeof(FillItem)));
-  FCK(cudaMalloc(&d_at.p, at.size() * sizeof(int)));
+  FCK(dmalloc(&d_items.p, (size_t) nitems * sizeof(FillItem)));
+  FCK(dmalloc(&d_top.p, top_items.size() * sizeof(FillItem)));
+  FCK(dmalloc(&d_at.p, at.size() * sizeof(int)));
   FCK(cudaMemcpy(d_top.p, top_items.data(), top_items.size() * sizeof(FillItem), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_at.p, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice));
   FCK(cudaMemcpy(d_litem.p, litem.data(), nleaves * sizeof(int), cudaMemcpyHostToDevice));
@@ -940,24 +958,24 @@ extern "C" int galic_force_grid_fill(const galic_fill_params_t *fp, int n, const
 
   // probes in key order (SoA) and the key-order rank of each probe
   DevBuf d_probes, d_res, d_rank, d_out, d_counts, d_flag2, d_before;
-  FCK(cudaMalloc(&d_probes.p, 3 * (size_t) np * sizeof(double)));
-  FCK(cudaMalloc(&d_res.p, 4 * (size_t) np * sizeof(double)));
-  FCK(cudaMalloc(&d_rank.p, (size_t) np * sizeof(int)));
-  FCK(cudaMalloc(&d_out.p, 3 * (size_t) NN * sizeof(double)));
-  FCK(cudaMalloc(&d_flag2.p, (size_t) ntot * sizeof(int)));
-  FCK(cudaMalloc(&d_before.p, (size_t) ntot * sizeof(int)));
+  FCK(dmalloc(&d_probes.p, 3 * (size_t) np * sizeof(double)));
+  FCK(dmalloc(&d_res.p, 4 * (size_t) np * sizeof(double)));
+  FCK(dmalloc(&d_rank.p, (size_t) np * sizeof(int)));
+  FCK(dmalloc(&d_out.p, 3 * (size_t) NN * sizeof(double)));
+  FCK(dmalloc(&d_flag2.p, (size_t) ntot * sizeof(int)));
+  FCK(dmalloc(&d_before.p, (size_t) ntot * sizeof(int)));
   k_is_probe<<<(ntot + 255) / 256, 256>>>(ntot, n, d_idx2.as<int>(), d_flag2.as<int>());
   {
     size_t b = 0;
     FCK(cub::DeviceScan::ExclusiveSum(nullptr, b, d_flag2.as<int>(), d_before.as<int>(), ntot));
     DevBuf d_t3;
-    FCK(cudaMalloc(&d_t3.p, b));
+    FCK(dmalloc(&d_t3.p, b));
     FCK(cub::DeviceScan::ExclusiveSum(d_t3.p, b, d_flag2.as<int>(), d_before.as<int>(), ntot));
   }
   k_probe_order<<<(ntot + 255) / 256, 256>>>(ntot, n, np, d_idx2.as<int>(), d_before.as<int>(), d_pos.as<double>(),
                                              d_probes.as<double>(), d_rank.as<int>());
   FCK(cudaGetLastError());
-  FCK(cudaMalloc(&d_counts.p, 2 * sizeof(unsigned long long)));
+  FCK(dmalloc(&d_counts.p, 2 * sizeof(unsigned long long)));
   FCK(cudaMemset(d_counts.p, 0, 2 * sizeof(unsigned long long)));
 
   cudaEvent_t e0, e1;
