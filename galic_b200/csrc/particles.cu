@@ -46,8 +46,50 @@ namespace {
 
 constexpr int LOOP_CAP = 1000000;     // tries of every rejection loop
 constexpr uint32_t LEN_CAPPED = 0xffffffffu;
+constexpr uint32_t LEN_DEFER = 0xfffffffeu;  // a halo velocity loop passed VEL_SHORT pairs unresolved
+constexpr int VEL_SHORT = 2048;               // pairs a warp tests before it defers the loop
+constexpr int MAX_TAKE = 4;                   // segments a walk takes over before it waits for a window
+constexpr int WIN_SEGS = 32;                  // segments' worth of positions in a long walk's window
+constexpr int WIN_SLOTS = 64;                 // windows evaluated together
 constexpr int PROBE = 1 << 16;        // positions of the draws-per-particle estimate
 constexpr int PBLOCK = 128;
+
+// Long halo velocity loops.  A loop that has not accepted a pair after
+// VEL_SHORT pairs is deferred: its start position and radius go to the
+// request list and the lane's particle returns LEN_DEFER.  Between launches
+// k_long_search tests the loop's further pairs with the whole GPU and
+// k_long_insert records the first accepted pair in an open-addressing table
+// keyed by the loop's start position; the deferring kernel then resumes its
+// suspended lanes, which find the loop in the table.
+constexpr unsigned long long LT_EMPTY = ~0ull;
+constexpr long long LT_CAPPED = -1;  // no pair accepted within LOOP_CAP pairs
+
+struct LongTab {
+  unsigned long long *key;  // mask + 1 entries, LT_EMPTY when free
+  long long *acc;           // accepted pair, counted from the loop's first draw pair
+  unsigned long long mask;
+  unsigned long long *rq_key;  // requests of the current launch
+  double *rq_r;
+  int *rq_n;  // [0] requests, [1] overflow
+  int rq_cap;
+};
+
+__device__ __forceinline__ unsigned long long lt_slot(unsigned long long key, unsigned long long mask)
+{
+  return (key * 0x9E3779B97F4A7C15ull >> 17) & mask;
+}
+
+// accepted pair of the loop starting at `key`; -2 when it is not in the table
+__device__ long long lt_find(const LongTab &T, unsigned long long key)
+{
+  unsigned long long i = lt_slot(key, T.mask);
+  for(unsigned long long probe = 0; probe <= T.mask; probe++, i = (i + 1) & T.mask) {
+    const unsigned long long k = T.key[i];
+    if(k == key) return T.acc[i];
+    if(k == LT_EMPTY) return -2;
+  }
+  return -2;
+}
 
 struct PInit {
   DevModel M;
@@ -56,11 +98,12 @@ struct PInit {
   uint64_t seed;
   uint32_t sa, sb;
   double MaxVel, LowerDispLimit, TorbitFac;
+  LongTab T;
 };
 
 struct POut {
   double *pos, *vel, *vel_theo, *vesc, *tint, *targets;
-  int *counts;  // [4][4] raised to LowerDispLimit, then [16] non-positive Tint
+  int *counts;  // [4][4] raised to LowerDispLimit, [16] non-positive Tint, [17] deferred in k_final
 };
 
 // halo_get_potential_from_radius (halo.c:69-73)
@@ -112,55 +155,91 @@ __device__ bool fresh_seq(const Shape &S, grng_t &g, double *pos)
 // halo_generate_v tests draw pairs (w, w+1), (w+2, w+3), ... until the first
 // accepted one, and set_particles.c repeats that while the speed is not below
 // MaxVelInUnitsVesc Vesc.  Near the centre the acceptance is small and the
-// number of pairs has a long tail; here the 32 lanes test 32 consecutive
-// pairs of one particle at once and a ballot picks the first accepted pair,
-// which is the sequential loop's result.  Every lane of the warp calls it;
-// need: this lane has a draw to make.  Returns false when capped.
-__device__ bool halo_velocity_warp(const PInit &P, bool need, double r, double vesc, uint64_t &w, double &vr_out)
+// number of pairs has a long tail (up to 10^5 pairs and more); here the 32
+// lanes test 32 consecutive pairs of one particle at once and a ballot picks
+// the first accepted pair, which is the sequential loop's result.  A loop
+// still open after its first 32 pairs is looked up in the long-loop table;
+// one still open after VEL_SHORT pairs is deferred (see LongTab).  Every lane
+// of the warp calls it; need: this lane has a draw to make.  Returns 0, or
+// LEN_CAPPED / LEN_DEFER for this lane.
+__device__ __forceinline__ bool halo_pair(const PInit &P, double rL, double v_max, double f_max, uint64_t j,
+                                          double &v_guess)
+{
+  v_guess = grng_uniform_at(P.seed, P.sa, P.sb, j) * v_max;
+  const double x_aux = grng_uniform_at(P.seed, P.sa, P.sb, j + 1) * f_max;
+  return !(x_aux > v_guess * v_guess * halo_f(P.M, rL, v_guess));
+}
+
+__device__ uint32_t halo_velocity_warp(const PInit &P, bool need, double r, double vesc, uint64_t &w,
+                                       double &vr_out)
 {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const DevModel &M = P.M;
-  bool ok = true;
+  uint32_t res = 0;
   unsigned pending = __ballot_sync(FULL, need);
   while(pending) {
     const int L = __ffs(pending) - 1;
     const double rL = __shfl_sync(FULL, r, L), vescL = __shfl_sync(FULL, vesc, L);
     uint64_t wpos = __shfl_sync(FULL, (unsigned long long) w, L);
     double vr = 0;
-    bool capped = false;
-    long long tries = 0;  // pairs tested for this particle, over all of its draws
+    uint32_t st = 0;
+    int redraws = 0;
     do {
+      if(++redraws > LOOP_CAP) {  // speeds at or above MaxVelInUnitsVesc Vesc without end
+        st = LEN_CAPPED;
+        break;
+      }
       const double pot = halo_pot_r(M, rL);
       const double v_max = sqrt(-2 * pot);
       const double f_max = v_max * v_max * halo_f(M, rL, 0);
-      for(long long base = 0;; base += 32) {
-        const uint64_t j = wpos + 2 * (uint64_t) (base + lane);
-        const double v_guess = grng_uniform_at(P.seed, P.sa, P.sb, j) * v_max;
-        const double x_aux = grng_uniform_at(P.seed, P.sa, P.sb, j + 1) * f_max;
-        const bool accept = !(x_aux > v_guess * v_guess * halo_f(M, rL, v_guess));
-        const unsigned mask = __ballot_sync(FULL, accept);
+      long long n = -2;
+      for(long long base = 0; base < VEL_SHORT; base += 32) {
+        double vg;
+        const unsigned mask = __ballot_sync(FULL, halo_pair(P, rL, v_max, f_max, wpos + 2 * (uint64_t) (base + lane), vg));
         if(mask) {
           const int first = __ffs(mask) - 1;
-          vr = __shfl_sync(FULL, v_guess, first);
-          wpos += 2 * (uint64_t) (base + first + 1);
+          vr = __shfl_sync(FULL, vg, first);
+          n = base + first;
           break;
         }
-        tries += 32;
-        if(tries >= LOOP_CAP) {
-          capped = true;
-          break;
+        if(base == 0) {  // a long loop: resolved already?
+          const long long t = lt_find(P.T, wpos);
+          if(t == LT_CAPPED) {
+            st = LEN_CAPPED;
+            break;
+          }
+          if(t >= 0) {
+            n = t;
+            vr = grng_uniform_at(P.seed, P.sa, P.sb, wpos + 2 * (uint64_t) t) * v_max;
+            break;
+          }
         }
       }
-    } while(!capped && vr >= P.MaxVel * vescL);
+      if(st) break;
+      if(n < 0) {  // still open after VEL_SHORT pairs
+        if(lane == 0) {
+          const int i = atomicAdd(&P.T.rq_n[0], 1);
+          if(i < P.T.rq_cap) {
+            P.T.rq_key[i] = wpos;
+            P.T.rq_r[i] = rL;
+          } else {
+            P.T.rq_n[1] = 1;
+          }
+        }
+        st = LEN_DEFER;
+        break;
+      }
+      wpos += 2 * (uint64_t) (n + 1);
+    } while(vr >= P.MaxVel * vescL);
     if(lane == L) {
       w = wpos;
       vr_out = vr;
-      ok = !capped;
+      res = st;
     }
     pending &= pending - 1;
   }
-  return ok;
+  return res;
 }
 
 // one iteration of initialize_particles' loop (set_particles.c:64-237) for a
@@ -198,11 +277,9 @@ __device__ uint32_t init_one(const PInit &P, uint64_t start, bool active, const 
   if constexpr(TYPE == 1) {
     uint64_t w = grng_position(&g);
     double vr = 0;
-    const bool vok = halo_velocity_warp(P, ok, r, vesc, w, vr);
-    if(ok) {
-      ok = vok;
-      grng_seek(&g, w);
-    }
+    const uint32_t vst = halo_velocity_warp(P, ok, r, vesc, w, vr);
+    if(ok && vst) return vst;
+    if(ok) grng_seek(&g, w);
     if(ok) {
       const double phi = grng_uniform(&g) * kPi * 2;
       const double theta = gm_acos(grng_uniform(&g) * 2 - 1);
@@ -296,6 +373,10 @@ __global__ void __launch_bounds__(PBLOCK) k_len(const PInit P, uint64_t base, ui
     next[o] = o;
     return;
   }
+  if(len == LEN_DEFER) {  // not counted in the estimate
+    next[o] = o;
+    return;
+  }
   const uint64_t e = (uint64_t) o + len;
   next[o] = (len == LEN_CAPPED) ? R + 1 : (e < R ? (uint32_t) e : R);
 }
@@ -314,6 +395,22 @@ struct Segs {
   uint32_t K, W;   // segments; bitmap words per segment (Lseg / 32)
   uint32_t *bits;  // K * W
   uint64_t *x, *cx;
+  // a lane whose particle deferred a long loop: where it stopped (segment,
+  // position of the particle), resumed by the next launch with resume = true
+  uint8_t *susp;  // 1: a long loop deferred, 2: a long walk stopped
+  uint32_t *rs_d;
+  uint64_t *rs_q;
+};
+
+// Windows of particle lengths ahead of the stopped long walks: walk k (lane
+// lane_of_slot) gets positions [lo[k], lo[k] + n) of the type's draws,
+// evaluated by the whole GPU (k_win_len); LEN_DEFER where a long loop is
+// still open, and then the walk evaluates the particle itself
+struct Win {
+  const uint32_t *len;  // [slots][n]
+  const uint64_t *lo;   // [slots]
+  const int *slot;      // [K]: the lane's window, -1 for none
+  uint32_t n;
 };
 
 // clears positions [lo, hi) of the segment that starts at a (a multiple of 32)
@@ -334,19 +431,31 @@ __device__ __forceinline__ bool bit_at(const uint32_t *w, uint64_t a, uint64_t q
 }
 
 // every segment decoded from its own first position (whole warps run
-// init_one together: lanes past K only keep the others company)
+// init_one together: lanes past K only keep the others company); with
+// resume, only the suspended segments, from where they stopped
 template <int TYPE, int VS>
-__global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, uint64_t base, const Segs S, uint64_t *exit)
+__global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, uint64_t base, const Segs S, uint64_t *exit,
+                                                       bool resume)
 {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = c < S.K;
+  const bool valid = c < S.K && (!resume || S.susp[c]);
   const uint64_t a = (uint64_t) c * S.Lseg, end = a + S.Lseg;
   uint32_t *w = S.bits + (size_t) (valid ? c : 0) * S.W;
   uint64_t q = a;
-  bool work = valid;
+  if(valid && resume) {
+    S.susp[c] = 0;
+    q = S.rs_q[c];
+  }
+  bool work = valid, done = valid;
   while(__any_sync(0xffffffffu, work)) {
     const uint32_t len = init_one<TYPE, VS>(P, base + (work ? q : 0), work, nullptr, 0);
     if(work) {
+      if(len == LEN_DEFER) {
+        S.susp[c] = 1;
+        S.rs_q[c] = q;
+        work = done = false;
+        continue;
+      }
       w[(q - a) >> 5] |= 1u << (q & 31);
       if(len == LEN_CAPPED || len == 0) {
         q = POS_CAPPED;
@@ -357,7 +466,7 @@ __global__ void __launch_bounds__(PBLOCK) k_seg_decode(const PInit P, uint64_t b
       }
     }
   }
-  if(valid) {
+  if(done) {
     S.x[c] = a;
     S.cx[c] = q;
     exit[c] = q;
@@ -388,19 +497,33 @@ __global__ void k_seg_prep(const Segs S, const uint64_t *pmax, const uint64_t *e
 // bits.  A walk that leaves with a new exit goes on into the next segment
 // when that one is not flagged (so no two lanes touch one segment), as the
 // next round would.  After round r segments 0 .. r are exact; the rounds end
-// when no exit changes.
+// when no exit changes.  With resume, only the suspended walks go on, in the
+// same round, from the segment and position where they stopped.
+// resume: 0 a new round; 1 the walks that deferred a long loop; 2 the
+// stopped long walks, each through its window in W.  A walk that has taken
+// over max_take segments outside a window stops and waits for one.
 template <int TYPE, int VS>
 __global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, uint64_t base, const Segs S,
                                                     const uint64_t *pmax, const uint8_t *flag,
-                                                    const uint64_t *exit_in, uint64_t *exit_out, int *changed)
+                                                    const uint64_t *exit_in, uint64_t *exit_out, int *changed,
+                                                    int resume, int max_take, Win W)
 {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  bool work = c < S.K && flag[c];
+  const int sl = (resume == 2 && c < S.K) ? W.slot[c] : -1;
+  bool work = c < S.K && (resume == 0 ? flag[c] != 0 : (resume == 1 ? S.susp[c] == 1 : sl >= 0));
+  const uint64_t wlo = sl >= 0 ? W.lo[sl] : 0;
   uint32_t d = c;
+  uint64_t q = 0;
+  int taken = 0;
+  if(work && resume) {
+    S.susp[c] = 0;
+    d = S.rs_d[c];
+    q = S.rs_q[c];
+  }
   uint64_t a = (uint64_t) d * S.Lseg, end = a + S.Lseg;
   uint32_t *w = S.bits + (size_t) (work ? d : 0) * S.W;
-  uint64_t q = work ? pmax[c - 1] : 0;  // flag[0] is never set
-  if(work) {
+  if(work && !resume) {
+    q = pmax[c - 1];  // flag[0] is never set
     S.x[d] = q;
     clear_bits(w, a, a, q < end ? q : end);
   }
@@ -423,14 +546,39 @@ __global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, uint64_t base
             S.x[d] = q;
             clear_bits(w, a, a, q < end ? q : end);
             work = true;
+            if(resume != 2 && ++taken > max_take) {  // a long walk: on with a window
+              S.susp[c] = 2;
+              S.rs_d[c] = d;
+              S.rs_q[c] = q;
+              work = false;
+            }
           }
         }
       } else {
         step = true;
       }
     }
-    const uint32_t len = init_one<TYPE, VS>(P, base + (step ? q : 0), step, nullptr, 0);
+    uint32_t len = LEN_DEFER;
+    const bool in_win = step && sl >= 0 && q >= wlo && q - wlo < W.n;
+    if(in_win) len = W.len[(size_t) sl * W.n + (q - wlo)];
+    const bool eval = step && len == LEN_DEFER;
+    const uint32_t len1 = init_one<TYPE, VS>(P, base + (eval ? q : 0), eval, nullptr, 0);
+    if(eval) len = len1;
     if(step) {
+      if(resume == 2 && !in_win) {  // past the window: another one
+        S.susp[c] = 2;
+        S.rs_d[c] = d;
+        S.rs_q[c] = q;
+        work = false;
+        continue;
+      }
+      if(len == LEN_DEFER) {
+        S.susp[c] = 1;
+        S.rs_d[c] = d;
+        S.rs_q[c] = q;
+        work = false;
+        continue;
+      }
       w[(q - a) >> 5] |= 1u << (q & 31);
       if(len == LEN_CAPPED || len == 0) {
         clear_bits(w, a, q + 1, end);
@@ -445,6 +593,66 @@ __global__ void __launch_bounds__(PBLOCK) k_seg_fix(const PInit P, uint64_t base
       }
     }
   }
+}
+
+// lengths of the particles starting at the windows' positions
+template <int TYPE, int VS>
+__global__ void __launch_bounds__(PBLOCK) k_win_len(const PInit P, uint64_t base, const uint64_t *lo, uint32_t n,
+                                                    uint32_t slots, uint32_t *len)
+{
+  const uint64_t o = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = o < (uint64_t) n * slots;
+  const uint64_t at = active ? lo[o / n] + o % n : 0;
+  const uint32_t l = init_one<TYPE, VS>(P, base + at, active, nullptr, 0);
+  if(active) len[o] = l;
+}
+
+// Long-loop search: pairs [lo, lo + len) of request i (blockIdx.y), each
+// thread a run of consecutive pairs; found[i] = the first accepted pair
+__global__ void __launch_bounds__(256) k_long_search(const PInit P, const unsigned long long *key, const double *r,
+                                                     long long lo, long long len, unsigned long long *found)
+{
+  const int i = blockIdx.y;
+  if(found[i] != LT_EMPTY) return;
+  constexpr int RUN = 8;
+  const long long first = lo + ((long long) blockIdx.x * blockDim.x + threadIdx.x) * RUN;
+  if(first >= lo + len) return;
+  const double rL = r[i];
+  const double v_max = sqrt(-2 * halo_pot_r(P.M, rL));
+  const double f_max = v_max * v_max * halo_f(P.M, rL, 0);
+  for(int k = 0; k < RUN; k++) {
+    double vg;
+    if(halo_pair(P, rL, v_max, f_max, key[i] + 2 * (uint64_t) (first + k), vg)) {
+      atomicMin(&found[i], (unsigned long long) (first + k));
+      return;
+    }
+  }
+}
+
+// requests still open after a search step
+__global__ void k_long_open(const unsigned long long *found, int n, int *open)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i < n && found[i] == LT_EMPTY) atomicAdd(open, 1);
+}
+
+// results into the table (requests for one loop may repeat); open ones
+// after LOOP_CAP pairs are capped
+__global__ void k_long_insert(LongTab T, const unsigned long long *found, int n, int *full)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  const unsigned long long key = T.rq_key[i];
+  const long long v = found[i] == LT_EMPTY ? LT_CAPPED : (long long) found[i];
+  unsigned long long s = lt_slot(key, T.mask);
+  for(unsigned long long probe = 0; probe <= T.mask; probe++, s = (s + 1) & T.mask) {
+    const unsigned long long prev = atomicCAS(&T.key[s], LT_EMPTY, key);
+    if(prev == LT_EMPTY || prev == key) {
+      T.acc[s] = v;  // the same value for every request of this key
+      return;
+    }
+  }
+  atomicAdd(full, 1);
 }
 
 // the first segment whose chain caps (every later one is cut off)
@@ -495,7 +703,8 @@ __global__ void __launch_bounds__(PBLOCK) k_final(const PInit P, uint64_t base, 
   const long long rank = (long long) (j & 31) * warps + (j >> 5);
   const bool active = j < warps * 32 && rank < count;
   const int i = active ? ord[rank] : 0;
-  init_one<TYPE, VS>(P, base + (active ? starts[i] : 0), active, &o, n0 + i);
+  const uint32_t len = init_one<TYPE, VS>(P, base + (active ? starts[i] : 0), active, &o, n0 + i);
+  if(active && len == LEN_DEFER) atomicAdd(&o.counts[17], 1);  // its values were not written
 }
 
 // particle lengths as sort keys (clamped to 32 bits) and their indices
@@ -555,6 +764,51 @@ void with_kind(int type, int vs, F &&f)
     vs ? f(I3{}, I1{}) : f(I3{}, V0{});
 }
 
+// Resolves the long loops requested since the last call: k_long_search over
+// growing runs of pairs (4096, then x4) until every request has its first
+// accepted pair or LOOP_CAP pairs were tested, then k_long_insert.  *n: the
+// requests there were.  d_aux: 2 ints of scratch.
+int resolve_long(const PInit &P, cudaStream_t s, unsigned long long *d_found, int *d_aux, int *n, int &launches)
+{
+  int h[2] = {0, 0};
+  if(cudaMemcpyAsync(h, P.T.rq_n, 2 * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+     cudaStreamSynchronize(s) != cudaSuccess)
+    return GALIC_ERR_CUDA;
+  *n = h[0];
+  if(h[1]) return GALIC_ERR_UNSUPPORTED;  // more requests than lanes: not reachable
+  if(h[0] == 0) return GALIC_OK;
+  const int nreq = h[0];
+  if(cudaMemsetAsync(d_found, 0xff, (size_t) nreq * sizeof(unsigned long long), s) != cudaSuccess)
+    return GALIC_ERR_CUDA;
+  for(long long lo = VEL_SHORT, len = 4096; lo < LOOP_CAP; lo += len, len *= 4) {
+    if(lo + len > LOOP_CAP) len = LOOP_CAP - lo;
+    const unsigned bx = (unsigned) ((len + 256 * 8 - 1) / (256 * 8));
+    for(int r0 = 0; r0 < nreq; r0 += 65535) {
+      const unsigned nr = (unsigned) std::min(65535, nreq - r0);
+      k_long_search<<<dim3(bx, nr), 256, 0, s>>>(P, P.T.rq_key + r0, P.T.rq_r + r0, lo, len, d_found + r0);
+      launches++;
+    }
+    int open = 0;
+    if(cudaMemsetAsync(d_aux, 0, sizeof(int), s) != cudaSuccess) return GALIC_ERR_CUDA;
+    k_long_open<<<gblocks(nreq, 256), 256, 0, s>>>(d_found, nreq, d_aux);
+    launches++;
+    if(cudaGetLastError() != cudaSuccess ||
+       cudaMemcpyAsync(&open, d_aux, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+       cudaStreamSynchronize(s) != cudaSuccess)
+      return GALIC_ERR_CUDA;
+    if(open == 0) break;
+  }
+  int full = 0;
+  if(cudaMemsetAsync(d_aux + 1, 0, sizeof(int), s) != cudaSuccess) return GALIC_ERR_CUDA;
+  k_long_insert<<<gblocks(nreq, 256), 256, 0, s>>>(P.T, d_found, nreq, d_aux + 1);
+  launches++;
+  if(cudaGetLastError() != cudaSuccess ||
+     cudaMemcpyAsync(&full, d_aux + 1, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+     cudaMemsetAsync(P.T.rq_n, 0, 2 * sizeof(int), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+    return GALIC_ERR_CUDA;
+  return full ? GALIC_ERR_UNSUPPORTED : GALIC_OK;  // the table is sized far above the loops there can be
+}
+
 }  // namespace
 
 extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_params_t *sp, double TorbitFac,
@@ -581,9 +835,17 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
   uint64_t *d_starts = nullptr;  // inside d_seg
   char *d_seg = nullptr;
   unsigned long long *d_keys = nullptr, *d_keys2 = nullptr;
-  void *d_tmp = nullptr;
+  void *d_tmp = nullptr, *d_long = nullptr;
+  unsigned long long *d_found = nullptr;
+  int *d_aux = nullptr;
+  uint32_t *d_wlen = nullptr;
+  uint64_t *d_wlo = nullptr;  // inside d_long
+  int *d_wslot = nullptr;  // inside d_seg
+  size_t win_cap = 0;
+  std::vector<uint64_t> h_rsq;
   size_t J_cap = 0, seg_cap = 0;
-  std::vector<int> h_counts(17);
+  std::vector<int> h_counts(18);
+  std::vector<uint8_t> h_susp;
   uint64_t pos = stream->position;
   PInit P{};
   POut O{};
@@ -617,9 +879,9 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     D.FG_Nbin = p.FG_Nbin;
   }
   PCK(cudaMallocAsync((void **) &d_f, (size_t) 15 * N * sizeof(double), s));
-  PCK(cudaMallocAsync((void **) &d_counts, 17 * sizeof(int), s));
+  PCK(cudaMallocAsync((void **) &d_counts, 18 * sizeof(int), s));
   PCK(cudaMemsetAsync(d_f, 0, (size_t) 15 * N * sizeof(double), s));
-  PCK(cudaMemsetAsync(d_counts, 0, 17 * sizeof(int), s));
+  PCK(cudaMemsetAsync(d_counts, 0, 18 * sizeof(int), s));
   O.pos = d_f;
   O.vel = d_f + 3 * (size_t) N;
   O.vel_theo = d_f + 6 * (size_t) N;
@@ -627,6 +889,28 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
   O.tint = d_f + 10 * (size_t) N;
   O.targets = d_f + 11 * (size_t) N;
   O.counts = d_counts;
+  {
+    // long-loop table (about one loop in 2 000 passes VEL_SHORT pairs) and
+    // the request list (at most one request per lane and launch)
+    unsigned long long cap = 8192;
+    while(cap < (unsigned long long) N / 16) cap <<= 1;
+    const int rq_cap = std::max(N, PROBE) + 64;
+    const size_t bytes = cap * 16 + (size_t) rq_cap * 24 + 64 + WIN_SLOTS * sizeof(uint64_t);
+    PCK(cudaMallocAsync(&d_long, bytes, s));
+    char *c = (char *) d_long;
+    P.T.key = (unsigned long long *) c;
+    P.T.acc = (long long *) (c + cap * 8);
+    P.T.mask = cap - 1;
+    P.T.rq_key = (unsigned long long *) (c + cap * 16);
+    P.T.rq_r = (double *) (c + cap * 16 + (size_t) rq_cap * 8);
+    d_found = (unsigned long long *) (c + cap * 16 + (size_t) rq_cap * 16);
+    P.T.rq_n = (int *) (c + cap * 16 + (size_t) rq_cap * 24);
+    d_aux = P.T.rq_n + 4;
+    d_wlo = (uint64_t *) (c + cap * 16 + (size_t) rq_cap * 24 + 64);
+    P.T.rq_cap = rq_cap;
+    PCK(cudaMemsetAsync(P.T.key, 0xff, cap * 8, s));
+    PCK(cudaMemsetAsync(P.T.rq_n, 0, 64, s));
+  }
   {
     int n0 = 0;
     for(int t = 1; t <= 3 && rc == GALIC_OK; n0 += nt[t], t++) {
@@ -640,11 +924,20 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         J_cap = (size_t) R + 2;
         PCK(cudaMallocAsync((void **) &d_J, J_cap * sizeof(uint32_t), s));
       }
-      with_kind(t, vs, [&](auto T, auto V) {
-        k_len<decltype(T)::value, decltype(V)::value><<<gblocks(R + 2, PBLOCK), PBLOCK, 0, s>>>(P, pos, R, d_J);
-      });
-      launches++;
-      PCK(cudaGetLastError());
+      // the long loops met are resolved and the probe repeated, so that the
+      // estimate holds them (the few long ones weigh much in the mean)
+      for(int rep = 0;; rep++) {
+        with_kind(t, vs, [&](auto T, auto V) {
+          k_len<decltype(T)::value, decltype(V)::value><<<gblocks(R + 2, PBLOCK), PBLOCK, 0, s>>>(P, pos, R, d_J);
+        });
+        launches++;
+        PCK(cudaGetLastError());
+        int nreq = 0;
+        rc = resolve_long(P, s, d_found, d_aux, &nreq, launches);
+        if(rc != GALIC_OK || nreq == 0 || rep >= 8) break;
+      }
+      if(rc != GALIC_OK) break;
+      PCK(cudaMemsetAsync(P.T.rq_n, 0, 2 * sizeof(int), s));
       PCK(cudaMemcpyAsync(probe.data(), d_J, (R + 2) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       PCK(cudaStreamSynchronize(s));
       double sum = 0;
@@ -686,7 +979,10 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         const size_t sz_bits = al(K * G.W * sizeof(uint32_t)), sz_k = al(K * sizeof(uint64_t)),
                      sz_k1 = al((K + 1) * sizeof(uint64_t)), sz_st = al(((size_t) nt[t] + 1) * sizeof(uint64_t)),
                      sz_n = al((size_t) nt[t] * sizeof(uint32_t));
-        const size_t need = sz_bits + 5 * sz_k + al(K) + 2 * sz_k1 + 256 + al(tb) + sz_st + 4 * sz_n;
+        // bits, x, cx, exits x 2, pmax, flag, cnt, off, first/changed, scan scratch, starts,
+        // length keys and order, resume positions, segments, suspended flags, window slots
+        const size_t need = sz_bits + 5 * sz_k + al(K) + 2 * sz_k1 + 256 + al(tb) + sz_st + 4 * sz_n + sz_k +
+                            al(K * sizeof(uint32_t)) + al(K) + al(K * sizeof(int));
         if(seg_cap < need) {
           if(d_seg) cudaFreeAsync(d_seg, s);
           d_seg = nullptr;
@@ -714,13 +1010,33 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         cur += sz_st;
         uint32_t *d_lkey = (uint32_t *) cur, *d_lkey2 = (uint32_t *) (cur + sz_n);
         int *d_lidx = (int *) (cur + 2 * sz_n), *d_ord = (int *) (cur + 3 * sz_n);
+        cur += 4 * sz_n;
+        G.rs_q = (uint64_t *) cur;
+        cur += sz_k;
+        G.rs_d = (uint32_t *) cur;
+        cur += al(K * sizeof(uint32_t));
+        G.susp = (uint8_t *) cur;
+        cur += al(K);
+        d_wslot = (int *) cur;
         PCK(cudaMemsetAsync(G.bits, 0, sz_bits, s));
-        with_kind(t, vs, [&](auto T, auto V) {
-          k_seg_decode<decltype(T)::value, decltype(V)::value>
-              <<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, pos, G, ex[0]);
-        });
-        launches++;
-        PCK(cudaGetLastError());
+        PCK(cudaMemsetAsync(G.susp, 0, K, s));
+        PCK(cudaMemsetAsync(d_wslot, 0xff, K * sizeof(int), s));
+        for(int resume = 0;; resume++) {
+          with_kind(t, vs, [&](auto T, auto V) {
+            k_seg_decode<decltype(T)::value, decltype(V)::value>
+                <<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, pos, G, ex[0], resume > 0);
+          });
+          launches++;
+          PCK(cudaGetLastError());
+          int nreq = 0;
+          rc = resolve_long(P, s, d_found, d_aux, &nreq, launches);
+          if(rc != GALIC_OK || nreq == 0) break;
+          if(resume > 100000) {  // each resume passes a resolved loop: cannot happen
+            rc = GALIC_ERR_CUDA;
+            break;
+          }
+        }
+        if(rc != GALIC_OK) break;
         int fin = -1;
         for(size_t r = 1; r <= K + 1; r++) {  // segment r - 1 is exact after round r - 1
           int h_changed = 0;
@@ -730,12 +1046,72 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
           PCK(cub::DeviceScan::InclusiveScan(d_scan, tbr, in, d_pmax, MaxU64(), K, s));
           k_seg_prep<<<gblocks((long long) K, 256), 256, 0, s>>>(G, d_pmax, in, out_, d_flag);
           PCK(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
-          with_kind(t, vs, [&](auto T, auto V) {
-            k_seg_fix<decltype(T)::value, decltype(V)::value>
-                <<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(P, pos, G, d_pmax, d_flag, in, out_, d_changed);
-          });
-          launches += 3;
-          PCK(cudaGetLastError());
+          launches += 2;
+          // the round, then the walks that deferred a long loop, then the long
+          // walks, through windows of particle lengths evaluated ahead
+          int mode = 0;
+          Win win{};
+          for(int it = 0;; it++) {
+            if(it > 1000000) {  // every launch passes a resolved loop or a window: cannot happen
+              rc = GALIC_ERR_CUDA;
+              break;
+            }
+            with_kind(t, vs, [&](auto T, auto V) {
+              k_seg_fix<decltype(T)::value, decltype(V)::value><<<gblocks((long long) K, PBLOCK), PBLOCK, 0, s>>>(
+                  P, pos, G, d_pmax, d_flag, in, out_, d_changed, mode, MAX_TAKE, win);
+            });
+            launches++;
+            PCK(cudaGetLastError());
+            if(mode == 2) PCK(cudaMemsetAsync(d_wslot, 0xff, K * sizeof(int), s));
+            int nreq = 0;
+            rc = resolve_long(P, s, d_found, d_aux, &nreq, launches);
+            if(rc != GALIC_OK) break;
+            if(nreq) {
+              mode = 1;
+              win = Win{};
+              continue;
+            }
+            // the stopped long walks, up to WIN_SLOTS at a time
+            h_susp.resize(K);
+            PCK(cudaMemcpyAsync(h_susp.data(), G.susp, K, cudaMemcpyDeviceToHost, s));
+            PCK(cudaStreamSynchronize(s));
+            std::vector<uint32_t> walks;
+            for(uint32_t k = 0; k < (uint32_t) K && walks.size() < (size_t) WIN_SLOTS; k++)
+              if(h_susp[k] == 2) walks.push_back(k);
+            if(walks.empty()) break;
+            const uint32_t wn = (uint32_t) (WIN_SEGS * Lseg), ns = (uint32_t) walks.size();
+            h_rsq.resize(K);
+            PCK(cudaMemcpyAsync(h_rsq.data(), G.rs_q, K * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+            PCK(cudaStreamSynchronize(s));
+            std::vector<uint64_t> wlo(ns);
+            std::vector<int> wslot(K, -1);
+            for(uint32_t k = 0; k < ns; k++) {
+              wlo[k] = h_rsq[walks[k]];
+              wslot[walks[k]] = (int) k;
+            }
+            if(win_cap < (size_t) wn * ns) {
+              if(d_wlen) cudaFreeAsync(d_wlen, s);
+              d_wlen = nullptr;
+              win_cap = (size_t) wn * WIN_SLOTS;
+              PCK(cudaMallocAsync((void **) &d_wlen, win_cap * sizeof(uint32_t), s));
+            }
+            PCK(cudaMemcpyAsync(d_wlo, wlo.data(), ns * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            PCK(cudaMemcpyAsync(d_wslot, wslot.data(), K * sizeof(int), cudaMemcpyHostToDevice, s));
+            // the windows' lengths; the long loops met there are resolved into
+            // the table, and the walks evaluate those particles themselves
+            with_kind(t, vs, [&](auto T, auto V) {
+              k_win_len<decltype(T)::value, decltype(V)::value>
+                  <<<gblocks((long long) wn * ns, PBLOCK), PBLOCK, 0, s>>>(P, pos, d_wlo, wn, ns, d_wlen);
+            });
+            launches++;
+            PCK(cudaGetLastError());
+            int nw = 0;
+            rc = resolve_long(P, s, d_found, d_aux, &nw, launches);
+            if(rc != GALIC_OK) break;
+            mode = 2;
+            win = Win{d_wlen, d_wlo, d_wslot, wn};
+          }
+          if(rc != GALIC_OK) break;
           PCK(cudaMemcpyAsync(&h_changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, s));
           PCK(cudaStreamSynchronize(s));
           if(!h_changed) {
@@ -743,6 +1119,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
             break;
           }
         }
+        if(rc != GALIC_OK) break;
         if(fin < 0) {  // cannot happen: round r fixes segment r for good
           rc = GALIC_ERR_CUDA;
           break;
@@ -787,12 +1164,15 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     }
   }
   if(rc != GALIC_OK) goto done;
-  PCK(cudaMemcpyAsync(h_counts.data(), d_counts, 17 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  PCK(cudaMemcpyAsync(h_counts.data(), d_counts, 18 * sizeof(int), cudaMemcpyDeviceToHost, s));
   PCK(cudaStreamSynchronize(s));
   for(int t = 1; t <= 3; t++)
     for(int k = 0; k < 4; k++)
       if(nt[t] > 0 && (double) h_counts[4 * t + k] / nt[t] > 0.05) rc = GALIC_ERR_UNSUPPORTED;
   if(rc == GALIC_OK && h_counts[16]) rc = GALIC_ERR_INVALID_ARGUMENT;  // galic_set_particles' tint check
+  // every particle of the chain had each of its long loops resolved while the
+  // chain was decoded, so k_final finds them all in the table
+  if(rc == GALIC_OK && h_counts[17]) rc = GALIC_ERR_CUDA;
   if(rc == GALIC_OK) {
     // the permutation (set_particles.c:298-303)
     size_t tb = 0;
@@ -833,7 +1213,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
     if(rc == GALIC_OK) pos += (uint64_t) N;
   }
 done:
-  for(void *q : {(void *) d_f, (void *) d_counts, (void *) d_vals, (void *) d_vals2, (void *) d_J, (void *) d_seg,
+  for(void *q : {(void *) d_f, (void *) d_counts, (void *) d_vals, (void *) d_vals2, (void *) d_J, (void *) d_seg, d_long, (void *) d_wlen,
                  (void *) d_keys, (void *) d_keys2, d_tmp})
     if(q) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
