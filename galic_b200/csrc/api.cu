@@ -462,6 +462,10 @@ extern "C" int galic_set_targets(galic_ctx *ctx, int type, const double *dgs_mas
   return fail(ctx, GALIC_OK);
 }
 
+namespace {
+cudaError_t order_by_type_radius(galic_ctx *ctx);
+}
+
 extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, const double *vel, const double *mass,
                                    const double *tint, const double *vesc, const int *type, const double *targets)
 {
@@ -493,21 +497,11 @@ extern "C" int galic_set_particles(galic_ctx *ctx, int n, const double *pos, con
   CK(cudaMemcpyAsync(ctx->d_ptargets, targets, 4 * (size_t) n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_type, type, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_vdisp, 0, 4 * (size_t) n * sizeof(double), ctx->stream));
-  {
-    // by type, then by radius: neighbouring lanes then integrate orbits of one
-    // type (one velocity structure, no divergent projections) that start at
-    // similar radii and read nearby force-grid cells; results do not depend
-    // on the order
-    std::vector<double> r2(n);
-    std::vector<int> order(n);
-    for(int i = 0; i < n; i++) {
-      r2[i] = pos[3 * i] * pos[3 * i] + pos[3 * i + 1] * pos[3 * i + 1] + pos[3 * i + 2] * pos[3 * i + 2];
-      order[i] = i;
-    }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return type[a] != type[b] ? type[a] < type[b] : r2[a] < r2[b]; });
-    CK(cudaMemcpyAsync(ctx->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-  }
+  // by type, then by radius: neighbouring lanes then integrate orbits of one
+  // type (one velocity structure, no divergent projections) that start at
+  // similar radii and read nearby force-grid cells; results do not depend on
+  // the order.  Sorted on the GPU from the uploaded positions and types.
+  CK(order_by_type_radius(ctx));
   CK(cudaMemsetAsync(ctx->d_orbits, 0, n * sizeof(int), ctx->stream));
   ctx->have_response = false;
   CK(cudaStreamSynchronize(ctx->stream));  // the upload is complete on return
@@ -537,18 +531,17 @@ __global__ void k_radius_keys(int n, const double *pos, unsigned long long *key,
   idx[i] = i;
 }
 
-__global__ void k_type_keys(int n, int n1, int n12, const int *idx, int *key)
+__global__ void k_type_keys(int n, const int *type, const int *idx, int *key)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if(i >= n) return;
-  const int j = idx[i];
-  key[i] = j < n1 ? 1 : (j < n12 ? 2 : 3);
+  key[i] = type[idx[i]];
 }
 
-// the orbit order of galic_set_particles (by type, then by radius, ties in
-// index order) for particles stored type by type: a stable radix sort by
-// r^2, then a stable one by type
-cudaError_t order_by_type_radius(galic_ctx *ctx, const int nt[4])
+// the orbit order (by type, then by radius, ties in index order) of the
+// context's particles into d_order: a stable radix sort by r^2, then a
+// stable one by type (1-3: two bits)
+cudaError_t order_by_type_radius(galic_ctx *ctx)
 {
   const int n = ctx->n;
   cudaStream_t s = ctx->stream;
@@ -574,7 +567,7 @@ cudaError_t order_by_type_radius(galic_ctx *ctx, const int nt[4])
     e = cub::DeviceRadixSort::SortPairs(tmp, tbx, k0, k1, i0, i1, n, 0, 64, s);
   }
   if(e == cudaSuccess) {
-    k_type_keys<<<g, 256, 0, s>>>(n, nt[1], nt[1] + nt[2], i1, t0);
+    k_type_keys<<<g, 256, 0, s>>>(n, ctx->d_type, i1, t0);
     tbx = std::max(tb, tb2);
     e = cub::DeviceRadixSort::SortPairs(tmp, tbx, t0, t1, i1, ctx->d_order, n, 0, 2, s);
   }
@@ -628,7 +621,7 @@ int set_particles_device(galic_ctx *ctx, const int nt[4], const double tmass[4],
                                                                 nt[2] ? tmass[2] / nt[2] : 0.0,
                                                                 nt[3] ? tmass[3] / nt[3] : 0.0, ctx->d_mass, ctx->d_type);
   CK(cudaGetLastError());
-  CK(order_by_type_radius(ctx, nt));
+  CK(order_by_type_radius(ctx));
   ctx->have_response = false;
   CK(cudaStreamSynchronize(s));
   return fail(ctx, GALIC_OK);
