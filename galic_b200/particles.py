@@ -19,10 +19,24 @@ FIELDS = (("pos", 3, np.float64), ("vel", 3, np.float64), ("vel_theo", 3, np.flo
           ("id", 1, np.int32), ("permutation", 1, np.int32))
 
 
+def _host_array(shape, dtype):
+    """Page-locked host memory from torch's caching allocator (the device
+    writes into it at full link speed, and repeated calls reuse the pages);
+    plain memory where torch has no CUDA device."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            t = torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.int32, pin_memory=True)
+            return t.numpy()
+    except ImportError:
+        pass
+    return np.empty(shape, dtype=dtype)
+
+
 def initialize_particles(ctx, sp, torbit_fac, stream):
     """Runs the initialisation; returns ({field: array}, low-dispersion counts [4, 4])."""
     n = sum(int(ctx.params.NType[t]) for t in (1, 2, 3))
-    arrs = {k: np.empty((n, w) if w > 1 else n, dtype=dt) for k, w, dt in FIELDS}  # the call fills every one
+    arrs = {k: _host_array((n, w) if w > 1 else (n,), dt) for k, w, dt in FIELDS}  # the call fills every one
     out = _ffi.GalicParticlesOut()
     for k, _, dt in FIELDS:
         setattr(out, k, _ffi.dptr(arrs[k]) if dt == np.float64 else _ffi.iptr(arrs[k]))
