@@ -281,9 +281,23 @@ struct Sink32 : NodeAcc {
     cur_iR = iR;
     cur_iz = iz;
   }
+  // straight-line form of `if(cell changed) move_to(iR, iz)`: every lane runs
+  // it (a warp nearly always has a lane whose cell changed), so the compiler
+  // can interleave it with the rest of the step; on an unchanged cell no
+  // slot leaves, on the orbit's first deposit every slot is cleared and
+  // nothing is parked
   __device__ __forceinline__ void add(int iR, int iz, float hdt, float fR, float fz, const Proj32 &p)
   {
-    if(iz * Nb + iR != cur) move_to(iR, iz);
+    const bool first = cur < 0;
+    bool out[4];
+    leaving(iR, iz, out);
+#pragma unroll
+    for(int s = 0; s < 4; s++) out[s] = first || out[s];
+    if(!first) park_masked(out);
+    clear(out);
+    cur = iz * Nb + iR;
+    cur_iR = iR;
+    cur_iz = iz;
     accumulate(iR, iz, hdt, fR, fz, p);
   }
 };
