@@ -320,7 +320,6 @@ struct State32 {
   int iR, iz;
   float fR, fz, radsign_prev;
   float pend;    // weight of the deferred end-of-step deposit
-  int cs_cell;   // DG cell whose size is in cs_val (the current cell)
   float cs_val;
   Proj32 proj;
   int norbit, flag, type, tovs, steps, status;
@@ -355,8 +354,7 @@ __device__ __forceinline__ void orbit32_init(const Model32 &M, State32 &s, const
   s.fR = c.fR;
   s.fz = c.fz;
   s.proj = project32(s.tovs, s.x, s.v, vstr);
-  s.cs_cell = s.iz * M.DG_Nbin + s.iR;
-  s.cs_val = __ldg(&M.cellsize[s.cs_cell]);
+  s.cs_val = __ldg(&M.cellsize[s.iz * M.DG_Nbin + s.iR]);
   s.pend = 0.f;
 }
 
@@ -396,15 +394,10 @@ __device__ __forceinline__ bool orbit32_step(const Model32 &M, State32 &s, Sink 
   s.iz = c.iz;
   s.fR = c.fR;
   s.fz = c.fz;
-  {
-    // DG_CellSize of the new cell for the next step's time step, loaded now
-    // so that its latency overlaps the rest of this step
-    const int dgc = s.iz * M.DG_Nbin + s.iR;
-    if(dgc != s.cs_cell) {
-      s.cs_cell = dgc;
-      s.cs_val = __ldg(&M.cellsize[dgc]);
-    }
-  }
+  // DG_CellSize of the new cell for the next step's time step, loaded now
+  // (every step, no branch: an L1 hit) so that its latency overlaps the rest
+  // of this step
+  s.cs_val = __ldg(&M.cellsize[s.iz * M.DG_Nbin + s.iR]);
   s.proj = project32(s.tovs, s.x, s.v, vstr);
   s.pend = hdt;
   s.tall += dt;
