@@ -22,11 +22,16 @@
 //    time keeping its values; then one uniform per particle after the last
 //    draw and a radix sort give the permutation.
 // The halo's velocity rejection loop has a long tail near the centre; its
-// draw pairs are tested 32 at a time by a whole warp (halo_velocity_warp).
-// A chain whose rejection loop hits its cap of 10^6 tries ends there; if
-// that happens before a type's last particle the call fails.  Built with
-// --fmad=false and gmath.h's functions, so every particle is bit-identical
-// to the CPU restatement.
+// draw pairs are tested 32 at a time by a whole warp (halo_velocity_warp),
+// and a loop still open after 2048 pairs is deferred and searched by the
+// whole GPU between launches (LongTab, k_long_search): the kernels resume
+// their suspended lanes, which then find the loop's answer in a table.  A
+// resynchronisation walk that has carried on through 4 segments stops too,
+// and goes on through a window of particle lengths evaluated ahead by the
+// whole GPU (k_win_len).  A chain whose rejection loop hits its cap of 10^6
+// tries ends there; if that happens before a type's last particle the call
+// fails.  Built with --fmad=false and gmath.h's functions, so every particle
+// is bit-identical to the CPU restatement.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
