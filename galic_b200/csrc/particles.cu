@@ -772,15 +772,20 @@ void with_kind(int type, int vs, F &&f)
 // Resolves the long loops requested since the last call: k_long_search over
 // growing runs of pairs (4096, then x4) until every request has its first
 // accepted pair or LOOP_CAP pairs were tested, then k_long_insert.  *n: the
-// requests there were.  d_aux: 2 ints of scratch.
-int resolve_long(const PInit &P, cudaStream_t s, unsigned long long *d_found, int *d_aux, int *n, int &launches)
+// requests there were.  d_aux: 2 ints of scratch.  partial: the launch that
+// made the requests (the probe, the windows) may lose some to a full list --
+// its positions stay deferred and are evaluated again where they matter --
+// so only the recorded ones are resolved; elsewhere a full list is an error.
+int resolve_long(const PInit &P, cudaStream_t s, unsigned long long *d_found, int *d_aux, int *n, int &launches,
+                 bool partial = false)
 {
   int h[2] = {0, 0};
   if(cudaMemcpyAsync(h, P.T.rq_n, 2 * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
      cudaStreamSynchronize(s) != cudaSuccess)
     return GALIC_ERR_CUDA;
+  if(h[1] && !partial) return GALIC_ERR_UNSUPPORTED;  // at most one request per lane: not reachable
+  if(h[0] > P.T.rq_cap) h[0] = P.T.rq_cap;
   *n = h[0];
-  if(h[1]) return GALIC_ERR_UNSUPPORTED;  // more requests than lanes: not reachable
   if(h[0] == 0) return GALIC_OK;
   const int nreq = h[0];
   if(cudaMemsetAsync(d_found, 0xff, (size_t) nreq * sizeof(unsigned long long), s) != cudaSuccess)
@@ -938,7 +943,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
         launches++;
         PCK(cudaGetLastError());
         int nreq = 0;
-        rc = resolve_long(P, s, d_found, d_aux, &nreq, launches);
+        rc = resolve_long(P, s, d_found, d_aux, &nreq, launches, true);
         if(rc != GALIC_OK || nreq == 0 || rep >= 8) break;
       }
       if(rc != GALIC_OK) break;
@@ -1111,7 +1116,7 @@ extern "C" int galic_initialize_particles(galic_ctx *ctx, const galic_sample_par
             launches++;
             PCK(cudaGetLastError());
             int nw = 0;
-            rc = resolve_long(P, s, d_found, d_aux, &nw, launches);
+            rc = resolve_long(P, s, d_found, d_aux, &nw, launches, true);
             if(rc != GALIC_OK) break;
             mode = 2;
             win = Win{d_wlen, d_wlo, d_wslot, wn};
