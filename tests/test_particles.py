@@ -73,6 +73,15 @@ def test_restatement_stops_on_low_dispersion():
     assert st == 6 and counts[1, 0] > 0.05 * m.params.NType[1]
 
 
+def test_result_arrays_shape_and_type():
+    """The wrapper's result arrays: page-locked where torch has a CUDA device,
+    plain memory otherwise; shapes and types as initialize_particles fills them."""
+    from galic_b200 import particles
+    for k, w, dt in particles.FIELDS:
+        a = particles._host_array((5, w) if w > 1 else (5,), dt)
+        assert a.shape == ((5, w) if w > 1 else (5,)) and a.dtype == dt and a.flags["C_CONTIGUOUS"], k
+
+
 def _gpu_particles(m, sp, tf, tables, stream, fit=True):
     from galic_b200 import particles, sampling
     from galic_b200.context import Context
