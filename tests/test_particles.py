@@ -42,7 +42,7 @@ def setup_inputs(m, halo_beta=0.2, bulge_beta=0.0, low=None, maxvel=None):
 
 
 @needs_ref
-@pytest.mark.parametrize("tovs", [(1, 3, 2), (0, 2, 1)])
+@pytest.mark.parametrize("tovs", [(1, 3, 2), (0, 2, 1), (2, 3, 0)])
 def test_restatement_matches_reference(tovs):
     m = particle_model(tovs=tovs)
     sp, _, tables, tf = setup_inputs(m)
@@ -102,7 +102,7 @@ def _gpu_particles(m, sp, tf, tables, stream, fit=True):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("tovs,n", [((1, 3, 2), (400, 200, 100)), ((0, 2, 1), (3000, 1000, 500)),
-                                    ((1, 3, 2), (60000, 20000, 8000))])
+                                    ((2, 3, 0), (3000, 1000, 500)), ((1, 3, 2), (60000, 20000, 8000))])
 def test_gpu_bit_identical(tovs, n):
     m = particle_model(tovs=tovs, n=n)
     sp, _, tables, tf = setup_inputs(m)
