@@ -31,6 +31,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "orbit-steps/s (FP32 batched vs FP64 plain, same χ²); p50/p99 model latency"
 FLOP_PER_STEP = 365  # algorithmic FP ops per orbit-step (orbit_response.c:211-458 and callees)
+# DRAM bytes per orbit of the orbit kernels (ncu, one launch at 0.1 of the
+# workload's particles; the count scales with the orbits: particle state in,
+# orbit counts out, the grids and tables stay in L2)
+KERNEL_DRAM_BYTES_PER_ORBIT = {}
+REF_BUILD = "-O3 -march=native (its Makefile.template flags), one single-rank process per host core"
 WORKLOAD = "halo+disk: Hernquist halo M=95 a=30 N=1e6 + exp disk M=5 h=3.5 z0=0.7 N=2e5, 128x128 DG/EG, 256^2 FG"
 
 
@@ -40,8 +45,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"],
-                    help="form of the headline value; the other form is measured beside it")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"],
+                    help="form of the headline value (default: the FP64 drop-in, the reference's precision); "
+                         "the other form is measured beside it")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's particle count")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ensemble-models", type=int, default=64, help="models of the batched ensemble (0: skip)")
@@ -52,7 +58,7 @@ def parse():
     ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
     ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
     ap.add_argument("--serve-workers", type=int, default=16, help="concurrent jobs of the serving loop")
-    ap.add_argument("--row", default="all", choices=["all", "fill", "sampling", "jeans", "particles"],
+    ap.add_argument("--row", default="all", choices=["all", "calc_all", "fill", "sampling", "jeans", "particles"],
                     help="one secondary measurement alone on this workload (a diagnostic line for profiling, "
                          "not the bench line)")
     return ap.parse_args()
@@ -81,7 +87,10 @@ def _cpu_worker(args):
     from make_golden import model_from_arrays
 
     m = model_from_arrays(arrays)
-    runner = oracle_lib.Reference(m.params) if kind == "reference" else oracle_lib.Oracle(m.params, use_libm=True)
+    # the timed runner is GALIC's C with its own -O3 -march=native flags
+    # (the parity build has contraction off and is slower)
+    runner = (oracle_lib.Reference(m.params, fast=oracle_lib.reference_fast_available()) if kind == "reference"
+              else oracle_lib.Oracle(m.params, use_libm=True))
     runner.load_model(m, particles=False)
     done = []
     t0 = time.perf_counter()
@@ -91,8 +100,9 @@ def _cpu_worker(args):
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
-    # step counts: the restatement with glibc math follows the same trajectory
-    # bit for bit, and returns its step count
+    # step counts: the restatement with glibc math follows the parity build's
+    # trajectory bit for bit and returns its step count (the -O3 build's
+    # contracted arithmetic moves trajectories only in the last bits)
     counter = oracle_lib.Oracle(m.params, use_libm=True)
     counter.load_model(m, particles=False)
     steps = 0
@@ -256,11 +266,12 @@ def measure_sampling(model, ctx, steps, cpu):
 
 def jeans_inputs(model):
     """Jeans parameters of the workload: disk (velocity structure 3) with
-    DispersionRoverZratio 1.5 and streaming parameter 0.8; halo structure 0."""
+    sigma_R / sigma_z = 1 (DispersionRoverZratio 1, as the halo + disk
+    configuration fixes it) and streaming parameter 0.8; halo structure 0."""
     from galic_b200 import jeans
 
     sp, _ = sampling_inputs(model)
-    jp = jeans.jeans_params(streaming=(0.0, 0.0, 0.8, 0.0), r_over_z=(0.0, 1.5, 1.5, 1.5))
+    jp = jeans.jeans_params(streaming=(0.0, 0.0, 0.8, 0.0), r_over_z=(0.0, 1.0, 1.0, 1.0))
     return sp, jp
 
 
@@ -295,7 +306,8 @@ def measure_jeans(model, steps, cpu):
     res = {"ms_per_call_e2e": ms, "fg_nbin": model.params.FG_Nbin,
            "velocity_structures": {t: model.params.TypeOfVelocityStructure[t] for t in (1, 2, 3)
                                    if model.params.NType[t] > 0},
-           "parameters": "synthetic: disk DispersionRoverZratio 1.5, StreamingVelocityParameter 0.8",
+           "parameters": "synthetic: disk DispersionRoverZratio 1 (sigma_R/sigma_z = 1), "
+                         "StreamingVelocityParameter 0.8",
            "gpu_launches": launches}
     if cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -578,12 +590,22 @@ def measured_fp64_peak(torch):
 # ------------------------------------------------------------------ arms
 
 
+def workload_config(model):
+    """The `config` object both arms print (identical for the same workload)."""
+    return {"workload": WORKLOAD, "particles": int(model.n)}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
 
+    from galic_b200 import synth
+
+    # the workload's set-up geometry from the C restatement: this arm never
+    # loads libgalic_cuda.so
+    synth.use_geometry(oracle_lib.OracleGeometry())
     model = build_workload(args.scale, seed=2)
     per_step = max(args.cpu_seconds / 3.0, 2.0)
     vals = []
@@ -593,16 +615,63 @@ def reference_arm(args, rank, world):
         if k >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
-    sample = f"{orbits} orbits of the workload per step, {cores} processes x {per_step:.1f} s"
+    sample = (f"{orbits} orbits of the workload per step, {cores} processes x {per_step:.1f} s, "
+              f"GALIC's C built {REF_BUILD}")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "orbit-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": f"{cores} host processes"},
+            "config": workload_config(model), "parallelism": f"{cores} host processes",
             "cpu_baseline": {"value": value, "unit": "orbit-steps/s", "cores": cores,
                              "kind": "reference" if kind == "reference" else "port", "sample": sample,
                              "cpu": cpu_model()},
             "e2e": {"value": value, "unit": "orbit-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def fp32_error(ctx, model):
+    """Error of the FP32-integrate / FP64-accumulate form against the FP64
+    drop-in on the same pass (same initial velocities): every committed grid
+    of every type, per bin relative to the FP64 bin (bins above a floor of
+    the grid's peak) and relative to the grid's peak, and the merit values."""
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64, _ffi
+
+    types = [t for t in (1, 2, 3) if model.params.NType[t]]
+    out = {}
+    for form in (GALIC_FORM_FP64, GALIC_FORM_FP32):
+        ctx.calc_all_response_fields(form)
+        out[form] = ({(t, w): ctx.response(t, w) for t in types for w in range(_ffi.GRID_COUNT)}, ctx.fit())
+    g64, f64 = out[GALIC_FORM_FP64]
+    g32, f32 = out[GALIC_FORM_FP32]
+    peak_rel = 0.0
+    floors = (1e-1, 1e-2, 1e-3)
+    per_bin = {f: [] for f in floors}
+    for key, a in g64.items():
+        if key[1] >= _ffi.GRID_MASS_I:
+            continue  # the instantaneous grids do not depend on the orbit form
+        b = g32[key]
+        peak = np.abs(a).max()
+        if peak <= 0:
+            continue
+        d = np.abs(b - a)
+        peak_rel = max(peak_rel, float(d.max() / peak))
+        for f in floors:
+            sel = np.abs(a) >= f * peak
+            per_bin[f].append(d[sel] / np.abs(a[sel]))
+    res = {"vs": "FP64 drop-in form on the same pass", "grids": "DG_MassLoc, EG_EgyResponse{R,T,Q,P}LocS per type",
+           "peak_relative_max": peak_rel}
+    for f in floors:
+        r = np.concatenate(per_bin[f])
+        res[f"per_bin_relative_bins_above_{f:g}_of_peak"] = {
+            "bins": int(r.size), "max": float(r.max()), "median": float(np.median(r)),
+            "p99": float(np.percentile(r, 99)), "frac_within_1e-4": float(np.mean(r <= 1e-4))}
+    fit = {}
+    for t in types:
+        sall64 = f64[t, 0] + (f64[t, 1] + f64[t, 2] + f64[t, 3] + f64[t, 4]) / max(f64[t, 6], 1.0)
+        sall32 = f32[t, 0] + (f32[t, 1] + f32[t, 2] + f32[t, 3] + f32[t, 4]) / max(f32[t, 6], 1.0)
+        fit[str(t)] = {"S_rel": float(abs(f32[t, 0] - f64[t, 0]) / abs(f64[t, 0])),
+                       "Sall_rel": float(abs(sall32 - sall64) / abs(sall64))}
+    res["fit_relative"] = fit
+    return res
 
 
 def ours_arm(args, rank, world, local_rank):
@@ -727,33 +796,44 @@ def ours_arm(args, rank, world, local_rank):
         serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
+        fp32_err = fp32_error(ctx, model)
         cpu = None
         if world == 1 and args.cpu_seconds > 0:
             v, kind, cores, orbits, st = cpu_orbit_steps_per_s(model, args.cpu_seconds)
             cpu = {"value": v, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
                    "sample": f"{orbits} orbits ({st} orbit-steps) of this workload, {cores} processes, "
                              f"~{args.cpu_seconds:.0f} s each", "cpu": cpu_model()}
+        fp64_form = form == GALIC_FORM_FP64
+        kern_name = "k_calc_all_fp64" if fp64_form else "k_calc_all_fp32"
+        traffic = KERNEL_DRAM_BYTES_PER_ORBIT.get(kern_name)
         line = {"metric": METRIC, "value": value, "unit": "orbit-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "strong" if sharded else "weak", "vs_baseline": None,
-                "dtype": "f64" if form == GALIC_FORM_FP64 else "f32",
+                "dtype": "f64" if fp64_form else "f32",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "form": args.form, "particles_per_gpu": model.n,
-                           "orbit_steps_per_step": steps[-1], "l2": "flushed (256 MiB write) between steps",
-                           "parallelism": (f"one model sharded over {world} GPUs (int64 allreduce)" if sharded
-                                           else f"{world} independent models (one per GPU)")},
-                "roofline": {"bound": "fp64" if form == GALIC_FORM_FP64 else "fp32", "achieved": achieved,
-                             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "config": workload_config(model),
+                "form": ("FP64 drop-in (bit-exact per orbit to the restatement of GALIC's C)" if fp64_form
+                         else "FP32-integrate / FP64-accumulate"),
+                "orbit_steps_per_step": steps[-1], "l2": "flushed (256 MiB write) between steps",
+                "parallelism": (f"one model sharded over {world} GPUs (int64 allreduce)" if sharded
+                                else f"{world} independent models (one per GPU)"),
+                "roofline": {"bound": "fp64" if fp64_form else "fp32", "achieved": achieved,
+                             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                             "traffic": (traffic * model.n) if traffic else None,
+                             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                                                "0.1 of the workload's particles, scaled by the orbit count "
+                                                f"(profiles/{kern_name}_halo_disk.md)") if traffic else None,
                              "peak_source": ("measured FP64 GEMM (torch.matmul float64 4096^3, burst)"
-                                             if form == GALIC_FORM_FP64 else
+                                             if fp64_form else
                                              "measured FP32 SIMT GEMM (torch.matmul float32 8192^3, TF32 off, "
                                              "burst)") + "; MEASURED_PEAKS.json has no FP32/FP64 figure",
                              "flop_per_orbit_step": FLOP_PER_STEP,
-                             "kernel": "k_calc_all_fp64" if form == GALIC_FORM_FP64 else "k_calc_all_fp32",
+                             "kernel": kern_name,
                              "kernel_ms": kern_avg},
                 "forms": {args.form: value, ("fp64" if args.form == "fp32" else "fp32"): other_value,
                           "fp32_over_fp64": (value / other_value) if args.form == "fp32" else (other_value / value),
                           "unit": "orbit-steps/s"},
+                "fp32_error": fp32_err,
                 "cpu_baseline": cpu,
                 "force_grid_fill": fill,
                 "target_sampling": target_sampling,
@@ -796,7 +876,25 @@ def row_alone(args):
 
     torch.cuda.set_device(0)
     model = build_workload(args.scale, seed=2)
-    if args.row == "fill":
+    if args.row == "calc_all":
+        # the orbit pass alone in the --form form (the command the orbit
+        # kernels' profile summaries run)
+        from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64
+
+        form = GALIC_FORM_FP64 if args.form == "fp64" else GALIC_FORM_FP32
+        with Context(model.params) as ctx:
+            ctx.load_model(model)
+            for _ in range(args.warmup):
+                ctx.calc_all_response_fields(form)
+            ms = []
+            for _ in range(args.steps):
+                ctx.calc_all_response_fields(form)
+                ms.append(ctx.last_timing()[1])
+            res = {"form": args.form, "particles": model.n, "orbit_steps": ctx.last_orbit_steps(),
+                   "kernel_ms": statistics.mean(ms),
+                   "orbit_steps_per_s": ctx.last_orbit_steps() / (statistics.mean(ms) * 1e-3),
+                   "max_energy_error": ctx.last_max_energy_error()}
+    elif args.row == "fill":
         res = measure_fill(model, args.steps, False, measured_fp64_peak(torch))
     elif args.row == "sampling":
         with Context(model.params) as ctx:

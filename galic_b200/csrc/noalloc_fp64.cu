@@ -3,25 +3,32 @@
 // allocate device memory.
 //
 // Some callers cannot call cudaMalloc: code running inside a host framework
-// that owns every device allocation through its own pool, code replayed
-// from a captured CUDA graph, or a host process whose device-memory budget is
-// fixed before the solver starts.  This entry point takes only caller-owned
-// device buffers for its inputs and outputs and allocates nothing.  Its
-// working memory (the exact fixed-point bin accumulators and a few counters)
-// is the file-scope array g_noalloc_scratch below: a fixed 3.75 MiB + 256 B
-// per device, resident on every GPU that loads the library until the process
-// exits.  The sizes it accepts are limited by that array: at most three
-// particle types and DG_MaxLevel <= 7 (16384 bins per grid); larger requests
-// are rejected with GALIC_ERR_BUDGET.
+// that owns every device allocation through its own pool, or a host process
+// whose device-memory budget is fixed before the solver starts.  This entry
+// point takes only caller-owned device buffers for its inputs and outputs and
+// allocates nothing.  Its working memory (the exact fixed-point bin
+// accumulators and two counters) is the file-scope array g_noalloc_scratch
+// below: a fixed 3.75 MiB + 256 B per device, resident on every GPU that
+// loads the library until the process exits.  The sizes it accepts are
+// limited by that array: at most three particle types and DG_MaxLevel <= 7
+// (16384 bins per grid); larger requests are rejected with GALIC_ERR_BUDGET.
 //
 // The array's name is only a host-side stand-in in host code.  Its device
 // address is looked up once per device with cudaGetSymbolAddress (with that
 // device current) on the first call made on the device; make that first call
-// before any stream capture.  All calls share the one array and leave the
-// last call's contents in it; each call clears the accumulators it uses
+// before any stream capture.  The cached address belongs to the device's
+// context: after cudaDeviceReset it is stale, and the library must be
+// reloaded.  All calls share the one array and leave the last call's
+// contents in it; each call clears the accumulators and counters it uses
 // before its kernel runs.  Calls whose work overlaps on the GPU (other
 // streams, other host threads) race on the array and must be serialised by
 // the caller.
+//
+// Particles are checked on the device before their orbit starts (a type
+// outside 1..3, a non-positive or non-finite Tint or a non-finite mass):
+// such a particle is skipped, deposits nothing, and the call returns
+// GALIC_ERR_INVALID_ARGUMENT.  Step counts and energy errors are not
+// returned; the context path reports them.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -35,12 +42,13 @@ constexpr int kTypes = 3;        // particle types 1..3
 constexpr int kFields = NF_ORBIT;  // m, r, t, q, p
 constexpr int kMaxGrid = 16384;  // DG_MaxLevel <= 7
 
+// status words beyond OrbitStatus (the worst code seen wins)
+enum { NOALLOC_OVERFLOW = 3, NOALLOC_INVALID = 4 };
+
 struct NoAllocScratch {
   FxWord fx[kTypes * kFields * kMaxGrid];
   int next;
   int status;
-  unsigned long long steps;
-  double max_egy_err;
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
@@ -140,12 +148,22 @@ __global__ void __launch_bounds__(128, 3) k_noalloc_orbits(DevModel M, NoAllocAr
   sink.cur = -1;
   sink.parked = false;
   int p = -1;
-  unsigned long long my_steps = 0;
   int my_status = 0;
   auto fetch = [&]() -> bool {
-    int k = atomicAdd(&A.scratch->next, 1);
-    if(k >= A.n) return false;
-    p = k;
+    for(;;) {
+      const int k = atomicAdd(&A.scratch->next, 1);
+      if(k >= A.n) return false;
+      // an invalid particle would index outside the grids (type) or never
+      // reach its time span (Tint): skip it and report it
+      const int t = A.type[k];
+      const double tint = A.tint[k], mass = A.mass[k];
+      if(t >= 1 && t <= kTypes && tint > 0 && tint <= 1.0e300 && mass == mass && fabs(mass) <= 1.0e300) {
+        p = k;
+        break;
+      }
+      if(A.orbits) A.orbits[k] = 0;
+      my_status = NOALLOC_INVALID;
+    }
     sink.type = A.type[p];
     sink.fac = A.mass[p] / A.tint[p];
     sink.cur = -1;
@@ -165,20 +183,26 @@ __global__ void __launch_bounds__(128, 3) k_noalloc_orbits(DevModel M, NoAllocAr
     } else if(state == ST_FINISH) {
       sink.park();
       if(A.orbits) A.orbits[p] = s.norbit;
-      my_steps += (unsigned long long) s.steps;
       if(s.status != ORBIT_OK) my_status = max(my_status, s.status);
       state = fetch() ? ST_ACTIVE : ST_DONE;
     }
   }
-  if(my_steps) atomicAdd(&A.scratch->steps, my_steps);
   if(my_status) atomicMax(&A.scratch->status, my_status);
 }
 
-__global__ void k_noalloc_finalize(const NoAllocScratch *sc, Shifts sh, double *out, int G)
+// fixed-point words -> FP64 grids; a high word beyond 2^62 means the bins
+// came close to the word's range (a phi_bound below max|FG_Pot|)
+__global__ void k_noalloc_finalize(NoAllocScratch *sc, Shifts sh, double *out, int G)
 {
   const size_t total = (size_t) kTypes * kFields * G;
-  for(size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < total; i += (size_t) gridDim.x * blockDim.x)
-    out[i] = fx_value(sc->fx[i], sh.s[i / G]);
+  bool over = false;
+  for(size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < total; i += (size_t) gridDim.x * blockDim.x) {
+    const FxWord w = sc->fx[i];
+    const long long h = (long long) w.hi;
+    over |= h > (1LL << 62) || h < -(1LL << 62);
+    out[i] = fx_value(w, sh.s[i / G]);
+  }
+  if(over) atomicMax(&sc->status, (int) NOALLOC_OVERFLOW);
 }
 
 std::mutex g_setup_mutex;
@@ -200,7 +224,7 @@ extern "C" int galic_orbit_responses_noalloc(const galic_params_t *prm, const do
                                              void *stream)
 {
   if(!prm || !d_fg_acc2 || !d_fg_pot || !d_vstream || !d_cellsize || !d_out || n < 0 ||
-     (n > 0 && (!d_pos || !d_vel || !d_mass || !d_tint || !d_type)))
+     (n > 0 && (!d_pos || !d_vel || !d_mass || !d_tint || !d_type)) || !(std::fabs(phi_bound) <= 1.0e300))
     return GALIC_ERR_INVALID_ARGUMENT;
   if(prm->DG_MaxLevel != prm->EG_MaxLevel || prm->DG_MaxLevel < 1 || prm->FG_Nbin < 2 || !(prm->Halo_Mass > 0))
     return GALIC_ERR_INVALID_ARGUMENT;
@@ -281,25 +305,26 @@ extern "C" int galic_orbit_responses_noalloc(const galic_params_t *prm, const do
   }
   // clear what must start at zero: the accumulators of this size and the counters
   if(cudaMemsetAsync(sc->fx, 0, (size_t) kTypes * kFields * G * sizeof(FxWord), s) != cudaSuccess ||
-     cudaMemsetAsync(&sc->next, 0, sizeof(int) + sizeof(int) + sizeof(unsigned long long) + sizeof(double), s) !=
-         cudaSuccess)
+     cudaMemsetAsync(&sc->next, 0, sizeof(int) + sizeof(int), s) != cudaSuccess)
     return GALIC_ERR_CUDA;
+  int sms = 0;
+  if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
   if(n > 0) {
-    int sms = 148, per_sm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_noalloc_orbits, 128, 0);
     int grid = (per_sm > 0 ? per_sm : 1) * sms;
     int need = (n + 127) / 128;
     if(grid > need) grid = need;
     k_noalloc_orbits<<<grid, 128, 0, s>>>(M, A);
   }
-  k_noalloc_finalize<<<148 * 4, 256, 0, s>>>(sc, A.shift, d_out, G);
+  k_noalloc_finalize<<<sms * 4, 256, 0, s>>>(sc, A.shift, d_out, G);
   int status = 0;
   if(cudaGetLastError() != cudaSuccess) return GALIC_ERR_CUDA;
   if(cudaMemcpyAsync(&status, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
      cudaStreamSynchronize(s) != cudaSuccess)
     return GALIC_ERR_CUDA;
+  if(status == NOALLOC_INVALID || status == ORBIT_NONFINITE) return GALIC_ERR_INVALID_ARGUMENT;
+  if(status == NOALLOC_OVERFLOW) return GALIC_ERR_OVERFLOW;
   if(status == ORBIT_STEP_CAP) return GALIC_ERR_STEP_CAP;
-  if(status == ORBIT_NONFINITE) return GALIC_ERR_INVALID_ARGUMENT;
   return GALIC_OK;
 }

@@ -38,6 +38,24 @@ UNIT_TIME = UNIT_LENGTH / UNIT_VELOCITY
 G_INTERNAL = GRAVITY / UNIT_LENGTH ** 3 * UNIT_MASS * UNIT_TIME ** 2
 H_INTERNAL = HUBBLE * UNIT_TIME
 
+# Set-up geometry (grid spacing, cell sizes, stack smoothing): by default the
+# host functions of libgalic_cuda.so (galic_grid_geometry,
+# galic_density_geometry, galic_smooth_stack).  use_geometry() swaps in any
+# object with the same three functions, so that a CPU-only process (the
+# benchmark's timing of GALIC's own C) builds the same workload without
+# loading the CUDA library.
+_geometry = None
+
+
+def use_geometry(provider):
+    """Routes the set-up geometry to `provider` (None: libgalic_cuda.so)."""
+    global _geometry
+    _geometry = provider
+
+
+def _geo():
+    return _geometry if _geometry is not None else _ffi.load_library()
+
 
 @dataclass
 class Component:
@@ -125,7 +143,7 @@ class _Potential:
 
 def make_params(comps, v200=None, fg_nbin=256, level=6, outer_frac=0.980296, inner_frac=9.80296e-5,
                 torbit_fac=5.0, f_orb=0.0314, f_cc=0.25, min_disp=100, min_dens=50):
-    lib = _ffi.load_library()
+    lib = _geo()
     m200 = sum(c.mass for c in comps)
     if v200 is None:
         v200 = (10.0 * G_INTERNAL * H_INTERNAL * m200) ** (1.0 / 3.0)  # structure.c:60
@@ -212,7 +230,7 @@ def _stack_offset(l):
 
 
 def _smooth(finest, level):
-    lib = _ffi.load_library()
+    lib = _geo()
     ns = ((1 << (2 + 2 * level)) - 1) // 3
     st = np.zeros(ns)
     st[_stack_offset(level):] = finest
@@ -256,7 +274,7 @@ def build_model(comps, seed=1, level=6, fg_nbin=256, outer_frac=0.980296, inner_
     rng = np.random.default_rng(seed)
     params, rmax, torbit_fac = make_params(comps, fg_nbin=fg_nbin, level=level, outer_frac=outer_frac,
                                            inner_frac=inner_frac, torbit_fac=torbit_fac, f_orb=f_orb, f_cc=f_cc)
-    lib = _ffi.load_library()
+    lib = _geo()
     potobj = _Potential(comps)
     N = params.FG_Nbin
     nodes = params.FG_Rmin * (params.FG_Fac ** np.arange(N) - 1.0)

@@ -206,9 +206,9 @@ int galic_last_kernel_launches(const galic_ctx *ctx);
 /* No counterpart in the reference.  The orbit-response binning of
  * galic_calc_all_response_fields (time-averaged grids only, no fit) for
  * callers that cannot allocate device memory: a host framework that owns
- * every device allocation through its own pool, work replayed from a
- * captured CUDA graph, or a process with a device-memory budget fixed in
- * advance.  Every pointer named d_* is caller-owned DEVICE memory:
+ * every device allocation through its own pool, or a process with a
+ * device-memory budget fixed in advance.  Every pointer named d_* is
+ * caller-owned DEVICE memory:
  *   d_fg_acc2   FG_DPotDR / FG_DPotDz interleaved: [FG_Nbin^2][2]
  *   d_fg_pot    FG_Pot [FG_Nbin^2]
  *   d_vstream   FG_Vstream of types 1..3: [3][FG_Nbin^2]
@@ -216,14 +216,19 @@ int galic_last_kernel_launches(const galic_ctx *ctx);
  *   particles   d_pos/d_vel [n][3], d_mass, d_tint [n], d_type [n] in 1..3
  *   d_out       [3 types][5][DG_Ngrid]: DG_MassLoc, EG_EgyResponse{R,T,Q,P}LocS
  *   d_orbits    [n] orbit counts, may be NULL
- * phi_bound bounds |FG_Pot| (e.g. -min FG_Pot); it sets the fixed-point
- * range exactly as the context path does.  stream is a cudaStream_t (NULL =
- * legacy default stream); the call returns after the stream has finished.
+ * phi_bound must be at least max|FG_Pot| (for example -min FG_Pot); it sets
+ * the fixed-point range as the context path does, and a bound too small to
+ * hold the bins gives GALIC_ERR_OVERFLOW.  A particle whose type is outside
+ * 1..3, whose Tint is not positive and finite or whose mass is not finite is
+ * skipped and the call returns GALIC_ERR_INVALID_ARGUMENT.  Step counts and
+ * energy errors are not returned.  stream is a cudaStream_t (NULL = legacy
+ * default stream); the call returns after the stream has finished.
  * Working memory is one file-scope device array of fixed size (3.75 MiB +
  * 256 B per device, kept until exit): DG_MaxLevel > 7 is rejected with
  * GALIC_ERR_BUDGET.  The first call on a device looks up the array's device
- * address; make it before any stream capture.  Calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * address; make it before any stream capture.  That address is stale after
+ * cudaDeviceReset (reload the library).  Calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 int galic_orbit_responses_noalloc(const galic_params_t *prm, const double *d_fg_acc2, const double *d_fg_pot,
                                   const double *d_vstream, const double *d_cellsize, double phi_bound, int n,
                                   const double *d_pos, const double *d_vel, const double *d_mass,

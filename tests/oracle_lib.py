@@ -20,7 +20,9 @@ from galic_b200 import _ffi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref.so")
-REF_SRC = "/root/reference/src"
+# GALIC's C with the reference's own optimisation flags (-O3 -march=native):
+# the timed CPU baseline; the parity build above has FP contraction off
+REF_FAST_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref_fast.so")
 
 dptr, iptr = _ffi.dptr, _ffi.iptr
 PD, PI, VP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
@@ -31,15 +33,31 @@ PJP = C.POINTER(_ffi.GalicJeansParams)
 
 
 def build_oracle():
-    """Compiles oracle/liboracle.so (and oracle/_ref when the reference tree is present)."""
+    """Compiles oracle/liboracle.so, and oracle/_ref when the reference tree
+    is present (oracle/Makefile locates it: $GALIC_REF_SRC or its default)."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "restatement"], check=True)
-    if os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF_SRC={REF_SRC}"],
-                       check=True)
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
 
 
 def reference_available():
     return os.path.exists(REF_SO)
+
+
+def reference_fast_available():
+    return os.path.exists(REF_FAST_SO)
+
+
+class OracleGeometry:
+    """The restatement's set-up geometry under the names synth.use_geometry()
+    expects (galic_grid_geometry, galic_density_geometry, galic_smooth_stack):
+    lets a CPU-only process build the synthetic workloads without loading
+    libgalic_cuda.so."""
+
+    def __init__(self):
+        L = oracle_lib()
+        self.galic_grid_geometry = L.orc_grid_geometry
+        self.galic_density_geometry = L.orc_density_geometry
+        self.galic_smooth_stack = L.orc_smooth_stack
 
 
 _olib = None
@@ -478,8 +496,8 @@ def reference_peano_keys(xyz, bits):
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
 
 
-def _ref_lib():
-    L = C.CDLL(REF_SO)
+def _ref_lib(fast=False):
+    L = C.CDLL(REF_FAST_SO if fast else REF_SO)
     sig = {
         "ref_setup": (C.c_int, [PP]),
         "ref_set_force_grid": (None, [PD, PD, PD]),
@@ -529,10 +547,12 @@ def _ref_lib():
 
 
 class Reference:
-    """GALIC's own C (one model per process: the reference keeps globals)."""
+    """GALIC's own C (one model per process: the reference keeps globals).
+    fast=True loads the build with the reference's own optimisation flags
+    (the timed baseline) instead of the contraction-free parity build."""
 
-    def __init__(self, params):
-        self.L = _ref_lib()
+    def __init__(self, params, fast=False):
+        self.L = _ref_lib(fast)
         self.params = params.copy()
         self.L.ref_setup(C.byref(self.params))
         Lv = params.DG_MaxLevel
