@@ -54,11 +54,17 @@ def parse():
     ap.add_argument("--mode", default="replicas", choices=["replicas", "sharded"],
                     help="N>1: independent models per GPU (weak scaling) or one model sharded over the GPUs "
                          "with an exact int64 allreduce of the response accumulators (strong scaling)")
-    ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving stream (0: skip)")
-    ap.add_argument("--serve-gap", type=float, default=0.05, help="mean Poisson gap between requests, s")
-    ap.add_argument("--serve-scale", type=float, default=0.1, help="particle-count factor of the requests")
+    ap.add_argument("--serve-requests", type=int, default=24,
+                    help="requests of the serving stream measured (a prefix of its 500; 0: skip)")
+    ap.add_argument("--serve-gap", type=float, default=0.5, help="mean Poisson gap between requests, s")
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="particle-count factor of the requests")
     ap.add_argument("--serve-workers", type=int, default=16, help="concurrent jobs of the serving loop")
-    ap.add_argument("--row", default="all", choices=["all", "calc_all", "fill", "sampling", "jeans", "particles"],
+    ap.add_argument("--construction", default="halo", choices=["halo", "composite", "none"],
+                    help="full model construction measured in the bench line (calc_all + iterations x "
+                         "repetitions, both forms); with --row construction it is the one measured")
+    ap.add_argument("--construction-scale", type=float, default=1.0)
+    ap.add_argument("--row", default="all",
+                    choices=["all", "calc_all", "construction", "serving", "fill", "sampling", "jeans", "particles"],
                     help="one secondary measurement alone on this workload (a diagnostic line for profiling, "
                          "not the bench line)")
     return ap.parse_args()
@@ -417,6 +423,151 @@ def measure_ensemble(count, steps):
     return res
 
 
+# ------------------------------------------------------------ model construction
+
+# main.c:83-110 with the optimisation settings every Model_*.param ships:
+# FractionToOptimizeIndependendly 0.001, IndepenentOptimizationsPerStep 100
+CONSTRUCTION = {
+    "halo": {"desc": "plain method: Hernquist halo M=100 a=30 N=1e5, 64x64 DG/EG, 256^2 FG, TorbitFac 5, "
+                     "MaximumNumberOfSteps 9 (10 iterations) x 100 repetitions, FractionToOptimizeIndependendly 0.001",
+             "n": 100_000, "iterations": 10, "reps": 100, "fraction": 0.001},
+    "composite": {"desc": "composite: beta=0.2 halo N=3e6 + disk N=7e5 (h=3.5, z0=0.7) + Hernquist bulge N=3e5 "
+                          "(M=1.5, a=1), 128x128 DG/EG, 256^2 FG, 20 iterations x 100 repetitions, "
+                          "FractionToOptimizeIndependendly 0.001",
+                  "n": 4_000_000, "iterations": 20, "reps": 100, "fraction": 0.001},
+}
+
+
+def construction_model(name, scale):
+    from galic_b200 import synth
+
+    if name == "halo":
+        return synth.config_halo(n=max(int(100_000 * scale), 200), level=6, seed=1)
+    return synth.config_composite(n_halo=max(int(3_000_000 * scale), 300), n_disk=max(int(700_000 * scale), 70),
+                                  n_bulge=max(int(300_000 * scale), 30), level=7, seed=3)
+
+
+def construction_lists(perm, n_per, reps, it):
+    """optimize_some_particles (main.c:120-146) on one rank: the next
+    reps x n_per particles of the permutation, wrapping around."""
+    pos = (it * reps * n_per + np.arange(reps * n_per)) % len(perm)
+    return perm[pos].reshape(reps, n_per).astype(np.int32)
+
+
+def run_construction(model, form, iterations, reps, fraction, seed=11, window_bytes=0):
+    """calc_all_response_fields, then `iterations` x `reps` repetitions
+    (main.c:83-110) through the C ABI, wall clock with the device synchronised
+    at both ends; Sall (main.c:1270) per type after every iteration."""
+    import torch
+
+    from galic_b200 import Context
+
+    n_per = 1 + int(fraction * model.n)  # main.c:128 with NTask = 1
+    perm = np.random.default_rng(seed).permutation(model.n)
+    types = [t for t in (1, 2, 3) if model.params.NType[t]]
+    with Context(model.params) as ctx:
+        ctx.load_model(model)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.calc_all_response_fields(form)
+        steps_calc = ctx.last_orbit_steps()
+        sall = [ctx.sall()[types].tolist()]
+        t_calc = time.perf_counter() - t0
+        steps_rep = 0
+        for it in range(iterations):
+            ctx.optimize_reps(construction_lists(perm, n_per, reps, it), seed, it * reps, form, window_bytes)
+            steps_rep += ctx.last_orbit_steps()
+            sall.append(ctx.sall()[types].tolist())
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        tries, changes = ctx.counters()
+    t_rep = wall - t_calc
+    return {"wall_s": wall, "calc_all_s": t_calc, "repetition_phase_s": t_rep, "particles_per_rep": n_per,
+            "orbit_steps": int(steps_calc + steps_rep), "repetition_orbit_steps": int(steps_rep),
+            "orbit_steps_per_s": (steps_calc + steps_rep) / wall,
+            "repetition_orbit_steps_per_s": steps_rep / t_rep if t_rep > 0 else None,
+            "final_sall": dict(zip(map(str, types), sall[-1])), "sall_per_iteration": sall,
+            "tries": int(tries.sum()), "changes": int(changes.sum())}
+
+
+def _ref_reps_timed(arrays, n_per, k_reps, fast):
+    """GALIC's own repetition (init_updates, optimize x n_per, commit_updates
+    with its calc_global_fit) after its calc_all_response_fields, one rank:
+    seconds per repetition over k_reps repetitions."""
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import oracle_lib
+    from make_golden import model_from_arrays
+
+    m = model_from_arrays(arrays)
+    ref = oracle_lib.Reference(m.params, fast=fast)
+    ref.load_model(m)
+    ref.calc_all()
+    perm = np.random.default_rng(5).permutation(m.n)
+    t = time.perf_counter()
+    for r in range(k_reps):
+        ref.optimize_rep(perm[r * n_per:(r + 1) * n_per], 11, r)
+    return (time.perf_counter() - t) / k_reps
+
+
+def cpu_construction_estimate(name, model, steps_calc, ranks=16, seconds=4.0):
+    """GALIC's own C at `ranks` single-rank processes (one per host core), as
+    its MPI decomposition splits the run (set_particles.c:320-330,
+    main.c:128): calc_all at the measured multi-process orbit-step rate; each
+    repetition as one rank's share, 1 + Fraction N / ranks particles timed on
+    a sample model of the same shape (its calc_global_fit runs on every rank;
+    the MPI allreduce of the grids is not counted)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import oracle_lib
+    from make_golden import model_arrays
+
+    cfg = CONSTRUCTION[name]
+    rate, kind, cores, _, _ = cpu_orbit_steps_per_s(model, seconds, cores=ranks)
+    n_rank = 1 + int(cfg["fraction"] * cfg["n"] / ranks)
+    sample = construction_model(name, 4000.0 / cfg["n"])
+    k_reps = 10
+    per_rep = oracle_lib.run_reference(_ref_reps_timed, model_arrays(sample), n_rank, k_reps,
+                                       oracle_lib.reference_fast_available(), timeout=1800)
+    reps_total = cfg["iterations"] * cfg["reps"]
+    t = steps_calc / rate + reps_total * per_rep
+    return {"seconds": t, "ranks": ranks, "kind": kind, "calc_all_orbit_steps_per_s": rate,
+            "seconds_per_repetition": per_rep, "particles_per_rank_per_rep": n_rank,
+            "sample": (f"calc_all: {ranks} processes on this model's orbits ({seconds:.0f} s each); repetitions: "
+                       f"{k_reps} of GALIC's own, {n_rank} particles each, on a {sample.n}-particle model of the "
+                       f"same shape, extrapolated to {reps_total} repetitions; MPI allreduce not counted")}
+
+
+def measure_construction(name, scale, cpu):
+    """Both forms of a full model construction, and GALIC's own C estimate."""
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64
+
+    cfg = CONSTRUCTION[name]
+    model = construction_model(name, scale)
+    window = (24 << 30) if model.params.DG_MaxLevel >= 7 else 0
+    res = {"config": cfg["desc"], "particles": model.n, "scale": scale}
+    for label, form in (("fp64", GALIC_FORM_FP64), ("fp32", GALIC_FORM_FP32)):
+        res[label] = run_construction(model, form, cfg["iterations"], cfg["reps"], cfg["fraction"],
+                                      window_bytes=window)
+    a, b = res["fp64"]["final_sall"], res["fp32"]["final_sall"]
+    res["fp32_vs_fp64_final_sall_rel"] = {t: abs(b[t] - a[t]) / abs(a[t]) for t in a}
+    target = {t: a[t] for t in a}
+    reached = None
+    for k, row in enumerate(res["fp32"]["sall_per_iteration"]):
+        if all(v <= target[t] * (1 + 1e-12) for t, v in zip(a, row)):
+            reached = k
+            break
+    res["fp32_iterations_to_fp64_final_sall"] = reached
+    res["wall_fp32_over_fp64"] = res["fp64"]["wall_s"] / res["fp32"]["wall_s"]
+    if cpu:
+        steps_calc = res["fp64"]["orbit_steps"] - res["fp64"]["repetition_orbit_steps"]
+        est = cpu_construction_estimate(name, model, steps_calc)
+        res["cpu_reference"] = est
+        res["speedup_fp64_vs_cpu"] = est["seconds"] / res["fp64"]["wall_s"]
+    return res
+
+
 def serving_requests(count, seed, scale):
     """The serving stream's requests: 70% halo-only (N log-uniform in
     [1e4, 1e6] x scale), 30% halo+disk+bulge (N log-uniform in [1e5, 2e6] x
@@ -443,19 +594,31 @@ def serving_requests(count, seed, scale):
     return out
 
 
+SERVE_SCHEDULE = {"iterations_max": 20, "reps_per_iteration": 100, "fraction_per_rep": 0.001,
+                  "converge_rel": 0.01}
+
+
 def measure_serving(count, mean_gap, scale, torch, workers=16):
-    """Poisson stream of model-construction jobs through the serving loop:
-    admission by HBM budget, concurrent jobs on one GPU, per-job
+    """The serving stream's first `count` requests (Poisson arrivals, mean gap
+    `mean_gap`) through the serving loop: admission by HBM budget, concurrent
+    jobs on one GPU, each job calc_all plus iterations of 100 repetitions
+    (FractionToOptimizeIndependendly 0.001, repetitions in windows) until an
+    iteration lowers Sall by less than 1 % (at most 20 iterations); p50/p99
     time-to-convergence (submit to done)."""
     from galic_b200 import GALIC_FORM_FP32
     from galic_b200.serving import Server
 
+    t_build = time.perf_counter()
     models = serving_requests(count, 5, scale)
+    t_build = time.perf_counter() - t_build
     rng = np.random.default_rng(6)
     arrivals = np.cumsum(rng.exponential(mean_gap, count))
     free, total = torch.cuda.mem_get_info()
     budget = int(0.5 * free)
-    schedule = dict(form=GALIC_FORM_FP32, max_iterations=2, reps_per_iteration=5, fraction_per_rep=0.001)
+    sch = SERVE_SCHEDULE
+    schedule = dict(form=GALIC_FORM_FP32, max_iterations=sch["iterations_max"],
+                    reps_per_iteration=sch["reps_per_iteration"], fraction_per_rep=sch["fraction_per_rep"],
+                    converge_rel=sch["converge_rel"])
     with Server(budget, workers=workers) as srv:
         t0 = time.perf_counter()
         ids = []
@@ -464,20 +627,22 @@ def measure_serving(count, mean_gap, scale, torch, workers=16):
             if dt > 0:
                 time.sleep(dt)
             ids.append(srv.submit(m, seed=1000 + k, **schedule))
-        res = [srv.wait(i, timeout=1800) for i in ids]
+        res = [srv.wait(i, timeout=3600) for i in ids]
         makespan = time.perf_counter() - t0
         st = srv.stats()
     ok = [r for r in res if r["status"] == 0]
     lat = np.array([r["t_done"] - r["t_submit"] for r in ok])
     steps = sum(r["orbit_steps"] for r in ok)
+    its = np.array([r["iterations"] for r in ok])
     return {"requests": count, "completed": len(ok), "mean_gap_s": mean_gap, "particles_scale": scale,
+            "arrivals": f"first {count} requests of the 500-request stream (Poisson, mean gap {mean_gap} s)",
             "n_range": [int(min(m.n for m in models)), int(max(m.n for m in models))],
-            "schedule": {"calc_all": "fp32", "iterations": 2, "reps_per_iteration": 5,
-                         "fraction_per_rep": 0.001, "reps": "fp32 orbits, fp64 merit"},
+            "schedule": {"calc_all": "fp32", "reps": "fp32 orbits, fp64 merit, windows of repetitions", **sch},
+            "iterations_to_convergence": {"median": float(np.median(its)), "max": int(its.max())},
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "makespan_s": makespan, "orbit_steps": int(steps), "orbit_steps_per_s": steps / makespan,
             "hbm_budget_bytes": budget, "peak_bytes": st["peak_bytes"], "peak_concurrent_jobs": st["peak_running"],
-            "workers": workers}
+            "workers": workers, "host_build_s": t_build}
 
 
 def cpu_model():
@@ -628,27 +793,17 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def fp32_error(ctx, model):
-    """Error of the FP32-integrate / FP64-accumulate form against the FP64
-    drop-in on the same pass (same initial velocities): every committed grid
-    of every type, per bin relative to the FP64 bin (bins above a floor of
-    the grid's peak) and relative to the grid's peak, and the merit values."""
-    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64, _ffi
+def _bin_errors(got, want, floors):
+    """Peak-relative and per-bin relative errors of `got` against `want`
+    ({(type, grid): array}), over the time-averaged grids."""
+    from galic_b200 import _ffi
 
-    types = [t for t in (1, 2, 3) if model.params.NType[t]]
-    out = {}
-    for form in (GALIC_FORM_FP64, GALIC_FORM_FP32):
-        ctx.calc_all_response_fields(form)
-        out[form] = ({(t, w): ctx.response(t, w) for t in types for w in range(_ffi.GRID_COUNT)}, ctx.fit())
-    g64, f64 = out[GALIC_FORM_FP64]
-    g32, f32 = out[GALIC_FORM_FP32]
     peak_rel = 0.0
-    floors = (1e-1, 1e-2, 1e-3)
     per_bin = {f: [] for f in floors}
-    for key, a in g64.items():
+    for key, a in want.items():
         if key[1] >= _ffi.GRID_MASS_I:
             continue  # the instantaneous grids do not depend on the orbit form
-        b = g32[key]
+        b = got[key]
         peak = np.abs(a).max()
         if peak <= 0:
             continue
@@ -657,13 +812,42 @@ def fp32_error(ctx, model):
         for f in floors:
             sel = np.abs(a) >= f * peak
             per_bin[f].append(d[sel] / np.abs(a[sel]))
-    res = {"vs": "FP64 drop-in form on the same pass", "grids": "DG_MassLoc, EG_EgyResponse{R,T,Q,P}LocS per type",
-           "peak_relative_max": peak_rel}
+    res = {"peak_relative_max": peak_rel}
     for f in floors:
         r = np.concatenate(per_bin[f])
         res[f"per_bin_relative_bins_above_{f:g}_of_peak"] = {
             "bins": int(r.size), "max": float(r.max()), "median": float(np.median(r)),
             "p99": float(np.percentile(r, 99)), "frac_within_1e-4": float(np.mean(r <= 1e-4))}
+    return res
+
+
+def fp32_error(ctx, model):
+    """Error of the FP32-integrate / FP64-accumulate form against the FP64
+    drop-in on the same pass (same initial velocities): every time-averaged
+    grid of every type, per bin relative to the FP64 bin (bins above a floor
+    of the grid's peak) and relative to the grid's peak, and the merit
+    values.  Beside it the orbits' own sensitivity: the FP64 form against
+    itself with the initial velocities perturbed by 1e-7 (relative)."""
+    from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64, _ffi
+
+    types = [t for t in (1, 2, 3) if model.params.NType[t]]
+    floors = (1e-1, 1e-2, 1e-3)
+
+    def grids():
+        return {(t, w): ctx.response(t, w) for t in types for w in range(_ffi.GRID_COUNT)}
+
+    ctx.calc_all_response_fields(GALIC_FORM_FP64)
+    g64, f64 = grids(), ctx.fit()
+    ctx.calc_all_response_fields(GALIC_FORM_FP32)
+    g32, f32 = grids(), ctx.fit()
+    vel = model.vel * (1 + 1e-7 * np.random.default_rng(1).standard_normal(model.vel.shape))
+    ctx.set_particles(model.pos, vel, model.mass, model.tint, model.vesc, model.ptype, model.ptargets)
+    ctx.calc_all_response_fields(GALIC_FORM_FP64)
+    gp = grids()
+    ctx.set_particles(model.pos, model.vel, model.mass, model.tint, model.vesc, model.ptype, model.ptargets)
+    res = {"vs": "FP64 drop-in form on the same pass", "grids": "DG_MassLoc, EG_EgyResponse{R,T,Q,P}LocS per type"}
+    res.update(_bin_errors(g32, g64, floors))
+    res["fp64_sensitivity_1e-7_velocity_perturbation"] = _bin_errors(gp, g64, floors)
     fit = {}
     for t in types:
         sall64 = f64[t, 0] + (f64[t, 1] + f64[t, 2] + f64[t, 3] + f64[t, 4]) / max(f64[t, 6], 1.0)
@@ -793,6 +977,9 @@ def ours_arm(args, rank, world, local_rank):
         jeans_solve = measure_jeans(model, args.steps, world == 1 and args.cpu_seconds > 0)
         init_particles = measure_particles(model, args.steps, world == 1 and args.cpu_seconds > 0)
         ensemble = measure_ensemble(args.ensemble_models, args.steps) if args.ensemble_models > 0 else None
+        construction = (measure_construction(args.construction, args.construction_scale,
+                                             world == 1 and args.cpu_seconds > 0)
+                        if args.construction != "none" else None)
         serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
                    if args.serve_requests > 0 else None)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
@@ -840,6 +1027,7 @@ def ours_arm(args, rank, world, local_rank):
                 "jeans": jeans_solve,
                 "particle_init": init_particles,
                 "ensemble": ensemble,
+                "construction": construction,
                 "serving": serving,
                 "e2e": {"value": e2e_value, "unit": "orbit-steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
@@ -894,6 +1082,10 @@ def row_alone(args):
                    "kernel_ms": statistics.mean(ms),
                    "orbit_steps_per_s": ctx.last_orbit_steps() / (statistics.mean(ms) * 1e-3),
                    "max_energy_error": ctx.last_max_energy_error()}
+    elif args.row == "serving":
+        res = measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
+    elif args.row == "construction":
+        res = measure_construction(args.construction, args.construction_scale, args.cpu_seconds > 0)
     elif args.row == "fill":
         res = measure_fill(model, args.steps, False, measured_fp64_peak(torch))
     elif args.row == "sampling":

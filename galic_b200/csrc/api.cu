@@ -195,7 +195,7 @@ int fixed_point_shift(double bound)
 }
 
 // form: two-word exact words (FP64 form) or one signed word (FP32 form,
-// flush.cuh:warp_drain32); both keep every bin total inside the word's range
+// flush.cuh:warp_drain_nodes); both keep every bin total inside the word's range
 void set_shifts(galic_ctx *ctx, int *shift, int form)
 {
   const galic_params_t &p = ctx->prm;
@@ -893,48 +893,18 @@ extern "C" int galic_calc_all_finish(galic_ctx *ctx)
   return fail(ctx, GALIC_OK);
 }
 
-extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial,
-                                  int form)
+namespace {
+
+// device arguments of `count` optimised particles starting at the context's
+// scratch (one repetition, or a window of repetitions of per_rep each)
+RepArgs make_rep_args(galic_ctx *ctx, int count, uint64_t seed, uint32_t rep_serial, int per_rep)
 {
-  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
-  if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
-  if(!ctx->have_response) return fail(ctx, GALIC_ERR_STATE);
-  if(form == GALIC_FORM_FP32) {
-    int st = ensure_tab32(ctx);
-    if(st) return st;
-  }
-  if(count < 0 || (count > 0 && !idx)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
-  // every particle at most once per repetition: the reference evaluates a
-  // repetition against committed state and P[n] only changes for n itself
-  std::vector<char> seen(ctx->n, 0);
-  for(int k = 0; k < count; k++) {
-    if(idx[k] < 0 || idx[k] >= ctx->n || seen[idx[k]]) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
-    seen[idx[k]] = 1;
-  }
-  cudaStream_t s = ctx->stream;
-  FitArgs f = make_fit_args(ctx);
-  if(count == 0) {  // init_updates + commit_updates with no particle: only the fit
-    ctx->last_launches = launch_global_fit(f, s);
-    CK(cudaStreamSynchronize(s));
-    return fail(ctx, GALIC_OK);
-  }
-  int st = ensure_rep_scratch(ctx, count);
-  if(st) return st;
-  // staging: idx, then status, per-orbit status and steps
-  const size_t off_st = ((size_t) count * sizeof(int) + 15) & ~(size_t) 15;
-  const size_t off_ost = off_st + 16;
-  const size_t off_steps = (off_ost + 2 * (size_t) count * sizeof(int) + 15) & ~(size_t) 15;
-  char *h = stage(ctx, off_steps + 2 * (size_t) count * sizeof(long long));
-  if(!h) return fail(ctx, GALIC_ERR_CUDA);
-  std::memcpy(h, idx, count * sizeof(int));
-  CK(cudaMemcpyAsync(ctx->d_idx, h, count * sizeof(int), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
-  CK(cudaMemsetAsync(ctx->d_b_status, 0, 2 * (size_t) count * sizeof(int), s));
   RepArgs R;
   R.count = count;
   R.idx = ctx->d_idx;
   R.seed = seed;
   R.rep_serial = rep_serial;
+  R.per_rep = per_rep;
   R.p_pos = ctx->d_pos;
   R.p_vel = ctx->d_vel;
   R.p_mass = ctx->d_mass;
@@ -965,6 +935,12 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
     R.fac_ps[t] = ctx->prm.fac_value_ps[t];
   }
   R.status = ctx->d_status;
+  return R;
+}
+
+// the 2 * count old / trial orbits of make_rep_args' particles
+OrbitBatch make_rep_batch(galic_ctx *ctx, int count)
+{
   OrbitBatch b;
   b.count = 2 * count;
   b.pos = ctx->d_b_pos;
@@ -979,25 +955,169 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
   b.egy_err = ctx->d_b_err;
   b.status = ctx->d_b_status;
   b.with_egy = 1;
-  ctx->last_launches = form == GALIC_FORM_FP32 ? launch_rep(ctx->dm, R, f, b, s, ctx->d_tab32, ctx->d_cellsize32)
-                                               : launch_rep(ctx->dm, R, f, b, s);
-  CK(cudaMemcpyAsync(h + off_st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(h + off_ost, ctx->d_b_status, 2 * (size_t) count * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(h + off_steps, ctx->d_b_steps, 2 * (size_t) count * sizeof(long long), cudaMemcpyDeviceToHost,
-                     s));
-  CK(cudaStreamSynchronize(s));
-  CK(cudaGetLastError());
+  return b;
+}
+
+// uploads `count` particle indices and clears the status words; returns the
+// pinned staging block (status, per-orbit status and steps are read back
+// into it by finish_rep_window), or null
+char *begin_rep_window(galic_ctx *ctx, const int *idx, int count, size_t *off_st, size_t *off_ost, size_t *off_steps)
+{
+  cudaStream_t s = ctx->stream;
+  *off_st = ((size_t) count * sizeof(int) + 15) & ~(size_t) 15;
+  *off_ost = *off_st + 16;
+  *off_steps = (*off_ost + 2 * (size_t) count * sizeof(int) + 15) & ~(size_t) 15;
+  char *h = stage(ctx, *off_steps + 2 * (size_t) count * sizeof(long long));
+  if(!h) return nullptr;
+  std::memcpy(h, idx, count * sizeof(int));
+  if(cudaMemcpyAsync(ctx->d_idx, h, count * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s) != cudaSuccess ||
+     cudaMemsetAsync(ctx->d_b_status, 0, 2 * (size_t) count * sizeof(int), s) != cudaSuccess)
+    return nullptr;
+  return h;
+}
+
+// waits for the window's work; adds its orbit-steps to *steps; returns the
+// worst status of the window
+int finish_rep_window(galic_ctx *ctx, char *h, int count, size_t off_st, size_t off_ost, size_t off_steps,
+                      long long *steps)
+{
+  cudaStream_t s = ctx->stream;
+  if(cudaMemcpyAsync(h + off_st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+     cudaMemcpyAsync(h + off_ost, ctx->d_b_status, 2 * (size_t) count * sizeof(int), cudaMemcpyDeviceToHost, s) !=
+         cudaSuccess ||
+     cudaMemcpyAsync(h + off_steps, ctx->d_b_steps, 2 * (size_t) count * sizeof(long long), cudaMemcpyDeviceToHost,
+                     s) != cudaSuccess ||
+     cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return GALIC_ERR_CUDA;
   int status;
   std::memcpy(&status, h + off_st, sizeof(int));
   const int *ost = (const int *) (h + off_ost);
-  const long long *steps = (const long long *) (h + off_steps);
-  long long tot = 0;
+  const long long *st = (const long long *) (h + off_steps);
   for(int k = 0; k < 2 * count; k++) {
-    tot += steps[k];
+    *steps += st[k];
     if(ost[k] == ORBIT_STEP_CAP) status = std::max(status, (int) GALIC_ERR_STEP_CAP);
   }
+  return status;
+}
+
+}  // namespace
+
+extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial,
+                                  int form)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(!ctx->have_response) return fail(ctx, GALIC_ERR_STATE);
+  if(form == GALIC_FORM_FP32) {
+    int st = ensure_tab32(ctx);
+    if(st) return st;
+  }
+  if(count < 0 || (count > 0 && !idx)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  // every particle at most once per repetition: the reference evaluates a
+  // repetition against committed state and P[n] only changes for n itself
+  std::vector<char> seen(ctx->n, 0);
+  for(int k = 0; k < count; k++) {
+    if(idx[k] < 0 || idx[k] >= ctx->n || seen[idx[k]]) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+    seen[idx[k]] = 1;
+  }
+  cudaStream_t s = ctx->stream;
+  FitArgs f = make_fit_args(ctx);
+  if(count == 0) {  // init_updates + commit_updates with no particle: only the fit
+    ctx->last_launches = launch_global_fit(f, s);
+    CK(cudaStreamSynchronize(s));
+    return fail(ctx, GALIC_OK);
+  }
+  int st = ensure_rep_scratch(ctx, count);
+  if(st) return st;
+  size_t off_st, off_ost, off_steps;
+  char *h = begin_rep_window(ctx, idx, count, &off_st, &off_ost, &off_steps);
+  if(!h) return fail(ctx, GALIC_ERR_CUDA);
+  RepArgs R = make_rep_args(ctx, count, seed, rep_serial, 0);
+  OrbitBatch b = make_rep_batch(ctx, count);
+  ctx->last_launches = form == GALIC_FORM_FP32 ? launch_rep(ctx->dm, R, f, b, s, ctx->d_tab32, ctx->d_cellsize32)
+                                               : launch_rep(ctx->dm, R, f, b, s);
+  long long tot = 0;
+  int status = finish_rep_window(ctx, h, count, off_st, off_ost, off_steps, &tot);
   ctx->last_steps = tot;
   if(status) return fail(ctx, status);
+  return fail(ctx, GALIC_OK);
+}
+
+extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, int reps, uint64_t seed,
+                                   uint32_t rep_serial, int form, size_t window_bytes)
+{
+  if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
+  if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(!ctx->have_response) return fail(ctx, GALIC_ERR_STATE);
+  if(count < 0 || reps < 0 || (count > 0 && reps > 0 && !idx)) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+  if(form == GALIC_FORM_FP32) {
+    int st = ensure_tab32(ctx);
+    if(st) return st;
+  }
+  // each repetition's particles distinct and in range (as galic_optimize_rep)
+  std::vector<int> last_rep(ctx->n, -1);
+  for(int r = 0; r < reps; r++)
+    for(int k = 0; k < count; k++) {
+      const int n = idx[(size_t) r * count + k];
+      if(n < 0 || n >= ctx->n || last_rep[n] == r) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
+      last_rep[n] = r;
+    }
+  cudaStream_t s = ctx->stream;
+  FitArgs f = make_fit_args(ctx);
+  int launches = 0;
+  if(count == 0) {
+    for(int r = 0; r < reps; r++) launches += launch_global_fit(f, s);
+    CK(cudaStreamSynchronize(s));
+    ctx->last_launches = launches;
+    ctx->last_steps = 0;
+    return fail(ctx, GALIC_OK);
+  }
+  // per optimised particle: two orbits' dense grids plus their small arrays
+  const size_t per_particle = 2 * ((size_t) NF_ORBIT * ctx->G * sizeof(double) + 128);
+  if(window_bytes == 0) window_bytes = (size_t) 4 << 30;
+  std::fill(last_rep.begin(), last_rep.end(), -1);
+  long long tot = 0;
+  int r0 = 0;
+  while(r0 < reps) {
+    // the window [r0, r1): its repetitions' particles all distinct (the old
+    // orbit of a particle optimised twice would depend on the first
+    // outcome) and its grids within window_bytes (at least one repetition)
+    int r1 = r0;
+    while(r1 < reps) {
+      if(r1 > r0 && (size_t) (r1 - r0 + 1) * count * per_particle > window_bytes) break;
+      bool repeat = false;
+      for(int k = 0; k < count && !repeat; k++) repeat = last_rep[idx[(size_t) r1 * count + k]] >= r0;
+      if(repeat && r1 > r0) break;
+      for(int k = 0; k < count; k++) last_rep[idx[(size_t) r1 * count + k]] = r1;
+      r1++;
+    }
+    const int W = r1 - r0, M = W * count;
+    int st = ensure_rep_scratch(ctx, M);
+    if(st) return st;
+    size_t off_st, off_ost, off_steps;
+    char *h = begin_rep_window(ctx, idx + (size_t) r0 * count, M, &off_st, &off_ost, &off_steps);
+    if(!h) return fail(ctx, GALIC_ERR_CUDA);
+    // the old and trial orbits of the whole window in one launch (a
+    // proposal depends only on P[n].Pos, the targets and its stream, the old
+    // orbit on P[n].Vel, which only n's own optimisation changes) ...
+    RepArgs R = make_rep_args(ctx, M, seed, rep_serial + (uint32_t) r0, count);
+    OrbitBatch b = make_rep_batch(ctx, M);
+    launches += form == GALIC_FORM_FP32 ? launch_rep_orbits(ctx->dm, R, b, s, ctx->d_tab32, ctx->d_cellsize32)
+                                        : launch_rep_orbits(ctx->dm, R, b, s);
+    // ... then each repetition's evaluation against the state its
+    // predecessors committed, acceptance and commit, in order
+    for(int w = 0; w < W; w++) launches += launch_rep_commit(ctx->dm, rep_slice(R, w * count, count, ctx->G), f, s);
+    int status = finish_rep_window(ctx, h, M, off_st, off_ost, off_steps, &tot);
+    if(status) {
+      ctx->last_steps = tot;
+      ctx->last_launches = launches;
+      return fail(ctx, status);
+    }
+    r0 = r1;
+  }
+  ctx->last_steps = tot;
+  ctx->last_launches = launches;
   return fail(ctx, GALIC_OK);
 }
 

@@ -114,7 +114,8 @@ __global__ void k_propose(DevModel M, RepArgs R)
   const int tovs = M.tovs[type];
   const double *pos = &R.p_pos[3 * n];
   grng_t g;
-  grng_init(&g, R.seed, (uint32_t) n, R.rep_serial);
+  // repetition k / per_rep of a window of repetitions draws from its own serial
+  grng_init(&g, R.seed, (uint32_t) n, R.rep_serial + (uint32_t) (R.per_rep > 0 ? k / R.per_rep : 0));
   (void) grng_uniform(&g);  // dir_rnd (main.c:370)
   double phi = gm_atan2(pos[1], pos[0]);
   double Rv[3], Tv[3], Qv[3];
@@ -354,26 +355,55 @@ int launch_global_fit(const FitArgs &f, cudaStream_t s)
   return 3;
 }
 
-int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s,
-               const float4 *const *quad32, const float *cellsize32)
+int launch_rep_orbits(const DevModel &M, const RepArgs &R, const OrbitBatch &b, cudaStream_t s,
+                      const float4 *const *quad32, const float *cellsize32)
 {
-  int launches = 0;
   const int count = R.count;
   k_propose<<<(count + 63) / 64, 64, 0, s>>>(M, R);
-  launches++;
   cudaMemsetAsync(b.grids, 0, (size_t) b.count * NF_ORBIT * M.DG_Ngrid * sizeof(double), s);
   if(quad32)
     launch_orbits_dense_fp32(M, quad32, cellsize32, b, s);
   else
     launch_orbits_dense(M, b, s);
   launch_scale_dense(M, b, s);
-  launches += 2;
+  return 3;
+}
+
+int launch_rep_commit(const DevModel &M, const RepArgs &R, const FitArgs &f, cudaStream_t s)
+{
+  const int count = R.count;
   size_t smem = (size_t) f.Nstack * sizeof(double);
   k_eval_fit<<<2 * count, 256, smem, s>>>(M, R, f);
   k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R);
   k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
   k_inst_delta<<<148 * 8, 256, 0, s>>>(R, f);
-  launches += 4;
-  launches += launch_global_fit(f, s);
-  return launches;
+  return 4 + launch_global_fit(f, s);
+}
+
+RepArgs rep_slice(const RepArgs &R, int first, int count, int G)
+{
+  RepArgs S = R;
+  S.count = count;
+  S.per_rep = 0;
+  S.idx = R.idx + first;
+  S.b_pos = R.b_pos + 3 * (size_t) (2 * first);
+  S.b_vel = R.b_vel + 3 * (size_t) (2 * first);
+  S.b_mass = R.b_mass + 2 * (size_t) first;
+  S.b_time = R.b_time + 2 * (size_t) first;
+  S.b_type = R.b_type + 2 * (size_t) first;
+  S.b_norbit = R.b_norbit + 2 * (size_t) first;
+  S.grids = R.grids + (size_t) (2 * first) * NF_ORBIT * G;
+  S.vel_try = R.vel_try + 3 * (size_t) first;
+  S.F = R.F + 2 * (size_t) first;
+  S.accepted = R.accepted + first;
+  S.inst_v = R.inst_v + 4 * (size_t) first;
+  S.inst_cell = R.inst_cell + first;
+  return S;
+}
+
+int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s,
+               const float4 *const *quad32, const float *cellsize32)
+{
+  const int launches = launch_rep_orbits(M, R, b, s, quad32, cellsize32);
+  return launches + launch_rep_commit(M, R, f, s);
 }

@@ -39,7 +39,8 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
   __syncwarp();
 }
 
-// FP32 variant.  A lane parks one record per grid node that leaves its
+// Node-record variant (the FP32 form, and the FP64 form's batched kernel
+// with FP64 sums).  A lane parks one record per grid node that leaves its
 // accumulators: the node's index and its five sums.  The drain scales them
 // by value x 2^(shift-24) in FP32 (the orbit's mass/Tint and the field's
 // fixed-point scale folded into one FP32 factor per field class when the
@@ -56,17 +57,21 @@ __device__ __forceinline__ void warp_drain(WarpQueue &q, unsigned full, FxWord *
 // The drain compacts all lanes' records and every lane adds the five words of
 // one record at a time, so the global atomics run on full warps.  PER is
 // chosen per block size so that the queues fit the static shared memory.
-template <int PER_>
-struct WarpQueue32 {
+template <int PER_, class T>
+struct WarpQueueT {
   static constexpr int PER = PER_;
-  int base[PER][32];      // the node's index in its grid (field f of the orbit's set: gbase + f * Ngrid + base)
-  float val[PER][5][32];  // the node's five sums
-  int off[32];            // drain: first compacted record of each lane
-  int gbase[32];          // per lane: first word of its orbit's grid set
-  float2 scale[32];       // per lane: {mass field, energy fields} fixed-point factors
+  int base[PER][32];  // the node's index in its grid (field f of the orbit's set: gbase + f * Ngrid + base)
+  T val[PER][5][32];  // the node's five sums
+  int off[32];        // drain: first compacted record of each lane
+  int gbase[32];      // per lane: first word of its orbit's grid set
+  T scale[2][32];     // per lane: {mass field, energy fields} fixed-point factors
+                      // (the exact drain: scale[0] = mass/Tint)
+  int shift[2][32];   // the exact drain: per lane {mass field, energy fields} shifts
 };
+template <int PER>
+using WarpQueue32 = WarpQueueT<PER, float>;
 
-// records per lane of a block of BLOCK threads
+// records per lane of a block of BLOCK threads (FP32 sums)
 __host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 8 : (block <= 192 ? 7 : 5); }
 
 // true when some lane could not park another cell's nodes
@@ -76,10 +81,13 @@ __device__ __forceinline__ bool queue32_due(int cnt)
   return __any_sync(0xffffffffu, cnt > PER - 4);
 }
 
+__device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
+__device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
+
 // all 32 lanes call this at the same point of the loop with their record
 // counts; cnt is 0 on return
-template <int PER>
-__device__ __forceinline__ void warp_drain32(WarpQueue32<PER> &q, FxWord *fx, int G, int &cnt)
+template <int PER, class T>
+__device__ __forceinline__ void warp_drain_nodes(WarpQueueT<PER, T> &q, FxWord *fx, int G, int &cnt)
 {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -100,15 +108,55 @@ __device__ __forceinline__ void warp_drain32(WarpQueue32<PER> &q, FxWord *fx, in
       if(q.off[L + step] <= r) L += step;
     const int k = r - q.off[L];
     const int b = q.gbase[L] + q.base[k][L];
-    const float2 sc = q.scale[L];
+    const T sm = q.scale[0][L], se = q.scale[1][L];
 #pragma unroll
     for(int f = 0; f < 5; f++) {
-      const long long X = __float2ll_rn(q.val[k][f][L] * (f == 0 ? sc.x : sc.y));
+      const long long X = to_fixed(q.val[k][f][L] * (f == 0 ? sm : se));
       if(X) atomicAdd(&fx[b + f * G].hi, (unsigned long long) X);
     }
   }
   __syncwarp();
   cnt = 0;
+}
+
+// Exact variant (FP64 sums): every value v = sum x mass/Tint is added as the
+// two-word fixed-point pair of fixedpoint.cuh:fx_add (resolution 2^-S, two
+// integer atomics), so the bins carry the full FP64 resolution whatever the
+// headroom of the field's range.
+template <int PER>
+__device__ __forceinline__ void warp_drain_nodes_exact(WarpQueueT<PER, double> &q, FxWord *fx, int G, int &cnt)
+{
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int incl = cnt;
+#pragma unroll
+  for(int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if(lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(FULL, incl, 31);
+  q.off[lane] = incl - cnt;
+  __syncwarp();
+  for(int r = lane; r < total; r += 32) {
+    int L = 0;
+#pragma unroll
+    for(int step = 16; step; step >>= 1)
+      if(q.off[L + step] <= r) L += step;
+    const int k = r - q.off[L];
+    const int b = q.gbase[L] + q.base[k][L];
+    const double fac = q.scale[0][L];
+    const int sm = q.shift[0][L], se = q.shift[1][L];
+#pragma unroll
+    for(int f = 0; f < 5; f++) fx_add(&fx[b + f * G], q.val[k][f][L] * fac, f == 0 ? sm : se);
+  }
+  __syncwarp();
+  cnt = 0;
+}
+
+template <int PER>
+__device__ __forceinline__ void warp_drain32(WarpQueue32<PER> &q, FxWord *fx, int G, int &cnt)
+{
+  warp_drain_nodes(q, fx, G, cnt);
 }
 
 #endif

@@ -184,15 +184,16 @@ GM_HD double gm_atan2(double y, double x)
   }
   if(ay == GM_INF) return gm_copysign(pio2_hi, y);
 
-  double a;
-  if(ay > ax) {
-    double t = ax / ay;
-    a = (pio2_hi - gm_atan_unit(t)) + pio2_lo;
-  } else {
-    double t = ay / ax;
-    a = gm_atan_unit(t);
-  }
-  if(xneg) a = (pi_hi - a) + pi_lo;
+  /* t = min/max: ax/ay when ay > ax, else ay/ax (one division, one
+   * atan_unit for every lane of a warp; the result does not depend on how
+   * the choice is compiled) */
+  const int swap = ay > ax;
+  double t = (swap ? ax : ay) / (swap ? ay : ax);
+  double a = gm_atan_unit(t);
+  double b = (pio2_hi - a) + pio2_lo;
+  a = swap ? b : a;
+  double c = (pi_hi - a) + pi_lo;
+  a = xneg ? c : a;
   return gm_copysign(a, y);
 }
 
@@ -263,6 +264,30 @@ GM_HD double gm_cos(double x)
     case 2: return -gm_cos_poly(r);
     default: return gm_sin_poly(r);
   }
+}
+
+/* sin and cos of one argument: one reduction, both polynomials and the
+ * quadrant's signs by selection, so a warp whose lanes sit in different
+ * quadrants evaluates each polynomial once; *s and *c equal gm_sin(x) and
+ * gm_cos(x) bit for bit */
+GM_HD void gm_sincos(double x, double *s, double *c)
+{
+  if(gm_isnan(x) || gm_fabs(x) == GM_INF) {
+    *s = GM_NAN;
+    *c = GM_NAN;
+    return;
+  }
+  if(gm_fabs(x) < 0x1.0p-27) {
+    *s = x;
+    *c = 1.0;
+    return;
+  }
+  double r;
+  const int q = gm_reduce_pio2(x, &r);
+  const double ps = gm_sin_poly(r), pc = gm_cos_poly(r);
+  const double sv = (q & 1) ? pc : ps, cv = (q & 1) ? ps : pc;
+  *s = (q & 2) ? -sv : sv;            /* quadrants 2, 3: -sin, -cos poly */
+  *c = ((q + 1) & 2) ? -cv : cv;      /* quadrants 1, 2: -sin, -cos poly */
 }
 
 /* ---------------------------------------------------------------- exp */

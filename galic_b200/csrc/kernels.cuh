@@ -18,7 +18,9 @@ enum { NG_COMMITTED = 10 };
 #define CALC_ALL_BLOCK_FP64 128
 #define CALC_ALL_BLOCK_FP32 128
 #ifndef GALIC_FP64_MIN_BLOCKS
-#define GALIC_FP64_MIN_BLOCKS 3
+// 4 CTAs of 128 threads per SM (128 registers, a few spilled) ran the
+// halo + disk pass 10 % faster than 3 CTAs at 156 registers
+#define GALIC_FP64_MIN_BLOCKS 4
 #endif
 #ifndef GALIC_FP32_MIN_BLOCKS
 #define GALIC_FP32_MIN_BLOCKS 4

@@ -126,8 +126,10 @@ __device__ __forceinline__ void forcegrid_acc(const DevModel &M, const FgCoord &
       double accz = t00.y * (1 - ifac) * (1 - jfac) + t01.y * (1 - ifac) * jfac + t10.y * ifac * (1 - jfac) +
                     t11.y * ifac * jfac;
       if(pos[2] < 0) accz = -accz;
-      acc[0] = accR * gm_cos(phi);
-      acc[1] = accR * gm_sin(phi);
+      double sp, cp;
+      gm_sincos(phi, &sp, &cp);  // gm_sin(phi), gm_cos(phi)
+      acc[0] = accR * cp;
+      acc[1] = accR * sp;
       acc[2] = accz;
     } else {
       halo_acc(M, pos, acc);
@@ -412,7 +414,9 @@ __device__ __forceinline__ void disp_components(const DevModel &M, const LogCons
   if(tovs == 0 || tovs == 1 || tovs == 3) {
     double phi = gm_atan2(pos[1], pos[0]);
     double theta = gm_acos(pos[2] / sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]));
-    double st = gm_sin(theta), ct = gm_cos(theta), sp = gm_sin(phi), cp = gm_cos(phi);
+    double st, ct, sp, cp;
+    gm_sincos(theta, &st, &ct);
+    gm_sincos(phi, &sp, &cp);
     double er0 = st * cp, er1 = st * sp, er2 = ct;
     double ep0 = -sp, ep1 = cp, ep2 = 0;
     double et0 = -ct * cp, et1 = -ct * sp, et2 = st;
@@ -427,7 +431,8 @@ __device__ __forceinline__ void disp_components(const DevModel &M, const LogCons
     out[3] = vphi * vphi;
   } else if(tovs == 2) {
     double phi = gm_atan2(pos[1], pos[0]);
-    double cp = gm_cos(phi), sp = gm_sin(phi);
+    double cp, sp;
+    gm_sincos(phi, &sp, &cp);
     double eR0 = cp, eR1 = sp, eR2 = 0;
     double ep0 = -sp, ep1 = cp, ep2 = 0;
     double ez0 = 0, ez1 = 0, ez2 = 1;

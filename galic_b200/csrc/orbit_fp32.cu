@@ -234,7 +234,8 @@ struct Sink32 : NodeAcc {
   __device__ __forceinline__ void set_orbit(int gbase, float scale_m, float scale_e)
   {
     q->gbase[lane] = gbase;
-    q->scale[lane] = make_float2(scale_m, scale_e);
+    q->scale[0][lane] = scale_m;
+    q->scale[1][lane] = scale_e;
   }
   __device__ __forceinline__ void park_masked(const bool out[4])
   {

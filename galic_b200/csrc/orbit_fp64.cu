@@ -6,9 +6,9 @@
 //  k_scale_dense    the mass/tall normalisation (orbit_response.c:475-486).
 //  k_calc_all_fp64  calc_all_response_fields (main.c:151-231): persistent
 //                   threads pull orbits from a work counter; deposits of
-//                   consecutive steps in the same cell are merged in
-//                   registers and flushed as exact fixed-point atomics into
-//                   the per-type grids.
+//                   consecutive steps are summed per grid node in registers
+//                   and flushed as exact fixed-point atomics into the
+//                   per-type grids when their node leaves the orbit's cell.
 //  k_instantaneous  calc_disp_components_for_particle + add_to_energy_grid
 //                   (main.c:226-229).
 //  k_fx_finalize    fixed-point words -> FP64 committed grids.
@@ -86,41 +86,96 @@ __global__ void k_scale_dense(OrbitBatch b, int G)
   }
 }
 
-// Register-merged sink of the batched path: deposits of consecutive steps in
-// the same cell are summed in registers; on a cell change the 20 sums are
-// scaled by mass/Tint and parked in the lane's slot of the warp queue, which
-// the whole warp drains into the fixed-point grids (flush.cuh).
-struct QueueSink {
-  WarpQueue *q;
-  int lane, type, Nb;
-  double fac;  // mass / timespan
-  int cur;     // merged cell iz*Nb+iR, -1 if none
-  bool parked;
+// Node sink of the batched path.  The deposits of consecutive steps are
+// summed per grid NODE in FP64 registers: node (z, r) lives in accumulator
+// slot ((z & 1) << 1) | (r & 1), so the four nodes of any cell have the four
+// parities, and when the orbit moves to a neighbouring cell the nodes the two
+// cells share stay in place.  Only the slots whose node leaves are parked, as
+// records {node index, 5 sums}, in the lane's column of the warp's queue; the
+// warp drains all lanes' records together (flush.cuh:warp_drain_nodes_exact),
+// each value scaled by mass/Tint and added as an exact two-word fixed-point
+// pair (order independent).
+template <int PER>
+struct NodeSink64 {
+  WarpQueueT<PER, double> *q;
+  int lane, Nb;
+  int cnt;  // records parked in this lane's column since the last drain
+  int cur, cur_iR, cur_iz;
   double a[4][5];
+  __device__ __forceinline__ void set_orbit(int gbase, double fac, int shift_m, int shift_e)
+  {
+    q->gbase[lane] = gbase;
+    q->scale[0][lane] = fac;
+    q->shift[0][lane] = shift_m;
+    q->shift[1][lane] = shift_e;
+    cur = -1;
+  }
+  // slot s of cell (iz, iR) holds node (iz + node_dz(s, iz), iR + node_dr(s, iR))
+  __device__ __forceinline__ static int node_dz(int s, int iz) { return ((s >> 1) ^ iz) & 1; }
+  __device__ __forceinline__ static int node_dr(int s, int iR) { return (s ^ iR) & 1; }
+  __device__ __forceinline__ void park_masked(const bool out[4])
+  {
+    // record positions first, then predicated stores: straight-line code
+    // for every lane of the warp
+    bool rec[4];
+    int at[4], k = cnt;
+#pragma unroll
+    for(int s = 0; s < 4; s++) {
+      rec[s] = out[s] && a[s][0] != 0.0;  // a node without mass has no deposit at all
+      at[s] = k;
+      k += rec[s] ? 1 : 0;
+    }
+#pragma unroll
+    for(int s = 0; s < 4; s++) {
+      if(rec[s]) {
+        q->base[at[s]][lane] = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
+#pragma unroll
+        for(int f = 0; f < 5; f++) q->val[at[s]][f][lane] = a[s][f];
+      }
+    }
+    cnt = k;
+  }
   __device__ __forceinline__ void park()
   {
     if(cur < 0) return;
-#pragma unroll
-    for(int c = 0; c < 4; c++)
-#pragma unroll
-      for(int f = 0; f < 5; f++) q->val[lane][c * 5 + f] = a[c][f] * fac;
-    q->cell[lane] = cur;
-    q->type[lane] = type;
-    parked = true;
+    const bool all[4] = {true, true, true, true};
+    park_masked(all);
     cur = -1;
+  }
+  __device__ __forceinline__ void move_to(int iR, int iz)
+  {
+    bool out[4];
+    if(cur >= 0) {
+      // along one axis a move by d leaves the node whose parity is that of
+      // the boundary left behind, both nodes when |d| > 1, none when d = 0
+      const int dz = iz - cur_iz, dr = iR - cur_iR;
+      const int bz = (dz > 0 ? cur_iz : cur_iz + 1) & 1, br = (dr > 0 ? cur_iR : cur_iR + 1) & 1;
+      const bool zall = dz > 1 || dz < -1, rall = dr > 1 || dr < -1;
+#pragma unroll
+      for(int s = 0; s < 4; s++)
+        out[s] = (zall || (dz != 0 && (s >> 1) == bz)) || (rall || (dr != 0 && (s & 1) == br));
+      park_masked(out);
+    } else {
+#pragma unroll
+      for(int s = 0; s < 4; s++) out[s] = true;
+    }
+#pragma unroll
+    for(int s = 0; s < 4; s++)
+#pragma unroll
+      for(int f = 0; f < 5; f++) a[s][f] = out[s] ? 0.0 : a[s][f];
+    cur = iz * Nb + iR;
+    cur_iR = iR;
+    cur_iz = iz;
   }
   __device__ __forceinline__ void operator()(const Deposit &d)
   {
-    int c = d.iz * Nb + d.iR;
-    if(c != cur) {
-      park();
-#pragma unroll
-      for(int k = 0; k < 4; k++)
-#pragma unroll
-        for(int f = 0; f < 5; f++) a[k][f] = 0;
-      cur = c;
-    }
-    const double w[4] = {d.m00, d.m10, d.m01, d.m11};
+    if(d.iz * Nb + d.iR != cur) move_to(d.iR, d.iz);
+    // slot s holds corner (dz, dr) = ((s >> 1) ^ (iz & 1), (s & 1) ^ (iR & 1));
+    // corner weights: (0,0) m00, (0,1) m10, (1,0) m01, (1,1) m11
+    const bool oz = d.iz & 1, orr = d.iR & 1;
+    const double z0r0 = oz ? d.m01 : d.m00, z0r1 = oz ? d.m11 : d.m10;  // slot z-parity 0: dz = oz
+    const double z1r0 = oz ? d.m00 : d.m01, z1r1 = oz ? d.m10 : d.m11;
+    const double w[4] = {orr ? z0r1 : z0r0, orr ? z0r0 : z0r1, orr ? z1r1 : z1r0, orr ? z1r0 : z1r1};
 #pragma unroll
     for(int k = 0; k < 4; k++) {
       a[k][0] += w[k];
@@ -139,20 +194,24 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
   atomicMax((unsigned long long *) addr, (unsigned long long) __double_as_longlong(v));
 }
 
-enum LaneState { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2 };
+enum LaneState { LANE_ACTIVE = 0, LANE_FINISH = 1, LANE_DONE = 2, LANE_START = 3 };
 
-__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevModel M, CalcAllArgs A)
+// records per lane of the FP64 queue (FP64 sums: 40 B per record and lane)
+constexpr int kPer64 = 8;
+
+template <int MINB>
+__global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(DevModel M, CalcAllArgs A)
 {
-  __shared__ WarpQueue queues[CALC_ALL_BLOCK_FP64 / 32];
+  __shared__ WarpQueueT<kPer64, double> queues[CALC_ALL_BLOCK_FP64 / 32];
   LogConsts L = make_log_consts(M);
   const int G = M.DG_Ngrid;
   OrbitState s;
-  QueueSink sink;
+  NodeSink64<kPer64> sink;
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
   sink.Nb = M.DG_Nbin;
   sink.cur = -1;
-  sink.parked = false;
+  sink.cnt = 0;
   int p = -1;
   unsigned long long my_steps = 0;
   double my_err = 0;
@@ -167,22 +226,23 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevMod
     }
     k = A.first + k * A.stride;
     p = A.order ? A.order[k] : k;
-    int type = A.type[p];
-    sink.type = type;
-    sink.fac = A.mass[p] / A.tint[p];
-    sink.cur = -1;
+    const int type = A.type[p];
+    const double fac = A.mass[p] / A.tint[p];
+    sink.set_orbit(type * NG_COMMITTED * G, fac, A.shift[type * NG_COMMITTED + GALIC_GRID_MASS_S],
+                   A.shift[type * NG_COMMITTED + GALIC_GRID_R_S]);
     orbit_begin(M, L, s, &A.pos[3 * p], &A.vel[3 * p], A.tint[p], type, true);
     return true;
   };
 
   int state = fetch() ? LANE_ACTIVE : LANE_DONE;
   for(;;) {
-    const unsigned full = __ballot_sync(0xffffffffu, sink.parked);
-    if(full) {
-      warp_drain(*sink.q, full, A.fx, A.shift, G, M.DG_Nbin);
-      sink.parked = false;
-    }
-    if(!__any_sync(0xffffffffu, state != LANE_DONE)) break;
+    const bool all_done = !__any_sync(0xffffffffu, state != LANE_DONE);
+    // records take the orbit's grid set and scale from the lane's queue
+    // header: a lane's records are drained before it starts the next orbit
+    if(queue32_due<kPer64>(sink.cnt) ||
+       __any_sync(0xffffffffu, (all_done || state == LANE_START) && sink.cnt > 0))
+      warp_drain_nodes_exact(*sink.q, A.fx, G, sink.cnt);
+    if(all_done) break;
     if(state == LANE_ACTIVE) {
       if(!orbit_step(M, L, s, true, sink)) state = LANE_FINISH;
     } else if(state == LANE_FINISH) {
@@ -195,6 +255,8 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, 3) k_calc_all_fp64(DevMod
         double e = orbit_energy_error(M, L, s);
         if(e > my_err) my_err = e;
       }
+      state = LANE_START;
+    } else if(state == LANE_START) {
       state = fetch() ? LANE_ACTIVE : LANE_DONE;
     }
   }
@@ -263,13 +325,13 @@ void launch_scale_dense(const DevModel &M, const OrbitBatch &b, cudaStream_t s)
 int calc_all_occupancy(int block)
 {
   int blocks = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_calc_all_fp64, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_calc_all_fp64<GALIC_FP64_MIN_BLOCKS>, block, 0);
   return blocks;
 }
 
 int launch_calc_all_fp64(const DevModel &M, const CalcAllArgs &a, int grid, int block, cudaStream_t s)
 {
-  k_calc_all_fp64<<<grid, block, 0, s>>>(M, a);
+  k_calc_all_fp64<GALIC_FP64_MIN_BLOCKS><<<grid, block, 0, s>>>(M, a);
   return 1;
 }
 

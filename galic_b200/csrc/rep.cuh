@@ -11,6 +11,9 @@ struct RepArgs {
   const int *idx;  // particles optimised in this repetition
   uint64_t seed;
   uint32_t rep_serial;
+  // particles per repetition when idx spans a window of repetitions
+  // (particle k draws from stream serial rep_serial + k / per_rep); 0: one
+  int per_rep = 0;
   // particle state P[] (device)
   const double *p_pos;
   double *p_vel;
@@ -35,5 +38,14 @@ struct RepArgs {
 // quad32/cellsize32 non-null: the orbits of the repetition in the FP32 form
 int launch_rep(const DevModel &M, const RepArgs &R, const FitArgs &f, const OrbitBatch &b, cudaStream_t s,
                const float4 *const *quad32 = nullptr, const float *cellsize32 = nullptr);
+// the two halves of launch_rep: proposals and the old/trial orbits of R.count
+// particles (which may span several repetitions, see per_rep), then the
+// evaluation, acceptance and commit of ONE repetition whose arrays R points at
+int launch_rep_orbits(const DevModel &M, const RepArgs &R, const OrbitBatch &b, cudaStream_t s,
+                      const float4 *const *quad32 = nullptr, const float *cellsize32 = nullptr);
+int launch_rep_commit(const DevModel &M, const RepArgs &R, const FitArgs &f, cudaStream_t s);
+// R restricted to the `count` particles of window positions first ..
+// first + count - 1 (G: bins per grid)
+RepArgs rep_slice(const RepArgs &R, int first, int count, int G);
 
 #endif

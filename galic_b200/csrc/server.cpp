@@ -53,6 +53,22 @@ double sall(const double *fit)
   return s;
 }
 
+// particles optimised per repetition (main.c:128 with NTask = 1)
+size_t job_count(const galic_job_t &d)
+{
+  return std::min((size_t) d.n, (size_t) (1 + d.fraction_per_rep * d.n));
+}
+
+// device bytes of the per-orbit grids of one window of repetitions: the
+// whole iteration, capped at 1 GiB (at least one repetition)
+size_t job_window_bytes(const galic_job_t &d)
+{
+  const size_t G = (size_t) 1 << (2 * d.prm->DG_MaxLevel);
+  const size_t per_rep = job_count(d) * 2 * (5 * G * 8 + 128);
+  const size_t iter = per_rep * (size_t) std::max(d.reps_per_iteration, 1);
+  return std::max(per_rep, std::min(iter, (size_t) 1 << 30));
+}
+
 int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const std::function<double()> &now)
 {
   galic_ctx *ctx = nullptr;
@@ -82,19 +98,25 @@ int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const 
   // optimize_some_particles (main.c:120-146): n_per_cpu from the fraction,
   // a cursor through the permutation that persists across repetitions
   const int n_per = std::min(d.n, (int) (1 + d.fraction_per_rep * d.n));
-  std::vector<int> idx(n_per);
+  // one iteration's repetitions in one call: their orbits run in windows of
+  // repetitions (galic_optimize_reps), the repetitions commit in order
+  std::vector<int> idx((size_t) n_per * std::max(d.reps_per_iteration, 0));
+  const size_t window = job_window_bytes(d);
   int cursor = 0;
   uint32_t rep_serial = 0;
   for(int it = 0; it < d.max_iterations; it++) {
     const double before = r.sall_last;
-    for(int rep = 0; rep < d.reps_per_iteration; rep++) {
-      for(int i = 0; i < n_per; i++, cursor++) {
-        if(cursor >= d.n) cursor = 0;
-        idx[i] = d.permutation ? d.permutation[cursor] : cursor;
-      }
-      if((st = galic_optimize_rep(ctx, idx.data(), n_per, d.seed, rep_serial++, d.form))) return done(st);
+    for(size_t i = 0; i < idx.size(); i++, cursor++) {
+      if(cursor >= d.n) cursor = 0;
+      idx[i] = d.permutation ? d.permutation[cursor] : cursor;
+    }
+    if(d.reps_per_iteration > 0) {
+      if((st = galic_optimize_reps(ctx, idx.data(), n_per, d.reps_per_iteration, d.seed, rep_serial, d.form,
+                                   window)))
+        return done(st);
       r.orbit_steps += galic_last_orbit_steps(ctx);
-      r.reps++;
+      rep_serial += (uint32_t) d.reps_per_iteration;
+      r.reps += d.reps_per_iteration;
     }
     galic_get_fit(ctx, fit);
     r.sall_last = sall(fit);
@@ -176,11 +198,10 @@ extern "C" size_t galic_job_device_bytes(const galic_job_t *job)
   const size_t NF = (size_t) p.FG_Nbin * p.FG_Nbin;
   const size_t G = (size_t) 1 << (2 * p.DG_MaxLevel);
   const size_t Ns = (((size_t) 1 << (2 + 2 * p.DG_MaxLevel)) - 1) / 3;
-  const size_t count = std::min(n, (size_t) (1 + job->fraction_per_rep * job->n));
   size_t b = n * 160;                       // particle state (allvars.h:844-868) and processing order
   b += NF * (16 + 8 + 3 * 8 + 3 * 64);      // FP64 force tables, streaming velocities, FP32 quad tables
   b += G * (8 + 4 + 320 + 640) + Ns * 520;  // geometry, committed grids, fixed point, stacks, targets
-  b += count * 2 * (5 * G * 8 + 128);       // per-orbit grids of a repetition
+  b += job_window_bytes(*job) + job_count(*job) * 64;  // per-orbit grids of a window of repetitions
   b += (size_t) 16 << 20;                   // fit scratch, allocator granularity
   return b;
 }

@@ -169,6 +169,23 @@ int galic_calc_all_finish(galic_ctx *ctx);
  * merit function and the commit stay FP64). */
 int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed, uint32_t rep_serial, int form);
 
+/* `reps` consecutive repetitions of `count` particles each: the loop body of
+ * main.c:94-100 (init_updates, optimize_some_particles, commit_updates) run
+ * reps times.  Repetition r optimises idx[r*count .. r*count+count-1] with
+ * proposal streams (seed, n, rep_serial + r); the result equals reps calls of
+ * galic_optimize_rep bit for bit.  The library integrates the old and trial
+ * orbits of a window of repetitions in one launch (a proposal depends only
+ * on P[n].Pos, the targets and its stream, and the old orbit on P[n].Vel,
+ * which only n's own optimisation changes), then evaluates, accepts and
+ * commits the repetitions in order.  A window ends before a particle
+ * repeats and when its per-orbit grids (2 x 5 x DG_Ngrid doubles per
+ * particle) would pass window_bytes (0: 4 GiB; at least one repetition).
+ * No counterpart function in the reference: it replaces the loop of
+ * main.c:94-100 (optimize_some_particles, main.c:120-146, is the caller's
+ * choice of idx). */
+int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, int reps, uint64_t seed, uint32_t rep_serial,
+                        int form, size_t window_bytes);
+
 /* Merit values of the last calc_global_fit: per type (index 1..3)
  * S, Sdisp_r, Sdisp_t, Sdisp_p, Sdisp_q, Srelfac, Srelfac_count
  * (main.c:294-358): out is 4 x 7 doubles, row = type. */

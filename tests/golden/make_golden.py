@@ -44,6 +44,13 @@ def scenario_models():
                                           C("disk", 5.0, 3.5, 20, z0=0.7, tovs=2),
                                           C("bulge", 1.5, 1.0, 12, tovs=0)],
                                          seed=13, level=5, fg_nbin=64, torbit_fac=2.0)
+    # halo from the force grid, bulge analytic (SampleForceNbulge = 0): the
+    # bulge_get_acceleration / _potential branch of grid.c:185-196 and
+    # grid.c:103-108 (bulge.c:64-85)
+    m = synth.build_model([C("halo", 98.5, 30.0, 30, tovs=0), C("bulge", 1.5, 1.0, 20, tovs=0)],
+                          seed=14, level=5, fg_nbin=64, torbit_fac=2.0)
+    m.params.SampleForceNbulge = 0
+    out["bulge_analytic"] = m
     for name, m in out.items():
         # edge cases: one particle mirrored below the midplane, one near the axis,
         # one outside the tabulated grid
@@ -124,10 +131,13 @@ def model_from_arrays(a):
                        ptype=np.ascontiguousarray(a["ptype"], dtype=np.int32), ptargets=a["ptargets"])
 
 
-def main():
+def main(names=None):
+    """Writes every scenario's fixture, or only those named on the command line."""
     oracle_lib.build_oracle()
     assert oracle_lib.reference_available(), "oracle/_ref/libgalic_ref.so missing (needs the reference tree)"
     for name, m in scenario_models().items():
+        if names and name not in names:
+            continue
         arrays = model_arrays(m)
         out = oracle_lib.run_reference(run, name, arrays)
         path = os.path.join(HERE, f"{name}.npz")
@@ -136,4 +146,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -23,6 +23,9 @@ REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref.so")
 # GALIC's C with the reference's own optimisation flags (-O3 -march=native):
 # the timed CPU baseline; the parity build above has FP contraction off
 REF_FAST_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref_fast.so")
+# GALIC's C (parity build) with log, atan2, sin, cos, acos from the project's
+# gmath.h, the CUDA kernels' elementary functions (oracle/shim/gmath_libm.c)
+REF_GMATH_SO = os.path.join(ROOT, "oracle", "_ref", "libgalic_ref_gmath.so")
 
 dptr, iptr = _ffi.dptr, _ffi.iptr
 PD, PI, VP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
@@ -45,6 +48,10 @@ def reference_available():
 
 def reference_fast_available():
     return os.path.exists(REF_FAST_SO)
+
+
+def reference_gmath_available():
+    return os.path.exists(REF_GMATH_SO)
 
 
 class OracleGeometry:
@@ -496,8 +503,8 @@ def reference_peano_keys(xyz, bits):
     return np.array([L.ref_peano_key(int(x), int(y), int(z), bits) for x, y, z in xyz], dtype=np.uint64)
 
 
-def _ref_lib(fast=False):
-    L = C.CDLL(REF_FAST_SO if fast else REF_SO)
+def _ref_lib(fast=False, gmath=False):
+    L = C.CDLL(REF_GMATH_SO if gmath else (REF_FAST_SO if fast else REF_SO))
     sig = {
         "ref_setup": (C.c_int, [PP]),
         "ref_set_force_grid": (None, [PD, PD, PD]),
@@ -549,10 +556,12 @@ def _ref_lib(fast=False):
 class Reference:
     """GALIC's own C (one model per process: the reference keeps globals).
     fast=True loads the build with the reference's own optimisation flags
-    (the timed baseline) instead of the contraction-free parity build."""
+    (the timed baseline) instead of the contraction-free parity build;
+    gmath=True loads the parity build whose elementary functions are the
+    CUDA kernels' (gmath.h)."""
 
-    def __init__(self, params, fast=False):
-        self.L = _ref_lib(fast)
+    def __init__(self, params, fast=False, gmath=False):
+        self.L = _ref_lib(fast, gmath)
         self.params = params.copy()
         self.L.ref_setup(C.byref(self.params))
         Lv = params.DG_MaxLevel
@@ -621,6 +630,27 @@ class Reference:
         vdisp = np.zeros((self.n, 4))
         self.L.ref_get_particles(dptr(vel), iptr(orbits), dptr(vdisp))
         return vel, orbits, vdisp
+
+
+def reference_calc_all(arrays, gmath=False, orbits=()):
+    """GALIC's own calc_all_response_fields (main.c:151-362, one rank) on a
+    model given as tests/golden/make_golden.py arrays; returns ({type: [10,
+    Ngrid] committed grids}, fit [4, 7], [orbit_mod results of the particles
+    `orbits`]).  gmath=True: the build with the CUDA kernels' elementary
+    functions.  Run it through run_reference()."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import model_from_arrays
+
+    m = model_from_arrays(arrays)
+    ref = Reference(m.params, gmath=gmath)
+    ref.load_model(m)
+    per_orbit = [ref.orbit_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i]) for i in orbits]
+    ref.calc_all()
+    grids = {t: np.stack([ref.response(t, w) for w in range(_ffi.GRID_COUNT)]) for t in (1, 2, 3)
+             if m.params.NType[t]}
+    return grids, ref.fit(), per_orbit
 
 
 def _child(fn, args, q):

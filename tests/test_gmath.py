@@ -22,6 +22,7 @@ double t_cos(double x) { return gm_cos(x); }
 double t_acos(double x) { return gm_acos(x); }
 double t_exp(double x) { return gm_exp(x); }
 double t_asin(double x) { return gm_asin(x); }
+void t_sincos(double x, double *s, double *c) { gm_sincos(x, s, c); }
 '''
 
 
@@ -38,6 +39,8 @@ def gm(tmp_path_factory):
         f = getattr(L, n)
         f.restype = C.c_double
         f.argtypes = [C.c_double] * k
+    L.t_sincos.restype = None
+    L.t_sincos.argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     return L
 
 
@@ -97,3 +100,18 @@ def test_asin_within_two_ulp(gm):
     xs = np.concatenate([rng.uniform(-1, 1, 20000), rng.uniform(-1e-3, 1e-3, 2000), [1.0, -1.0, 0.0, -0.0, 1 - 2 ** -52]])
     assert max(ulps(gm.t_asin(x), math.asin(x)) for x in xs) <= 2.0
     assert math.isnan(gm.t_asin(1.5))
+
+
+def test_sincos_equals_sin_and_cos(gm):
+    """gm_sincos (one reduction, both polynomials, selected by quadrant) gives
+    gm_sin and gm_cos bit for bit, special and tiny arguments included."""
+    rng = np.random.default_rng(11)
+    xs = np.concatenate([rng.uniform(-math.pi, math.pi, 20000), rng.uniform(-1e4, 1e4, 2000),
+                         [0.0, -0.0, 1e-300, -1e-9, 2.0 ** -28, math.pi / 4, math.pi / 2, -math.pi, math.pi,
+                          float("inf"), float("nan")]])
+    s, c = C.c_double(), C.c_double()
+    for x in xs:
+        gm.t_sincos(float(x), C.byref(s), C.byref(c))
+        ws, wc = gm.t_sin(float(x)), gm.t_cos(float(x))
+        assert (math.isnan(ws) and math.isnan(s.value)) or np.float64(s.value).tobytes() == np.float64(ws).tobytes()
+        assert (math.isnan(wc) and math.isnan(c.value)) or np.float64(c.value).tobytes() == np.float64(wc).tobytes()

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import golden_lib
+import oracle_lib
 from oracle_lib import Oracle
 
 # per-bin tolerance of the gmath form against the reference: relative to the
@@ -102,3 +103,31 @@ def test_gmath_form_within_tolerance(golden):
         assert rel_to_peak(got, outs[f"calc_resp{t}"]) < BIN_TOL
     f, g = o.fit()[present, :5], outs["calc_fit"][present, :5]
     assert np.all(np.abs(f - g) <= FIT_TOL * np.abs(g) + FIT_ATOL)
+
+
+@pytest.mark.skipif(not oracle_lib.reference_gmath_available(), reason="GALIC's own C (oracle/_ref) is not built")
+def test_reference_with_project_math_equals_restatement(golden):
+    """GALIC's unmodified C linked with the project's elementary functions
+    (oracle/shim/gmath_libm.c) and the restatement with the same functions
+    (what the CUDA kernels evaluate) agree bit for bit: per orbit, the whole
+    calc_all_response_fields and its fit."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import model_arrays
+
+    ins, outs = golden
+    m = golden_lib.model(ins)
+    idx = list(range(m.n))
+    ref, ref_fit, per_orbit = oracle_lib.run_reference(oracle_lib.reference_calc_all, model_arrays(m), True, idx)
+    o = Oracle(m.params, use_libm=False)
+    o.load_model(m)
+    for i, r in zip(idx, per_orbit):
+        b = o.orbit_mod(m.pos[i], m.vel[i], m.mass[i], m.tint[i], m.ptype[i])
+        assert r[0] == b[0] and r[1] == b[1], i
+        for k in range(2, 7):
+            assert np.array_equal(r[k], b[k]), (i, k)
+    assert o.calc_all() == 0
+    for t, g in ref.items():
+        assert np.array_equal(np.stack([o.response(t, w) for w in range(10)]), g), t
+    assert np.array_equal(o.fit(), ref_fit, equal_nan=True)  # absent types: NaN on both sides
