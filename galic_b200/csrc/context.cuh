@@ -50,7 +50,7 @@ struct galic_ctx {
   int *d_b_type = nullptr, *d_b_norbit = nullptr, *d_b_status = nullptr;
   long long *d_b_steps = nullptr;
   int scratch_rep = 0;
-  int *d_idx = nullptr, *d_accepted = nullptr;
+  int *d_idx = nullptr, *d_accepted = nullptr, *d_acc_list = nullptr, *d_acc_n = nullptr;
   double *d_vel_try = nullptr, *d_F = nullptr, *d_inst_v = nullptr;
   Cell *d_inst_cell = nullptr;
   // diagnostics

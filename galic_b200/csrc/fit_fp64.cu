@@ -2,13 +2,15 @@
 //
 //  k_fit_smooth / k_fit_diff / k_fit_final   calc_global_fit (main.c:251-362)
 //  k_propose      the proposal part of optimize (main.c:365-441)
-//  k_eval_fit     eval_fit_mod (main.c:1021-1217), one CTA per evaluation
+//  k_eval_terms   the nine stack terms of eval_fit_mod (main.c:1021-1217), one
+//                 CTA per term of each evaluation; k_accept combines them
 //  k_accept       the accept branch of optimize (main.c:468-507)
 //  k_delta_cols   the _delta accumulation (main.c:477-486) and commit_updates
 //                 (main.c:818-827): per bin, the accepted particles'
 //                 new - old values are summed in particle order, as the
 //                 reference's sequential loop does, then added to the
 //                 committed grid.
+//  k_compact      the accepted positions of a repetition, in order
 //  k_inst_delta   add_to_energy_grid of the accepted particles
 //                 (main.c:488-498) and its commit (main.c:830-835).
 #include <cuda_runtime.h>
@@ -161,13 +163,22 @@ __global__ void k_propose(DevModel M, RepArgs R)
   R.b_type[2 * k] = R.b_type[2 * k + 1] = type;
 }
 
-// one CTA per (particle k, which): which 0 = F_base, 1 = F_try
-__global__ void __launch_bounds__(256) k_eval_fit(DevModel M, RepArgs R, FitArgs f)
+// The nine stack terms of eval_fit_mod (main.c:1021-1217), one CTA per
+// (particle k, which, term): which 0 = F_base, 1 = F_try; term 0 the
+// density term (main.c:1033-1047), 1-4 the time-averaged dispersion terms
+// r, t, q, p (main.c:1052-1120), 5-8 the instantaneous terms r, t, p, q
+// (main.c:1125-1176).  Each writes its stack difference to
+// R.F[(2k + which) * NTERM + term]; k_accept combines them into F in the
+// reference's order.
+enum { NTERM = 9 };
+
+__global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitArgs f)
 {
   extern __shared__ double sm[];
   __shared__ double sh_d[4];
   __shared__ Cell sh_c;
-  const int k = blockIdx.x >> 1, which = blockIdx.x & 1;
+  const int term = blockIdx.x % NTERM, ev = blockIdx.x / NTERM;
+  const int k = ev >> 1, which = ev & 1;
   const int n = R.idx[k];
   const int type = R.p_type[n];
   const int L = f.L, G = f.Ngrid, Ns = f.Nstack;
@@ -176,76 +187,79 @@ __global__ void __launch_bounds__(256) k_eval_fit(DevModel M, RepArgs R, FitArgs
   const double *gnew = R.grids + (size_t) (2 * k + which) * NF_ORBIT * G;
   const double *stk = f.stacks + (size_t) type * NG_COMMITTED * Ns;
   const double *tg = f.targets + (size_t) type * NT_TARGET * Ns;
-  const double MT = f.MType[type];
-
-  // density term (main.c:1033-1047)
-  for(int i = threadIdx.x; i < G; i += blockDim.x)
-    sm[off + i] = stk[(size_t) GALIC_GRID_MASS_S * Ns + off + i] + gnew[F_M * G + i] - gold[F_M * G + i];
-  __syncthreads();
-  stack_smooth_cta(sm, L);
-  double value = stack_diff_cta(sm, tg + T_DGM * Ns, tg + T_DGM * Ns, nullptr, f.dgs_distance, f.thr_d[type], 0, 0, L,
-                                f.R200_20, f.LowerDispLimit);
-  value *= 1.0 / MT;
-
-  // time-averaged dispersion terms (main.c:1052-1120): r, t, q, p
-  const int fs[4] = {F_R, F_T, F_Q, F_P};
-  const int gs[4] = {GALIC_GRID_R_S, GALIC_GRID_T_S, GALIC_GRID_Q_S, GALIC_GRID_P_S};
-  const int ts[4] = {T_R, T_T, T_Q, T_P};
-  double vs[4];
-  for(int a = 0; a < 4; a++) {
+  double v;
+  if(term == 0) {
+    // density term: committed + new - old
+    for(int i = threadIdx.x; i < G; i += blockDim.x)
+      sm[off + i] = stk[(size_t) GALIC_GRID_MASS_S * Ns + off + i] + gnew[F_M * G + i] - gold[F_M * G + i];
+    __syncthreads();
+    stack_smooth_cta(sm, L);
+    v = stack_diff_cta(sm, tg + T_DGM * Ns, tg + T_DGM * Ns, nullptr, f.dgs_distance, f.thr_d[type], 0, 0, L,
+                       f.R200_20, f.LowerDispLimit);
+  } else if(term <= 4) {
+    // time-averaged dispersion terms r, t, q, p
+    const int a = term - 1;
+    const int fs[4] = {F_R, F_T, F_Q, F_P};
+    const int gs[4] = {GALIC_GRID_R_S, GALIC_GRID_T_S, GALIC_GRID_Q_S, GALIC_GRID_P_S};
+    const int ts[4] = {T_R, T_T, T_Q, T_P};
     for(int i = threadIdx.x; i < G; i += blockDim.x)
       sm[off + i] = stk[(size_t) gs[a] * Ns + off + i] + gnew[fs[a] * G + i] - gold[fs[a] * G + i];
     __syncthreads();
     stack_smooth_cta(sm, L);
-    vs[a] = stack_diff_cta(sm, tg + ts[a] * Ns, tg + T_DGM * Ns, tg + ts[a] * Ns, f.dgs_distance, f.thr_d[type], 2, 1,
-                           L, f.R200_20, f.LowerDispLimit) /
-            MT;
-  }
-  const double value_rs = vs[0], value_ts = vs[1], value_qs = vs[2], value_ps = vs[3];
-
-  // instantaneous terms (main.c:1125-1176)
-  if(threadIdx.x == 0) {
-    LogConsts Lc = make_log_consts(M);
-    const double *vel = which ? &R.vel_try[3 * k] : &R.p_vel[3 * n];
-    disp_components(M, Lc, type, &R.p_pos[3 * n], vel, sh_d);
-    sh_c = energy_cell(M, Lc, &R.p_pos[3 * n]);
-  }
-  __syncthreads();
-  const double mass = R.p_mass[n];
-  const double *vd = &R.p_vdisp[4 * n];
-  // add_to_energy_grid: vr2 *= mass etc. (main.c:885-888); order r, t, p, q
-  const double dv[4] = {(sh_d[0] - vd[0]) * mass, (sh_d[1] - vd[1]) * mass, (sh_d[2] - vd[2]) * mass,
-                        (sh_d[3] - vd[3]) * mass};
-  const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
-  const int ti[4] = {T_R, T_T, T_P, T_Q};
-  const Cell c = sh_c;
-  const int Nb = 1 << L;
-  const int cells[4] = {c.iz * Nb + c.iR, c.iz * Nb + c.iR + 1, (c.iz + 1) * Nb + c.iR, (c.iz + 1) * Nb + c.iR + 1};
-  const double w[4] = {(1 - c.fR) * (1 - c.fz), (c.fR) * (1 - c.fz), (1 - c.fR) * (c.fz), (c.fR) * (c.fz)};
-  double vi[4];
-  for(int a = 0; a < 4; a++) {
+    v = stack_diff_cta(sm, tg + ts[a] * Ns, tg + T_DGM * Ns, tg + ts[a] * Ns, f.dgs_distance, f.thr_d[type], 2, 1,
+                       L, f.R200_20, f.LowerDispLimit);
+  } else {
+    // instantaneous terms r, t, p, q: the particle's current (or trial)
+    // velocity replaces its committed projections at its energy-grid cell
+    const int a = term - 5;
+    if(threadIdx.x == 0) {
+      LogConsts Lc = make_log_consts(M);
+      const double *vel = which ? &R.vel_try[3 * k] : &R.p_vel[3 * n];
+      disp_components(M, Lc, type, &R.p_pos[3 * n], vel, sh_d);
+      sh_c = energy_cell(M, Lc, &R.p_pos[3 * n]);
+    }
+    __syncthreads();
+    const double mass = R.p_mass[n];
+    const double *vd = &R.p_vdisp[4 * n];
+    // add_to_energy_grid: vr2 *= mass etc. (main.c:885-888); order r, t, p, q
+    const double dv = (sh_d[a] - vd[a]) * mass;
+    const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
+    const int ti[4] = {T_R, T_T, T_P, T_Q};
+    const Cell c = sh_c;
+    const int Nb = 1 << L;
+    const int cells[4] = {c.iz * Nb + c.iR, c.iz * Nb + c.iR + 1, (c.iz + 1) * Nb + c.iR,
+                          (c.iz + 1) * Nb + c.iR + 1};
+    const double w[4] = {(1 - c.fR) * (1 - c.fz), (c.fR) * (1 - c.fz), (1 - c.fR) * (c.fz), (c.fR) * (c.fz)};
     for(int i = threadIdx.x; i < G; i += blockDim.x) sm[off + i] = stk[(size_t) gi[a] * Ns + off + i];
     __syncthreads();
     if(threadIdx.x == 0)
-      for(int j = 0; j < 4; j++) sm[off + cells[j]] += w[j] * dv[a];
+      for(int j = 0; j < 4; j++) sm[off + cells[j]] += w[j] * dv;
     __syncthreads();
     stack_smooth_cta(sm, L);
-    vi[a] = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns, nullptr,
-                           f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
+    v = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns, nullptr,
+                       f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
   }
-  double value_r = vi[0], value_t = vi[1], value_p = vi[2], value_q = vi[3];
-  if(M.tovs[type] == 0 || type == 2) value_q = 0;  // main.c:1195
-  if(threadIdx.x == 0) {
-    const double *fit = f.fit + type * 7;
-    double F = value + fit[5] / fit[6] * (value_r + value_t + value_p + value_q) +
-               (R.fac_rs[type] * value_rs + R.fac_ts[type] * value_ts + R.fac_ps[type] * value_ps +
-                R.fac_qs[type] * value_qs) /
-                   4;
-    R.F[blockIdx.x] = F;
-  }
+  if(threadIdx.x == 0) R.F[blockIdx.x] = v;
 }
 
-__global__ void k_accept(DevModel M, RepArgs R)
+// F of eval_fit_mod from its nine stack terms t[] (main.c:1047, 1120, 1195-1212)
+__device__ __forceinline__ double combine_terms(const DevModel &M, const RepArgs &R, const FitArgs &f, int type,
+                                                const double *t)
+{
+  const double MT = f.MType[type];
+  double value = t[0];
+  value *= 1.0 / MT;
+  const double value_rs = t[1] / MT, value_ts = t[2] / MT, value_qs = t[3] / MT, value_ps = t[4] / MT;
+  double value_r = t[5], value_t = t[6], value_p = t[7], value_q = t[8];
+  if(M.tovs[type] == 0 || type == 2) value_q = 0;  // main.c:1195
+  const double *fit = f.fit + type * 7;
+  return value + fit[5] / fit[6] * (value_r + value_t + value_p + value_q) +
+         (R.fac_rs[type] * value_rs + R.fac_ts[type] * value_ts + R.fac_ps[type] * value_ps +
+          R.fac_qs[type] * value_qs) /
+             4;
+}
+
+__global__ void k_accept(DevModel M, RepArgs R, FitArgs f)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if(k >= R.count) return;
@@ -253,7 +267,9 @@ __global__ void k_accept(DevModel M, RepArgs R)
   const int type = R.p_type[n];
   R.p_orbits[n] = R.b_norbit[2 * k];  // main.c:460 writes the old orbit's count
   atomicAdd(&R.tries[type], 1ULL);
-  const bool acc = R.F[2 * k + 1] < R.F[2 * k];
+  const double F_base = combine_terms(M, R, f, type, &R.F[(2 * k) * NTERM]);
+  const double F_try = combine_terms(M, R, f, type, &R.F[(2 * k + 1) * NTERM]);
+  const bool acc = F_try < F_base;  // main.c:468
   R.accepted[k] = acc ? 1 : 0;
   if(!acc) return;
   for(int j = 0; j < 3; j++) R.p_vel[3 * n + j] = R.vel_try[3 * k + j];
@@ -271,11 +287,41 @@ __global__ void k_accept(DevModel M, RepArgs R)
   R.inst_cell[k] = energy_cell(M, L, &R.p_pos[3 * n]);
 }
 
+// the accepted positions of one repetition in increasing k (one CTA): the
+// commit kernels below loop over these instead of over every position
+__global__ void __launch_bounds__(1024) k_compact(RepArgs R)
+{
+  __shared__ int warp_sum[32];
+  __shared__ int base;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if(threadIdx.x == 0) base = 0;
+  __syncthreads();
+  for(int k0 = 0; k0 < R.count; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    const int a = (k < R.count && R.accepted[k]) ? 1 : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, a);
+    if(lane == 0) warp_sum[wid] = __popc(m);
+    __syncthreads();
+    int before = 0;
+    for(int w = 0; w < wid; w++) before += warp_sum[w];
+    if(a) R.acc_list[base + before + __popc(m & ((1u << lane) - 1))] = k;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+      int tot = 0;
+      for(int w = 0; w < (int) (blockDim.x >> 5); w++) tot += warp_sum[w];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if(threadIdx.x == 0) *R.acc_n = base;
+}
+
 // per (type, field, bin): delta = sum over accepted particles, in order, of
 // new - old; committed += delta
 __global__ void k_delta_cols(RepArgs R, FitArgs f)
 {
   const int G = f.Ngrid;
+  const int na = *R.acc_n;
   const size_t total = (size_t) 4 * NF_ORBIT * G;
   for(size_t t = blockIdx.x * (size_t) blockDim.x + threadIdx.x; t < total; t += (size_t) gridDim.x * blockDim.x) {
     const int type = (int) (t / ((size_t) NF_ORBIT * G));
@@ -283,8 +329,9 @@ __global__ void k_delta_cols(RepArgs R, FitArgs f)
     const int i = (int) (t % G);
     if(type < 1 || !f.present[type]) continue;
     double delta = 0;
-    for(int k = 0; k < R.count; k++) {
-      if(!R.accepted[k] || R.b_type[2 * k] != type) continue;
+    for(int j = 0; j < na; j++) {
+      const int k = R.acc_list[j];
+      if(R.b_type[2 * k] != type) continue;
       const double *gold = R.grids + (size_t) (2 * k) * NF_ORBIT * G;
       const double *gnew = gold + (size_t) NF_ORBIT * G;
       delta += gnew[fld * G + i] - gold[fld * G + i];
@@ -298,6 +345,7 @@ __global__ void k_delta_cols(RepArgs R, FitArgs f)
 __global__ void k_inst_delta(RepArgs R, FitArgs f)
 {
   const int G = f.Ngrid, Nb = 1 << f.L;
+  const int na = *R.acc_n;
   const size_t total = (size_t) 4 * 4 * G;
   const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
   for(size_t t = blockIdx.x * (size_t) blockDim.x + threadIdx.x; t < total; t += (size_t) gridDim.x * blockDim.x) {
@@ -306,8 +354,9 @@ __global__ void k_inst_delta(RepArgs R, FitArgs f)
     const int cidx = (int) (t % G);
     if(type < 1 || !f.present[type]) continue;
     double delta = 0;
-    for(int k = 0; k < R.count; k++) {
-      if(!R.accepted[k] || R.b_type[2 * k] != type) continue;
+    for(int j = 0; j < na; j++) {
+      const int k = R.acc_list[j];
+      if(R.b_type[2 * k] != type) continue;
       const Cell c = R.inst_cell[k];
       const int base = c.iz * Nb + c.iR;
       double w;
@@ -340,7 +389,7 @@ cudaError_t prepare_fit_kernels()
   if(dev >= 0 && dev < 256 && done[dev]) return cudaSuccess;
   if((e = cudaFuncSetAttribute(k_fit_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if((e = cudaFuncSetAttribute(k_fit_diff, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
-  if((e = cudaFuncSetAttribute(k_eval_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  if((e = cudaFuncSetAttribute(k_eval_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if(dev >= 0 && dev < 256) done[dev] = true;
   return cudaSuccess;
 }
@@ -373,11 +422,15 @@ int launch_rep_commit(const DevModel &M, const RepArgs &R, const FitArgs &f, cud
 {
   const int count = R.count;
   size_t smem = (size_t) f.Nstack * sizeof(double);
-  k_eval_fit<<<2 * count, 256, smem, s>>>(M, R, f);
-  k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R);
+  // a level-7 stack (171 KiB) leaves room for one CTA per SM: give it the
+  // SM's threads; smaller stacks share the SM between several CTAs
+  const int threads = f.L >= 7 ? 1024 : 512;
+  k_eval_terms<<<2 * count * NTERM, threads, smem, s>>>(M, R, f);
+  k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R, f);
+  k_compact<<<1, 1024, 0, s>>>(R);
   k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
   k_inst_delta<<<148 * 8, 256, 0, s>>>(R, f);
-  return 4 + launch_global_fit(f, s);
+  return 5 + launch_global_fit(f, s);
 }
 
 RepArgs rep_slice(const RepArgs &R, int first, int count, int G)
@@ -394,8 +447,10 @@ RepArgs rep_slice(const RepArgs &R, int first, int count, int G)
   S.b_norbit = R.b_norbit + 2 * (size_t) first;
   S.grids = R.grids + (size_t) (2 * first) * NF_ORBIT * G;
   S.vel_try = R.vel_try + 3 * (size_t) first;
-  S.F = R.F + 2 * (size_t) first;
+  S.F = R.F + 2 * (size_t) NTERM * first;
   S.accepted = R.accepted + first;
+  S.acc_list = R.acc_list + first;
+  S.acc_n = R.acc_n + first / count;
   S.inst_v = R.inst_v + 4 * (size_t) first;
   S.inst_cell = R.inst_cell + first;
   return S;

@@ -72,7 +72,7 @@ template <int PER>
 using WarpQueue32 = WarpQueueT<PER, float>;
 
 // records per lane of a block of BLOCK threads (FP32 sums)
-__host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 8 : (block <= 192 ? 7 : 5); }
+__host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 12 : (block <= 192 ? 7 : 5); }
 
 // true when some lane could not park another cell's nodes
 template <int PER>

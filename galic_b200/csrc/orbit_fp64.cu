@@ -23,31 +23,39 @@ struct DenseSink {
   double *m, *r, *t, *q, *p;
   int Nb;
   int with_egy;
+  // bin += value for the 4 corners of the deposit's cell in each grid, in the
+  // reference's order per bin; the 4 corner bins are distinct and the 5
+  // grids are separate arrays, so all loads are issued before the adds and
+  // stores (their latencies overlap instead of following one another)
   __device__ __forceinline__ void operator()(const Deposit &d)
   {
-    int i00 = d.iz * Nb + d.iR, i10 = d.iz * Nb + (d.iR + 1);
-    int i01 = (d.iz + 1) * Nb + d.iR, i11 = (d.iz + 1) * Nb + (d.iR + 1);
-    m[i00] += d.m00;
-    m[i10] += d.m10;
-    m[i01] += d.m01;
-    m[i11] += d.m11;
+    const int i00 = d.iz * Nb + d.iR, i10 = d.iz * Nb + (d.iR + 1);
+    const int i01 = (d.iz + 1) * Nb + d.iR, i11 = (d.iz + 1) * Nb + (d.iR + 1);
+    const int idx[4] = {i00, i10, i01, i11};
+    const double w[4] = {d.m00, d.m10, d.m01, d.m11};
+    double vm[4];
+#pragma unroll
+    for(int c = 0; c < 4; c++) vm[c] = m[idx[c]];
     if(with_egy) {
-      r[i00] += d.m00 * d.p.vr2;
-      r[i10] += d.m10 * d.p.vr2;
-      r[i01] += d.m01 * d.p.vr2;
-      r[i11] += d.m11 * d.p.vr2;
-      t[i00] += d.m00 * d.p.vt2;
-      t[i10] += d.m10 * d.p.vt2;
-      t[i01] += d.m01 * d.p.vt2;
-      t[i11] += d.m11 * d.p.vt2;
-      q[i00] += d.m00 * d.p.vq2;
-      q[i10] += d.m10 * d.p.vq2;
-      q[i01] += d.m01 * d.p.vq2;
-      q[i11] += d.m11 * d.p.vq2;
-      p[i00] += d.m00 * d.p.vp2;
-      p[i10] += d.m10 * d.p.vp2;
-      p[i01] += d.m01 * d.p.vp2;
-      p[i11] += d.m11 * d.p.vp2;
+      double vr[4], vt[4], vq[4], vp[4];
+#pragma unroll
+      for(int c = 0; c < 4; c++) {
+        vr[c] = r[idx[c]];
+        vt[c] = t[idx[c]];
+        vq[c] = q[idx[c]];
+        vp[c] = p[idx[c]];
+      }
+#pragma unroll
+      for(int c = 0; c < 4; c++) {
+        m[idx[c]] = vm[c] + w[c];
+        r[idx[c]] = vr[c] + w[c] * d.p.vr2;
+        t[idx[c]] = vt[c] + w[c] * d.p.vt2;
+        q[idx[c]] = vq[c] + w[c] * d.p.vq2;
+        p[idx[c]] = vp[c] + w[c] * d.p.vp2;
+      }
+    } else {
+#pragma unroll
+      for(int c = 0; c < 4; c++) m[idx[c]] = vm[c] + w[c];
     }
   }
 };

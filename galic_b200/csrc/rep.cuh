@@ -26,8 +26,10 @@ struct RepArgs {
   int *b_type, *b_norbit;
   double *grids;  // 2*count x NF_ORBIT x Ngrid
   double *vel_try;  // count x 3
-  double *F;        // 2*count: F_base, F_try
+  double *F;        // 2*count x 9: the stack terms of F_base, F_try (fit_fp64.cu:k_eval_terms)
   int *accepted;    // count
+  int *acc_list;    // count: the accepted positions k in increasing order (k_compact)
+  int *acc_n;       // one per repetition of the window: the length of its acc_list
   double *inst_v;   // count x 4
   Cell *inst_cell;  // count
   unsigned long long *tries, *changes;  // [4]
