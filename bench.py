@@ -548,6 +548,9 @@ def measure_construction(name, scale, cpu):
     model = construction_model(name, scale)
     window = (24 << 30) if model.params.DG_MaxLevel >= 7 else 0
     res = {"config": cfg["desc"], "particles": model.n, "scale": scale}
+    # warm-up: one short run of each form loads every kernel of the path
+    for form in (GALIC_FORM_FP64, GALIC_FORM_FP32):
+        run_construction(model, form, 1, 2, cfg["fraction"], window_bytes=window)
     for label, form in (("fp64", GALIC_FORM_FP64), ("fp32", GALIC_FORM_FP32)):
         res[label] = run_construction(model, form, cfg["iterations"], cfg["reps"], cfg["fraction"],
                                       window_bytes=window)

@@ -150,6 +150,7 @@ int ensure_rep_scratch(galic_ctx *ctx, int count)
   CK(dalloc(ctx, &ctx->d_idx, count));
   CK(dalloc(ctx, &ctx->d_acc_list, count));
   CK(dalloc(ctx, &ctx->d_acc_n, count));  // one per repetition: at most count repetitions per window
+  if(!ctx->d_inst0) CK(dalloc(ctx, &ctx->d_inst0, 16));
   CK(dalloc(ctx, &ctx->d_accepted, count));
   CK(dalloc(ctx, &ctx->d_vel_try, 3 * (size_t) count));
   CK(dalloc(ctx, &ctx->d_F, 2 * 9 * (size_t) count));  // 9 merit terms per evaluation
@@ -382,7 +383,7 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx, ctx->d_b_tall); dfree(ctx, ctx->d_b_err); dfree(ctx, ctx->d_b_type); dfree(ctx, ctx->d_b_norbit); dfree(ctx, ctx->d_b_status);
   dfree(ctx, ctx->d_b_steps);
   dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
-  dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n);
+  dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n); dfree(ctx, ctx->d_inst0);
   for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_tab32[t]);
   dfree(ctx, ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
@@ -928,6 +929,7 @@ RepArgs make_rep_args(galic_ctx *ctx, int count, uint64_t seed, uint32_t rep_ser
   R.accepted = ctx->d_accepted;
   R.acc_list = ctx->d_acc_list;
   R.acc_n = ctx->d_acc_n;
+  R.inst0 = ctx->d_inst0;
   R.inst_v = ctx->d_inst_v;
   R.inst_cell = ctx->d_inst_cell;
   R.tries = ctx->d_counters;

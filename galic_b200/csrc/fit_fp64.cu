@@ -170,15 +170,21 @@ __global__ void k_propose(DevModel M, RepArgs R)
 // (main.c:1125-1176).  Each writes its stack difference to
 // R.F[(2k + which) * NTERM + term]; k_accept combines them into F in the
 // reference's order.
-enum { NTERM = 9 };
+// The base evaluation's instantaneous terms (which 0, terms 5-8) are not
+// launched per particle: its velocity is the particle's own, whose
+// projections are the committed ones (p_vdisp was computed from p_vel by
+// the same disp_components), so the change it adds to the energy grid is
+// exactly zero and the term is its type's committed misfit, computed once
+// per repetition by k_base_inst.  Each particle launches 5 + 9 CTAs.
+enum { NTERM = 9, NLAUNCH = 14 };
 
 __global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitArgs f)
 {
   extern __shared__ double sm[];
   __shared__ double sh_d[4];
   __shared__ Cell sh_c;
-  const int term = blockIdx.x % NTERM, ev = blockIdx.x / NTERM;
-  const int k = ev >> 1, which = ev & 1;
+  const int j = blockIdx.x % NLAUNCH, k = blockIdx.x / NLAUNCH;
+  const int which = j < 5 ? 0 : 1, term = j < 5 ? j : j - 5;
   const int n = R.idx[k];
   const int type = R.p_type[n];
   const int L = f.L, G = f.Ngrid, Ns = f.Nstack;
@@ -239,7 +245,28 @@ __global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitA
     v = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns, nullptr,
                        f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
   }
-  if(threadIdx.x == 0) R.F[blockIdx.x] = v;
+  if(threadIdx.x == 0) R.F[(2 * k + which) * NTERM + term] = v;
+}
+
+// the committed instantaneous misfit of each present type: terms 5-8 of
+// every base evaluation of the repetition (see k_eval_terms)
+__global__ void __launch_bounds__(1024) k_base_inst(RepArgs R, FitArgs f)
+{
+  extern __shared__ double sm[];
+  const int type = blockIdx.x >> 2, a = blockIdx.x & 3;
+  if(type < 1 || !f.present[type]) return;
+  const int L = f.L, G = f.Ngrid, Ns = f.Nstack;
+  const int off = ((1 << (2 * L)) - 1) / 3;
+  const double *stk = f.stacks + (size_t) type * NG_COMMITTED * Ns;
+  const double *tg = f.targets + (size_t) type * NT_TARGET * Ns;
+  const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
+  const int ti[4] = {T_R, T_T, T_P, T_Q};
+  for(int i = threadIdx.x; i < G; i += blockDim.x) sm[off + i] = stk[(size_t) gi[a] * Ns + off + i];
+  __syncthreads();
+  stack_smooth_cta(sm, L);
+  const double v = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns,
+                                  nullptr, f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
+  if(threadIdx.x == 0) R.inst0[blockIdx.x] = v;
 }
 
 // F of eval_fit_mod from its nine stack terms t[] (main.c:1047, 1120, 1195-1212)
@@ -267,7 +294,10 @@ __global__ void k_accept(DevModel M, RepArgs R, FitArgs f)
   const int type = R.p_type[n];
   R.p_orbits[n] = R.b_norbit[2 * k];  // main.c:460 writes the old orbit's count
   atomicAdd(&R.tries[type], 1ULL);
-  const double F_base = combine_terms(M, R, f, type, &R.F[(2 * k) * NTERM]);
+  double tb[NTERM];
+  for(int j = 0; j < 5; j++) tb[j] = R.F[(2 * k) * NTERM + j];
+  for(int j = 0; j < 4; j++) tb[5 + j] = R.inst0[4 * type + j];
+  const double F_base = combine_terms(M, R, f, type, tb);
   const double F_try = combine_terms(M, R, f, type, &R.F[(2 * k + 1) * NTERM]);
   const bool acc = F_try < F_base;  // main.c:468
   R.accepted[k] = acc ? 1 : 0;
@@ -390,6 +420,7 @@ cudaError_t prepare_fit_kernels()
   if((e = cudaFuncSetAttribute(k_fit_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if((e = cudaFuncSetAttribute(k_fit_diff, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if((e = cudaFuncSetAttribute(k_eval_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  if((e = cudaFuncSetAttribute(k_base_inst, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   if(dev >= 0 && dev < 256) done[dev] = true;
   return cudaSuccess;
 }
@@ -425,12 +456,13 @@ int launch_rep_commit(const DevModel &M, const RepArgs &R, const FitArgs &f, cud
   // a level-7 stack (171 KiB) leaves room for one CTA per SM: give it the
   // SM's threads; smaller stacks share the SM between several CTAs
   const int threads = f.L >= 7 ? 1024 : 512;
-  k_eval_terms<<<2 * count * NTERM, threads, smem, s>>>(M, R, f);
+  k_base_inst<<<16, threads, smem, s>>>(R, f);
+  k_eval_terms<<<count * NLAUNCH, threads, smem, s>>>(M, R, f);
   k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R, f);
   k_compact<<<1, 1024, 0, s>>>(R);
   k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
   k_inst_delta<<<148 * 8, 256, 0, s>>>(R, f);
-  return 5 + launch_global_fit(f, s);
+  return 6 + launch_global_fit(f, s);
 }
 
 RepArgs rep_slice(const RepArgs &R, int first, int count, int G)

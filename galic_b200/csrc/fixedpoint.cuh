@@ -37,6 +37,33 @@ __device__ __forceinline__ void fx_split(double v, int S, long long *H, unsigned
   *L = l;
 }
 
+// the word pair of t = v * 2^(S-24) (t given: a caller that scales many values
+// by the same power of two and factor folds them into one multiplier; a
+// power-of-two factor is exact, so the pair equals fx_split's)
+__device__ __forceinline__ void fx_split_scaled(double t, long long *H, unsigned long long *L)
+{
+  double fh = floor(t);
+  double fr = t - fh;
+  long long h = (long long) fh;
+  unsigned long long l = (unsigned long long) rint(fr * 16777216.0);
+  if(l == 16777216ULL) {
+    l = 0;
+    h += 1;
+  }
+  *H = h;
+  *L = l;
+}
+
+__device__ __forceinline__ void fx_add_scaled(FxWord *w, double t)
+{
+  if(t == 0.0) return;
+  long long H;
+  unsigned long long L;
+  fx_split_scaled(t, &H, &L);
+  if(H) atomicAdd(&w->hi, (unsigned long long) H);
+  if(L) atomicAdd(&w->lo, L);
+}
+
 // adds v to the word pair w (no return value needed: red.global.add.u64)
 __device__ __forceinline__ void fx_add(FxWord *w, double v, int S)
 {

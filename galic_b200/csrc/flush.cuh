@@ -65,14 +65,12 @@ struct WarpQueueT {
   int off[32];        // drain: first compacted record of each lane
   int gbase[32];      // per lane: first word of its orbit's grid set
   T scale[2][32];     // per lane: {mass field, energy fields} fixed-point factors
-                      // (the exact drain: scale[0] = mass/Tint)
-  int shift[2][32];   // the exact drain: per lane {mass field, energy fields} shifts
 };
 template <int PER>
 using WarpQueue32 = WarpQueueT<PER, float>;
 
 // records per lane of a block of BLOCK threads (FP32 sums)
-__host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 12 : (block <= 192 ? 7 : 5); }
+__host__ __device__ constexpr int queue32_per(int block) { return block <= 128 ? 8 : (block <= 192 ? 7 : 5); }
 
 // true when some lane could not park another cell's nodes
 template <int PER>
@@ -122,7 +120,9 @@ __device__ __forceinline__ void warp_drain_nodes(WarpQueueT<PER, T> &q, FxWord *
 // Exact variant (FP64 sums): every value v = sum x mass/Tint is added as the
 // two-word fixed-point pair of fixedpoint.cuh:fx_add (resolution 2^-S, two
 // integer atomics), so the bins carry the full FP64 resolution whatever the
-// headroom of the field's range.
+// headroom of the field's range.  The lane header holds mass/Tint x
+// 2^(S-24) per field class (scale), which gives the pair of fx_add(v, S)
+// bit for bit: the power-of-two factor is exact.
 template <int PER>
 __device__ __forceinline__ void warp_drain_nodes_exact(WarpQueueT<PER, double> &q, FxWord *fx, int G, int &cnt)
 {
@@ -144,10 +144,9 @@ __device__ __forceinline__ void warp_drain_nodes_exact(WarpQueueT<PER, double> &
       if(q.off[L + step] <= r) L += step;
     const int k = r - q.off[L];
     const int b = q.gbase[L] + q.base[k][L];
-    const double fac = q.scale[0][L];
-    const int sm = q.shift[0][L], se = q.shift[1][L];
+    const double sm = q.scale[0][L], se = q.scale[1][L];
 #pragma unroll
-    for(int f = 0; f < 5; f++) fx_add(&fx[b + f * G], q.val[k][f][L] * fac, f == 0 ? sm : se);
+    for(int f = 0; f < 5; f++) fx_add_scaled(&fx[b + f * G], q.val[k][f][L] * (f == 0 ? sm : se));
   }
   __syncwarp();
   cnt = 0;

@@ -110,12 +110,12 @@ struct NodeSink64 {
   int cnt;  // records parked in this lane's column since the last drain
   int cur, cur_iR, cur_iz;
   double a[4][5];
-  __device__ __forceinline__ void set_orbit(int gbase, double fac, int shift_m, int shift_e)
+  // fac x 2^(shift - 24) of the mass and the energy fields (exact scalings)
+  __device__ __forceinline__ void set_orbit(int gbase, double scale_m, double scale_e)
   {
     q->gbase[lane] = gbase;
-    q->scale[0][lane] = fac;
-    q->shift[0][lane] = shift_m;
-    q->shift[1][lane] = shift_e;
+    q->scale[0][lane] = scale_m;
+    q->scale[1][lane] = scale_e;
     cur = -1;
   }
   // slot s of cell (iz, iR) holds node (iz + node_dz(s, iz), iR + node_dr(s, iR))
@@ -236,8 +236,8 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(Dev
     p = A.order ? A.order[k] : k;
     const int type = A.type[p];
     const double fac = A.mass[p] / A.tint[p];
-    sink.set_orbit(type * NG_COMMITTED * G, fac, A.shift[type * NG_COMMITTED + GALIC_GRID_MASS_S],
-                   A.shift[type * NG_COMMITTED + GALIC_GRID_R_S]);
+    sink.set_orbit(type * NG_COMMITTED * G, ldexp(fac, A.shift[type * NG_COMMITTED + GALIC_GRID_MASS_S] - 24),
+                   ldexp(fac, A.shift[type * NG_COMMITTED + GALIC_GRID_R_S] - 24));
     orbit_begin(M, L, s, &A.pos[3 * p], &A.vel[3 * p], A.tint[p], type, true);
     return true;
   };

@@ -27,6 +27,7 @@ struct RepArgs {
   double *grids;  // 2*count x NF_ORBIT x Ngrid
   double *vel_try;  // count x 3
   double *F;        // 2*count x 9: the stack terms of F_base, F_try (fit_fp64.cu:k_eval_terms)
+  double *inst0;    // [4 types][4]: the committed instantaneous terms of the base evaluations
   int *accepted;    // count
   int *acc_list;    // count: the accepted positions k in increasing order (k_compact)
   int *acc_n;       // one per repetition of the window: the length of its acc_list
