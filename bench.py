@@ -546,7 +546,9 @@ def measure_construction(name, scale, cpu):
 
     cfg = CONSTRUCTION[name]
     model = construction_model(name, scale)
-    window = (24 << 30) if model.params.DG_MaxLevel >= 7 else 0
+    # level-7 orbit grids are 640 KiB each: 64 GiB windows hold ~12 repetitions of
+    # config 3 (a window lasts as long as its longest orbit)
+    window = (64 << 30) if model.params.DG_MaxLevel >= 7 else 0
     res = {"config": cfg["desc"], "particles": model.n, "scale": scale}
     # warm-up: one short run of each form loads every kernel of the path
     for form in (GALIC_FORM_FP64, GALIC_FORM_FP32):

@@ -146,7 +146,7 @@ int ensure_rep_scratch(galic_ctx *ctx, int count)
   if(st) return st;
   if(count <= ctx->scratch_rep) return GALIC_OK;
   dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
-  dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n);
+  dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n); dfree(ctx, ctx->d_fac);
   CK(dalloc(ctx, &ctx->d_idx, count));
   CK(dalloc(ctx, &ctx->d_acc_list, count));
   CK(dalloc(ctx, &ctx->d_acc_n, count));  // one per repetition: at most count repetitions per window
@@ -154,6 +154,7 @@ int ensure_rep_scratch(galic_ctx *ctx, int count)
   CK(dalloc(ctx, &ctx->d_accepted, count));
   CK(dalloc(ctx, &ctx->d_vel_try, 3 * (size_t) count));
   CK(dalloc(ctx, &ctx->d_F, 2 * 9 * (size_t) count));  // 9 merit terms per evaluation
+  CK(dalloc(ctx, &ctx->d_fac, 2 * (size_t) count));
   CK(dalloc(ctx, &ctx->d_inst_v, 4 * (size_t) count));
   CK(dalloc(ctx, &ctx->d_inst_cell, count));
   ctx->scratch_rep = count;
@@ -384,6 +385,7 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx, ctx->d_b_steps);
   dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
   dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n); dfree(ctx, ctx->d_inst0);
+  dfree(ctx, ctx->d_fac);
   for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_tab32[t]);
   dfree(ctx, ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
@@ -924,6 +926,8 @@ RepArgs make_rep_args(galic_ctx *ctx, int count, uint64_t seed, uint32_t rep_ser
   R.b_type = ctx->d_b_type;
   R.b_norbit = ctx->d_b_norbit;
   R.grids = ctx->d_grids;
+  R.b_tall = ctx->d_b_tall;
+  R.fac = ctx->d_fac;
   R.vel_try = ctx->d_vel_try;
   R.F = ctx->d_F;
   R.accepted = ctx->d_accepted;

@@ -51,7 +51,7 @@ struct galic_ctx {
   long long *d_b_steps = nullptr;
   int scratch_rep = 0;
   int *d_idx = nullptr, *d_accepted = nullptr, *d_acc_list = nullptr, *d_acc_n = nullptr;
-  double *d_vel_try = nullptr, *d_F = nullptr, *d_inst_v = nullptr, *d_inst0 = nullptr;
+  double *d_vel_try = nullptr, *d_F = nullptr, *d_inst_v = nullptr, *d_inst0 = nullptr, *d_fac = nullptr;
   Cell *d_inst_cell = nullptr;
   // diagnostics
   long long last_steps = 0;

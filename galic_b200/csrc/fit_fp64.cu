@@ -178,8 +178,10 @@ __global__ void k_propose(DevModel M, RepArgs R)
 // per repetition by k_base_inst.  Each particle launches 5 + 9 CTAs.
 enum { NTERM = 9, NLAUNCH = 14 };
 
-__global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitArgs f)
+__global__ void __launch_bounds__(512) k_eval_terms(DevModel M, RepArgs R, FitArgs f)
 {
+  // levels 0 .. L-1 of the evaluated stack; its finest level is formed on
+  // the fly from the committed stack and the orbit grids (stack.cuh:*_from)
   extern __shared__ double sm[];
   __shared__ double sh_d[4];
   __shared__ Cell sh_c;
@@ -191,32 +193,36 @@ __global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitA
   const int off = ((1 << (2 * L)) - 1) / 3;
   const double *gold = R.grids + (size_t) (2 * k) * NF_ORBIT * G;
   const double *gnew = R.grids + (size_t) (2 * k + which) * NF_ORBIT * G;
+  // the orbit grids are stored unscaled: x mass/tall on the fly, the
+  // operation k_scale_dense would have applied
+  const double fo = R.b_mass[2 * k] / R.b_tall[2 * k];
+  const double fn = R.b_mass[2 * k + which] / R.b_tall[2 * k + which];
   const double *stk = f.stacks + (size_t) type * NG_COMMITTED * Ns;
   const double *tg = f.targets + (size_t) type * NT_TARGET * Ns;
   double v;
   if(term == 0) {
     // density term: committed + new - old
-    for(int i = threadIdx.x; i < G; i += blockDim.x)
-      sm[off + i] = stk[(size_t) GALIC_GRID_MASS_S * Ns + off + i] + gnew[F_M * G + i] - gold[F_M * G + i];
-    __syncthreads();
-    stack_smooth_cta(sm, L);
-    v = stack_diff_cta(sm, tg + T_DGM * Ns, tg + T_DGM * Ns, nullptr, f.dgs_distance, f.thr_d[type], 0, 0, L,
-                       f.R200_20, f.LowerDispLimit);
+    const double *c = stk + (size_t) GALIC_GRID_MASS_S * Ns + off;
+    const double *gn = gnew + F_M * G, *go = gold + F_M * G;
+    auto fin = [&](int i) { return c[i] + gn[i] * fn - go[i] * fo; };
+    stack_smooth_cta_from(sm, L, fin);
+    v = stack_diff_cta_from(sm, fin, tg + T_DGM * Ns, tg + T_DGM * Ns, nullptr, f.dgs_distance, f.thr_d[type], 0, 0,
+                            L, f.R200_20, f.LowerDispLimit);
   } else if(term <= 4) {
     // time-averaged dispersion terms r, t, q, p
     const int a = term - 1;
     const int fs[4] = {F_R, F_T, F_Q, F_P};
     const int gs[4] = {GALIC_GRID_R_S, GALIC_GRID_T_S, GALIC_GRID_Q_S, GALIC_GRID_P_S};
     const int ts[4] = {T_R, T_T, T_Q, T_P};
-    for(int i = threadIdx.x; i < G; i += blockDim.x)
-      sm[off + i] = stk[(size_t) gs[a] * Ns + off + i] + gnew[fs[a] * G + i] - gold[fs[a] * G + i];
-    __syncthreads();
-    stack_smooth_cta(sm, L);
-    v = stack_diff_cta(sm, tg + ts[a] * Ns, tg + T_DGM * Ns, tg + ts[a] * Ns, f.dgs_distance, f.thr_d[type], 2, 1,
-                       L, f.R200_20, f.LowerDispLimit);
+    const double *c = stk + (size_t) gs[a] * Ns + off;
+    const double *gn = gnew + fs[a] * G, *go = gold + fs[a] * G;
+    auto fin = [&](int i) { return c[i] + gn[i] * fn - go[i] * fo; };
+    stack_smooth_cta_from(sm, L, fin);
+    v = stack_diff_cta_from(sm, fin, tg + ts[a] * Ns, tg + T_DGM * Ns, tg + ts[a] * Ns, f.dgs_distance,
+                            f.thr_d[type], 2, 1, L, f.R200_20, f.LowerDispLimit);
   } else {
-    // instantaneous terms r, t, p, q: the particle's current (or trial)
-    // velocity replaces its committed projections at its energy-grid cell
+    // instantaneous terms r, t, p, q of the trial velocity: its change of the
+    // particle's projections at its energy-grid cell
     const int a = term - 5;
     if(threadIdx.x == 0) {
       LogConsts Lc = make_log_consts(M);
@@ -231,41 +237,43 @@ __global__ void __launch_bounds__(1024) k_eval_terms(DevModel M, RepArgs R, FitA
     const double dv = (sh_d[a] - vd[a]) * mass;
     const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
     const int ti[4] = {T_R, T_T, T_P, T_Q};
-    const Cell c = sh_c;
+    const Cell cc = sh_c;
     const int Nb = 1 << L;
-    const int cells[4] = {c.iz * Nb + c.iR, c.iz * Nb + c.iR + 1, (c.iz + 1) * Nb + c.iR,
-                          (c.iz + 1) * Nb + c.iR + 1};
-    const double w[4] = {(1 - c.fR) * (1 - c.fz), (c.fR) * (1 - c.fz), (1 - c.fR) * (c.fz), (c.fR) * (c.fz)};
-    for(int i = threadIdx.x; i < G; i += blockDim.x) sm[off + i] = stk[(size_t) gi[a] * Ns + off + i];
-    __syncthreads();
-    if(threadIdx.x == 0)
-      for(int j = 0; j < 4; j++) sm[off + cells[j]] += w[j] * dv;
-    __syncthreads();
-    stack_smooth_cta(sm, L);
-    v = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns, nullptr,
-                       f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
+    const int c00 = cc.iz * Nb + cc.iR;
+    const double w00 = (1 - cc.fR) * (1 - cc.fz), w10 = (cc.fR) * (1 - cc.fz), w01 = (1 - cc.fR) * (cc.fz),
+                 w11 = (cc.fR) * (cc.fz);
+    const double *c = stk + (size_t) gi[a] * Ns + off;
+    // committed value, plus w * dv at the four corners of the cell
+    auto fin = [&](int i) {
+      const double x = c[i];
+      return i == c00 ? x + w00 * dv
+                      : (i == c00 + 1 ? x + w10 * dv : (i == c00 + Nb ? x + w01 * dv : (i == c00 + Nb + 1 ? x + w11 * dv : x)));
+    };
+    stack_smooth_cta_from(sm, L, fin);
+    v = stack_diff_cta_from(sm, fin, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns,
+                            nullptr, f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
   }
   if(threadIdx.x == 0) R.F[(2 * k + which) * NTERM + term] = v;
 }
 
 // the committed instantaneous misfit of each present type: terms 5-8 of
 // every base evaluation of the repetition (see k_eval_terms)
-__global__ void __launch_bounds__(1024) k_base_inst(RepArgs R, FitArgs f)
+__global__ void __launch_bounds__(512) k_base_inst(RepArgs R, FitArgs f)
 {
   extern __shared__ double sm[];
   const int type = blockIdx.x >> 2, a = blockIdx.x & 3;
   if(type < 1 || !f.present[type]) return;
-  const int L = f.L, G = f.Ngrid, Ns = f.Nstack;
+  const int L = f.L, Ns = f.Nstack;
   const int off = ((1 << (2 * L)) - 1) / 3;
   const double *stk = f.stacks + (size_t) type * NG_COMMITTED * Ns;
   const double *tg = f.targets + (size_t) type * NT_TARGET * Ns;
   const int gi[4] = {GALIC_GRID_R_I, GALIC_GRID_T_I, GALIC_GRID_P_I, GALIC_GRID_Q_I};
   const int ti[4] = {T_R, T_T, T_P, T_Q};
-  for(int i = threadIdx.x; i < G; i += blockDim.x) sm[off + i] = stk[(size_t) gi[a] * Ns + off + i];
-  __syncthreads();
-  stack_smooth_cta(sm, L);
-  const double v = stack_diff_cta(sm, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns, tg + T_EGM * Ns,
-                                  nullptr, f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
+  const double *c = stk + (size_t) gi[a] * Ns + off;
+  auto fin = [&](int i) { return c[i]; };
+  stack_smooth_cta_from(sm, L, fin);
+  const double v = stack_diff_cta_from(sm, fin, tg + ti[a] * Ns, stk + (size_t) GALIC_GRID_MASS_I * Ns,
+                                       tg + T_EGM * Ns, nullptr, f.thr_e[type], 1, 0, L, f.R200_20, f.LowerDispLimit);
   if(threadIdx.x == 0) R.inst0[blockIdx.x] = v;
 }
 
@@ -300,6 +308,10 @@ __global__ void k_accept(DevModel M, RepArgs R, FitArgs f)
   const double F_base = combine_terms(M, R, f, type, tb);
   const double F_try = combine_terms(M, R, f, type, &R.F[(2 * k + 1) * NTERM]);
   const bool acc = F_try < F_base;  // main.c:468
+  // mass/tall of the old and trial orbits (orbit_response.c:477-486) for
+  // the commit, which reads the unscaled orbit grids
+  R.fac[2 * k] = R.b_mass[2 * k] / R.b_tall[2 * k];
+  R.fac[2 * k + 1] = R.b_mass[2 * k + 1] / R.b_tall[2 * k + 1];
   R.accepted[k] = acc ? 1 : 0;
   if(!acc) return;
   for(int j = 0; j < 3; j++) R.p_vel[3 * n + j] = R.vel_try[3 * k + j];
@@ -364,7 +376,9 @@ __global__ void k_delta_cols(RepArgs R, FitArgs f)
       if(R.b_type[2 * k] != type) continue;
       const double *gold = R.grids + (size_t) (2 * k) * NF_ORBIT * G;
       const double *gnew = gold + (size_t) NF_ORBIT * G;
-      delta += gnew[fld * G + i] - gold[fld * G + i];
+      // unscaled orbit grids: x mass/tall as k_scale_dense would (the
+      // factors k_accept stored, the same divisions)
+      delta += gnew[fld * G + i] * R.fac[2 * k + 1] - gold[fld * G + i] * R.fac[2 * k];
     }
     // orbit fields m,r,t,q,p map to committed MASS_S, R_S, T_S, Q_S, P_S
     double *dst = (double *) f.committed + ((size_t) type * NG_COMMITTED + fld) * G + i;
@@ -445,19 +459,19 @@ int launch_rep_orbits(const DevModel &M, const RepArgs &R, const OrbitBatch &b, 
     launch_orbits_dense_fp32(M, quad32, cellsize32, b, s);
   else
     launch_orbits_dense(M, b, s);
-  launch_scale_dense(M, b, s);
-  return 3;
+  // the grids stay unscaled: the merit and commit kernels multiply by
+  // mass/tall where they read them (one pass over the grids less)
+  return 2;
 }
 
 int launch_rep_commit(const DevModel &M, const RepArgs &R, const FitArgs &f, cudaStream_t s)
 {
   const int count = R.count;
-  size_t smem = (size_t) f.Nstack * sizeof(double);
-  // a level-7 stack (171 KiB) leaves room for one CTA per SM: give it the
-  // SM's threads; smaller stacks share the SM between several CTAs
-  const int threads = f.L >= 7 ? 1024 : 512;
-  k_base_inst<<<16, threads, smem, s>>>(R, f);
-  k_eval_terms<<<count * NLAUNCH, threads, smem, s>>>(M, R, f);
+  // levels 0 .. L-1 of a stack in shared memory (43 KiB at L = 7): four
+  // CTAs of 512 threads per SM
+  const size_t smem = (size_t) (((1 << (2 * f.L)) - 1) / 3) * sizeof(double);
+  k_base_inst<<<16, 512, smem, s>>>(R, f);
+  k_eval_terms<<<count * NLAUNCH, 512, smem, s>>>(M, R, f);
   k_accept<<<(count + 127) / 128, 128, 0, s>>>(M, R, f);
   k_compact<<<1, 1024, 0, s>>>(R);
   k_delta_cols<<<148 * 8, 256, 0, s>>>(R, f);
@@ -477,6 +491,8 @@ RepArgs rep_slice(const RepArgs &R, int first, int count, int G)
   S.b_time = R.b_time + 2 * (size_t) first;
   S.b_type = R.b_type + 2 * (size_t) first;
   S.b_norbit = R.b_norbit + 2 * (size_t) first;
+  S.b_tall = R.b_tall + 2 * (size_t) first;
+  S.fac = R.fac + 2 * (size_t) first;
   S.grids = R.grids + (size_t) (2 * first) * NF_ORBIT * G;
   S.vel_try = R.vel_try + 3 * (size_t) first;
   S.F = R.F + 2 * (size_t) NTERM * first;

@@ -24,7 +24,9 @@ struct RepArgs {
   // 2*count orbits: [2k] old velocity, [2k+1] trial velocity
   double *b_pos, *b_vel, *b_mass, *b_time;
   int *b_type, *b_norbit;
-  double *grids;  // 2*count x NF_ORBIT x Ngrid
+  double *grids;  // 2*count x NF_ORBIT x Ngrid, unscaled (the kernels multiply by b_mass / b_tall)
+  const double *b_tall;  // 2*count: each orbit's tall
+  double *fac;           // 2*count: mass / tall of each orbit (k_accept, for the commit)
   double *vel_try;  // count x 3
   double *F;        // 2*count x 9: the stack terms of F_base, F_try (fit_fp64.cu:k_eval_terms)
   double *inst0;    // [4 types][4]: the committed instantaneous terms of the base evaluations

@@ -83,4 +83,80 @@ __device__ __forceinline__ double stack_diff_cta(double *s, const double *d2, co
   return r;
 }
 
+// The same two routines for a pyramid whose finest level (level L) is not
+// stored: fin(i) returns its value at grid index i = iz * 2^L + iR (a sum
+// the caller forms on the fly from global memory), and s holds levels
+// 0 .. L-1 only ((4^L - 1) / 3 doubles: 43 KiB at L = 7 instead of 171 KiB).
+// Level L-1 is summed from fin() in smooth_stack's order; in the misfit a
+// non-leaf node of level L-1 evaluates its four children's leaf terms from
+// fin() and the reference arrays, in the recursion's order.  Same values,
+// same operations: bit-identical to the stored-stack versions.
+template <class F>
+__device__ __forceinline__ void stack_smooth_cta_from(double *s, int L, const F &fin)
+{
+  {
+    const int l = L - 1, n = 1 << l, base = stack_off(l), cn = n << 1;
+    for(int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const int i = idx >> l, j = idx & (n - 1);
+      s[base + idx] = fin((2 * i) * cn + 2 * j) + fin((2 * i + 1) * cn + 2 * j) + fin((2 * i) * cn + 2 * j + 1) +
+                      fin((2 * i + 1) * cn + 2 * j + 1);
+    }
+    __syncthreads();
+  }
+  for(int l = L - 2; l >= 0; l--) {
+    const int n = 1 << l, base = stack_off(l), cb = stack_off(l + 1), cn = n << 1;
+    for(int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      int i = idx >> l, j = idx & (n - 1);
+      s[base + idx] = s[cb + (2 * i) * cn + 2 * j] + s[cb + (2 * i + 1) * cn + 2 * j] +
+                      s[cb + (2 * i) * cn + 2 * j + 1] + s[cb + (2 * i + 1) * cn + 2 * j + 1];
+    }
+    __syncthreads();
+  }
+}
+
+template <class F>
+__device__ __forceinline__ double stack_diff_cta_from(double *s, const F &fin, const double *d2, const double *ref1,
+                                                      const double *ref2, const double *dist, double thresh,
+                                                      int flag, int mod, int L, double R200_20, double lowdisp)
+{
+  const int cbL = stack_off(L);
+  // leaf term of the finest-level node at grid index g
+  auto fine_leaf = [&](int g) {
+    const int node = cbL + g;
+    return stack_leaf(fin(g), d2[node], ref1[node], ref2 ? ref2[node] : 0.0, dist ? dist[node] : 0.0, flag, mod,
+                      R200_20, lowdisp);
+  };
+  for(int l = L - 1; l >= 0; l--) {
+    const int n = 1 << l, base = stack_off(l);
+    const int cb = stack_off(l + 1), cn = n << 1;
+    for(int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const int node = base + idx;
+      const double r1 = ref1[node];
+      double v;
+      if(r1 < thresh) {
+        v = stack_leaf(s[node], d2[node], r1, ref2 ? ref2[node] : 0.0, dist ? dist[node] : 0.0, flag, mod, R200_20,
+                       lowdisp);
+      } else {
+        const int i = idx >> l, j = idx & (n - 1);
+        if(l == L - 1) {
+          v = fine_leaf((2 * i) * cn + 2 * j);
+          v += fine_leaf((2 * i) * cn + 2 * j + 1);
+          v += fine_leaf((2 * i + 1) * cn + 2 * j);
+          v += fine_leaf((2 * i + 1) * cn + 2 * j + 1);
+        } else {
+          v = s[cb + (2 * i) * cn + 2 * j];
+          v += s[cb + (2 * i) * cn + 2 * j + 1];
+          v += s[cb + (2 * i + 1) * cn + 2 * j];
+          v += s[cb + (2 * i + 1) * cn + 2 * j + 1];
+        }
+      }
+      s[node] = v;
+    }
+    __syncthreads();
+  }
+  double r = s[0];
+  __syncthreads();
+  return r;
+}
+
 #endif
