@@ -64,6 +64,8 @@ def parse():
                     help="full model construction measured in the bench line (calc_all + iterations x "
                          "repetitions, both forms); with --row construction it is the one measured")
     ap.add_argument("--construction-scale", type=float, default=1.0)
+    ap.add_argument("--construction-window-gib", type=float, default=0.0,
+                    help="byte budget of a window of repetitions (0: 32 GiB at level 7, 16 GiB below)")
     ap.add_argument("--row", default="all",
                     choices=["all", "calc_all", "construction", "serving", "fill", "sampling", "jeans", "particles"],
                     help="one secondary measurement alone on this workload (a diagnostic line for profiling, "
@@ -455,10 +457,19 @@ def construction_lists(perm, n_per, reps, it):
     return perm[pos].reshape(reps, n_per).astype(np.int32)
 
 
+def _sall(fit, types):
+    """Sall = S + (Sdisp_r + Sdisp_t + Sdisp_p + Sdisp_q) / Srelfac_count per type (main.c:1270)."""
+    return [float(fit[t, 0] + (fit[t, 1] + fit[t, 2] + fit[t, 3] + fit[t, 4]) / (fit[t, 6] if fit[t, 6] else 1.0))
+            for t in types]
+
+
 def run_construction(model, form, iterations, reps, fraction, seed=11, window_bytes=0):
     """calc_all_response_fields, then `iterations` x `reps` repetitions
-    (main.c:83-110) through the C ABI, wall clock with the device synchronised
-    at both ends; Sall (main.c:1270) per type after every iteration."""
+    (main.c:83-110) through the C ABI — the repetitions of the whole run in
+    one galic_optimize_reps call, whose windows of repetitions overlap their
+    orbits with the commits — wall clock with the device synchronised at both
+    ends; Sall (main.c:1270) per type after every iteration, from the fits the
+    call returns per repetition."""
     import torch
 
     from galic_b200 import Context
@@ -466,22 +477,21 @@ def run_construction(model, form, iterations, reps, fraction, seed=11, window_by
     n_per = 1 + int(fraction * model.n)  # main.c:128 with NTask = 1
     perm = np.random.default_rng(seed).permutation(model.n)
     types = [t for t in (1, 2, 3) if model.params.NType[t]]
+    lists = np.concatenate([construction_lists(perm, n_per, reps, it) for it in range(iterations)])
     with Context(model.params) as ctx:
         ctx.load_model(model)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.calc_all_response_fields(form)
         steps_calc = ctx.last_orbit_steps()
-        sall = [ctx.sall()[types].tolist()]
+        sall = [_sall(ctx.fit(), types)]
         t_calc = time.perf_counter() - t0
-        steps_rep = 0
-        for it in range(iterations):
-            ctx.optimize_reps(construction_lists(perm, n_per, reps, it), seed, it * reps, form, window_bytes)
-            steps_rep += ctx.last_orbit_steps()
-            sall.append(ctx.sall()[types].tolist())
+        fits = ctx.optimize_reps(lists, seed, 0, form, window_bytes, fits=True)
+        steps_rep = ctx.last_orbit_steps()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         tries, changes = ctx.counters()
+    sall += [_sall(fits[(it + 1) * reps - 1], types) for it in range(iterations)]
     t_rep = wall - t_calc
     return {"wall_s": wall, "calc_all_s": t_calc, "repetition_phase_s": t_rep, "particles_per_rep": n_per,
             "orbit_steps": int(steps_calc + steps_rep), "repetition_orbit_steps": int(steps_rep),
@@ -540,15 +550,18 @@ def cpu_construction_estimate(name, model, steps_calc, ranks=16, seconds=4.0):
                        f"same shape, extrapolated to {reps_total} repetitions; MPI allreduce not counted")}
 
 
-def measure_construction(name, scale, cpu):
+def measure_construction(name, scale, cpu, window_gib=0.0):
     """Both forms of a full model construction, and GALIC's own C estimate."""
     from galic_b200 import GALIC_FORM_FP32, GALIC_FORM_FP64
 
     cfg = CONSTRUCTION[name]
     model = construction_model(name, scale)
-    # level-7 orbit grids are 640 KiB each: 64 GiB windows hold ~12 repetitions of
-    # config 3 (a window lasts as long as its longest orbit)
-    window = (64 << 30) if model.params.DG_MaxLevel >= 7 else 0
+    # a window's orbit launch lasts as long as its longest orbit: large windows
+    # (two are held at once) — level-7 grids are 640 KiB per orbit, 32 GiB
+    # hold ~6 repetitions of config 3; 16 GiB hold ~500 of config 1
+    window = (32 << 30) if model.params.DG_MaxLevel >= 7 else (16 << 30)
+    if window_gib > 0:
+        window = int(window_gib * (1 << 30))
     res = {"config": cfg["desc"], "particles": model.n, "scale": scale}
     # warm-up: one short run of each form loads every kernel of the path
     for form in (GALIC_FORM_FP64, GALIC_FORM_FP32):
@@ -1091,7 +1104,8 @@ def row_alone(args):
     elif args.row == "serving":
         res = measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
     elif args.row == "construction":
-        res = measure_construction(args.construction, args.construction_scale, args.cpu_seconds > 0)
+        res = measure_construction(args.construction, args.construction_scale, args.cpu_seconds > 0,
+                                   args.construction_window_gib)
     elif args.row == "fill":
         res = measure_fill(model, args.steps, False, measured_fp64_peak(torch))
     elif args.row == "sampling":

@@ -179,7 +179,7 @@ SIGNATURES = [
     ("galic_accumulators", C.c_int, [VP, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     ("galic_calc_all_finish", C.c_int, [VP]),
     ("galic_optimize_rep", C.c_int, [VP, PI, C.c_int, C.c_uint64, C.c_uint32, C.c_int]),
-    ("galic_optimize_reps", C.c_int, [VP, PI, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_int, C.c_size_t]),
+    ("galic_optimize_reps", C.c_int, [VP, PI, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_int, C.c_size_t, PD]),
     ("galic_get_fit", C.c_int, [VP, PD]),
     ("galic_get_counters", C.c_int, [VP, PLL, PLL]),
     ("galic_get_response", C.c_int, [VP, C.c_int, C.c_int, PD]),

@@ -122,14 +122,18 @@ class Context:
         _check(self.lib.galic_optimize_rep(self.h, _ffi.iptr(idx), len(idx), int(seed), int(rep_serial), form),
                "galic_optimize_rep")
 
-    def optimize_reps(self, idx, seed, rep_serial, form=_ffi.GALIC_FORM_FP64, window_bytes=0):
+    def optimize_reps(self, idx, seed, rep_serial, form=_ffi.GALIC_FORM_FP64, window_bytes=0, fits=False):
         """idx: [reps, count] particle indices; repetition r draws its
-        proposals from serial rep_serial + r (galic_optimize_reps)."""
+        proposals from serial rep_serial + r (galic_optimize_reps).  With
+        fits=True returns the [reps, 4, 7] fit after every repetition."""
         idx = np.ascontiguousarray(idx, dtype=np.int32)
         if idx.ndim != 2:
             raise ValueError("idx must be [reps, count]")
+        out = np.zeros((idx.shape[0], 4, 7)) if fits else None
         _check(self.lib.galic_optimize_reps(self.h, _ffi.iptr(idx), idx.shape[1], idx.shape[0], int(seed),
-                                            int(rep_serial), form, int(window_bytes)), "galic_optimize_reps")
+                                            int(rep_serial), form, int(window_bytes),
+                                            _ffi.dptr(out) if fits else None), "galic_optimize_reps")
+        return out
 
     def fit(self):
         """4 x 7 array: per type S, Sdisp_r, Sdisp_t, Sdisp_p, Sdisp_q, Srelfac, Srelfac_count."""

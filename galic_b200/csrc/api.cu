@@ -322,6 +322,7 @@ extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
   CK(dalloc(ctx, &ctx->d_status, 1));
   CK(dalloc(ctx, &ctx->d_next, 1));
   CK(dalloc(ctx, &ctx->d_maxerr, 1));
+  CK(dalloc(ctx, &ctx->d_rep_stats, 2));
 
   DevModel &M = ctx->dm;
   M.V200 = prm->V200;
@@ -385,11 +386,17 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
   dfree(ctx, ctx->d_b_steps);
   dfree(ctx, ctx->d_idx); dfree(ctx, ctx->d_accepted); dfree(ctx, ctx->d_vel_try); dfree(ctx, ctx->d_F); dfree(ctx, ctx->d_inst_v);
   dfree(ctx, ctx->d_inst_cell); dfree(ctx, ctx->d_acc_list); dfree(ctx, ctx->d_acc_n); dfree(ctx, ctx->d_inst0);
-  dfree(ctx, ctx->d_fac);
+  dfree(ctx, ctx->d_fac); dfree(ctx, ctx->d_idx_all); dfree(ctx, ctx->d_fit_hist); dfree(ctx, ctx->d_rep_stats);
   for(int t = 0; t < 4; t++) dfree(ctx, ctx->d_tab32[t]);
   dfree(ctx, ctx->d_cellsize32);
   for(int k = 0; k < 3; k++)
     if(ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if(ctx->stream2) {
+    cudaStreamSynchronize(ctx->stream2);
+    cudaStreamDestroy(ctx->stream2);
+  }
+  for(int k = 0; k < 3; k++)
+    if(ctx->ev2[k]) cudaEventDestroy(ctx->ev2[k]);
   if(ctx->stream) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
@@ -1054,8 +1061,53 @@ extern "C" int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uin
   return fail(ctx, GALIC_OK);
 }
 
+namespace {
+
+// one window of repetitions: reps [r0, r1); dep: some particle of the
+// window was optimised in the window before it
+struct RepWindow {
+  int r0, r1;
+  bool dep;
+};
+
+// the orbit batch of `count` orbit pairs starting at pair `first` of the
+// context's scratch
+OrbitBatch batch_slice(const OrbitBatch &b, int first, int count, int G)
+{
+  OrbitBatch o = b;
+  const size_t k = 2 * (size_t) first;
+  o.count = 2 * count;
+  o.pos = b.pos + 3 * k;
+  o.vel = b.vel + 3 * k;
+  o.mass = b.mass + k;
+  o.timespan = b.timespan + k;
+  o.type = b.type + k;
+  o.grids = b.grids + k * NF_ORBIT * G;
+  o.tall = b.tall + k;
+  o.norbit = b.norbit + k;
+  o.steps = b.steps + k;
+  o.egy_err = b.egy_err + k;
+  o.status = b.status + k;
+  return o;
+}
+
+__global__ void k_window_stats(const long long *steps, const int *status, int n, unsigned long long *total,
+                               int *worst)
+{
+  long long my = 0;
+  int w = 0;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    my += steps[i];
+    w = max(w, status[i]);
+  }
+  if(my) atomicAdd(total, (unsigned long long) my);
+  if(w) atomicMax(worst, w);
+}
+
+}  // namespace
+
 extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, int reps, uint64_t seed,
-                                   uint32_t rep_serial, int form, size_t window_bytes)
+                                   uint32_t rep_serial, int form, size_t window_bytes, double *fits)
 {
   if(!ctx) return GALIC_ERR_INVALID_ARGUMENT;
   if(form != GALIC_FORM_FP64 && form != GALIC_FORM_FP32) return fail(ctx, GALIC_ERR_INVALID_ARGUMENT);
@@ -1076,8 +1128,31 @@ extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, in
   cudaStream_t s = ctx->stream;
   FitArgs f = make_fit_args(ctx);
   int launches = 0;
+  if(reps > 0 && fits) {
+    if(ctx->fit_hist_cap < (size_t) reps) {
+      dfree(ctx, ctx->d_fit_hist);
+      CK(dalloc(ctx, &ctx->d_fit_hist, (size_t) reps * 28));
+      ctx->fit_hist_cap = reps;
+    }
+  }
+  auto record_fit = [&](int r) -> cudaError_t {
+    if(!fits) return cudaSuccess;
+    return cudaMemcpyAsync(ctx->d_fit_hist + (size_t) r * 28, ctx->d_fit, 28 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, s);
+  };
+  auto copy_fits = [&]() -> int {
+    if(!fits || reps == 0) return GALIC_OK;
+    CK(cudaMemcpyAsync(fits, ctx->d_fit_hist, (size_t) reps * 28 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GALIC_OK;
+  };
   if(count == 0) {
-    for(int r = 0; r < reps; r++) launches += launch_global_fit(f, s);
+    for(int r = 0; r < reps; r++) {
+      launches += launch_global_fit(f, s);
+      CK(record_fit(r));
+    }
+    int st = copy_fits();
+    if(st) return st;
     CK(cudaStreamSynchronize(s));
     ctx->last_launches = launches;
     ctx->last_steps = 0;
@@ -1086,48 +1161,112 @@ extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, in
   // per optimised particle: two orbits' dense grids plus their small arrays
   const size_t per_particle = 2 * ((size_t) NF_ORBIT * ctx->G * sizeof(double) + 128);
   if(window_bytes == 0) window_bytes = (size_t) 4 << 30;
+  // the windows: each one's particles all distinct (the old orbit of a
+  // particle optimised twice would depend on the first outcome) and its
+  // grids within window_bytes (at least one repetition)
   std::fill(last_rep.begin(), last_rep.end(), -1);
-  long long tot = 0;
-  int r0 = 0;
-  while(r0 < reps) {
-    // the window [r0, r1): its repetitions' particles all distinct (the old
-    // orbit of a particle optimised twice would depend on the first
-    // outcome) and its grids within window_bytes (at least one repetition)
+  std::vector<RepWindow> wins;
+  int maxM = 0;
+  for(int r0 = 0; r0 < reps;) {
     int r1 = r0;
+    bool dep = false;
     while(r1 < reps) {
       if(r1 > r0 && (size_t) (r1 - r0 + 1) * count * per_particle > window_bytes) break;
-      bool repeat = false;
-      for(int k = 0; k < count && !repeat; k++) repeat = last_rep[idx[(size_t) r1 * count + k]] >= r0;
+      bool repeat = false, before = false;
+      for(int k = 0; k < count; k++) {
+        const int q = last_rep[idx[(size_t) r1 * count + k]];
+        repeat |= q >= r0;
+        before |= q >= 0 && q < r0 && !wins.empty() && q >= wins.back().r0;
+      }
       if(repeat && r1 > r0) break;
+      dep |= before;
       for(int k = 0; k < count; k++) last_rep[idx[(size_t) r1 * count + k]] = r1;
       r1++;
     }
-    const int W = r1 - r0, M = W * count;
-    int st = ensure_rep_scratch(ctx, M);
-    if(st) return st;
-    size_t off_st, off_ost, off_steps;
-    char *h = begin_rep_window(ctx, idx + (size_t) r0 * count, M, &off_st, &off_ost, &off_steps);
-    if(!h) return fail(ctx, GALIC_ERR_CUDA);
-    // the old and trial orbits of the whole window in one launch (a
-    // proposal depends only on P[n].Pos, the targets and its stream, the old
-    // orbit on P[n].Vel, which only n's own optimisation changes) ...
-    RepArgs R = make_rep_args(ctx, M, seed, rep_serial + (uint32_t) r0, count);
-    OrbitBatch b = make_rep_batch(ctx, M);
-    launches += form == GALIC_FORM_FP32 ? launch_rep_orbits(ctx->dm, R, b, s, ctx->d_tab32, ctx->d_cellsize32)
-                                        : launch_rep_orbits(ctx->dm, R, b, s);
-    // ... then each repetition's evaluation against the state its
-    // predecessors committed, acceptance and commit, in order
-    for(int w = 0; w < W; w++) launches += launch_rep_commit(ctx->dm, rep_slice(R, w * count, count, ctx->G), f, s);
-    int status = finish_rep_window(ctx, h, M, off_st, off_ost, off_steps, &tot);
-    if(status) {
-      ctx->last_steps = tot;
-      ctx->last_launches = launches;
-      return fail(ctx, status);
-    }
+    wins.push_back({r0, r1, dep});
+    maxM = std::max(maxM, (r1 - r0) * count);
     r0 = r1;
   }
-  ctx->last_steps = tot;
+  // two halves of the scratch: the orbits of window w + 1 run on the second
+  // stream while window w commits on the context's stream
+  const int nbuf = wins.size() > 1 ? 2 : 1;
+  int st = ensure_rep_scratch(ctx, nbuf * maxM);
+  if(st) return st;
+  if(ctx->idx_cap < (size_t) reps * count) {
+    dfree(ctx, ctx->d_idx_all);
+    CK(dalloc(ctx, &ctx->d_idx_all, (size_t) reps * count));
+    ctx->idx_cap = (size_t) reps * count;
+  }
+  if(!ctx->stream2) {
+    CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+    for(int k = 0; k < 3; k++) CK(cudaEventCreateWithFlags(&ctx->ev2[k], cudaEventDisableTiming));
+  }
+  cudaStream_t so = ctx->stream2;
+  // every index of the call in one copy; staged through pinned memory
+  {
+    char *h = stage(ctx, (size_t) reps * count * sizeof(int));
+    if(!h) return fail(ctx, GALIC_ERR_CUDA);
+    std::memcpy(h, idx, (size_t) reps * count * sizeof(int));
+    CK(cudaMemcpyAsync(ctx->d_idx_all, h, (size_t) reps * count * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(ctx->d_rep_stats, 0, sizeof(unsigned long long) + sizeof(int) * 2, s));
+  // ev2[2]: the context's stream reached this point (scratch allocated, indices uploaded)
+  CK(cudaEventRecord(ctx->ev2[2], s));
+  CK(cudaStreamWaitEvent(so, ctx->ev2[2], 0));
+  const RepArgs Rall = make_rep_args(ctx, nbuf * maxM, seed, rep_serial, count);
+  const OrbitBatch ball = make_rep_batch(ctx, nbuf * maxM);
+  unsigned long long *d_total = (unsigned long long *) ctx->d_rep_stats;
+  int *d_worst = (int *) (ctx->d_rep_stats + 1);
+  for(size_t w = 0; w < wins.size(); w++) {
+    const int half = (int) (w % nbuf), W = wins[w].r1 - wins[w].r0, M = W * count;
+    RepArgs R = rep_slice(Rall, half * maxM, M, ctx->G);
+    R.idx = ctx->d_idx_all + (size_t) wins[w].r0 * count;
+    R.per_rep = count;
+    R.rep_serial = rep_serial + (uint32_t) wins[w].r0;
+    const OrbitBatch b = batch_slice(ball, half * maxM, M, ctx->G);
+    // the half is free once the window before the previous one has
+    // committed; a window whose particles were optimised in the previous
+    // window waits for that window's commit as well
+    if(w >= 2) CK(cudaStreamWaitEvent(so, ctx->ev2[half], 0));
+    if(wins[w].dep && w >= 1) CK(cudaStreamWaitEvent(so, ctx->ev2[1 - half], 0));
+    CK(cudaMemsetAsync(b.status, 0, (size_t) b.count * sizeof(int), so));
+    launches += form == GALIC_FORM_FP32 ? launch_rep_orbits(ctx->dm, R, b, so, ctx->d_tab32, ctx->d_cellsize32)
+                                        : launch_rep_orbits(ctx->dm, R, b, so);
+    cudaEvent_t orbits_done;
+    CK(cudaEventCreateWithFlags(&orbits_done, cudaEventDisableTiming));
+    CK(cudaEventRecord(orbits_done, so));
+    CK(cudaStreamWaitEvent(s, orbits_done, 0));
+    CK(cudaEventDestroy(orbits_done));
+    // each repetition's evaluation against the state its predecessors
+    // committed, acceptance and commit, in order
+    for(int j = 0; j < W; j++) {
+      launches += launch_rep_commit(ctx->dm, rep_slice(R, j * count, count, ctx->G), f, s);
+      CK(record_fit(wins[w].r0 + j));
+    }
+    k_window_stats<<<(b.count + 255) / 256 < 148 ? (b.count + 255) / 256 : 148, 256, 0, s>>>(b.steps, b.status,
+                                                                                             b.count, d_total, d_worst);
+    launches++;
+    CK(cudaEventRecord(ctx->ev2[half], s));
+  }
+  // totals of the call
+  char *h = stage(ctx, 32);
+  if(!h) return fail(ctx, GALIC_ERR_CUDA);
+  CK(cudaMemcpyAsync(h, ctx->d_rep_stats, 16, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h + 16, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  unsigned long long tot;
+  int worst, status;
+  std::memcpy(&tot, h, 8);
+  std::memcpy(&worst, h + 8, 4);
+  std::memcpy(&status, h + 16, 4);
+  ctx->last_steps = (long long) tot;
   ctx->last_launches = launches;
+  if(worst == ORBIT_STEP_CAP) status = std::max(status, (int) GALIC_ERR_STEP_CAP);
+  if(status) return fail(ctx, status);
+  st = copy_fits();
+  if(st) return st;
   return fail(ctx, GALIC_OK);
 }
 

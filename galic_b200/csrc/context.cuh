@@ -17,6 +17,16 @@ struct galic_ctx {
   int status = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream of galic_optimize_reps (the orbits of the next window of
+  // repetitions) and its events: [0], [1] a half of the scratch committed,
+  // [2] the context's stream reached the call's start
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev2[3] = {nullptr, nullptr, nullptr};
+  int *d_idx_all = nullptr;               // every particle index of a galic_optimize_reps call
+  size_t idx_cap = 0;
+  double *d_fit_hist = nullptr;           // [reps][4][7] fits after each repetition
+  size_t fit_hist_cap = 0;
+  unsigned long long *d_rep_stats = nullptr;  // orbit-steps total, worst orbit status
   DevModel dm{};
   int G = 0, Ns = 0, L = 0;
   // tables

@@ -82,27 +82,24 @@ GM_HD double gm_round(double x)
 #define GM_NAN gm_from_bits(0x7ff8000000000000ULL)
 
 /* ---------------------------------------------------------------- log */
+/* The special arguments (NaN, negative, zero, infinity) are selected at the
+ * end instead of returned early, and the subnormal scaling is a selection:
+ * the body is one basic block, so the several logs of an orbit step can be
+ * interleaved by the compiler.  Values equal the early-return form's. */
 GM_HD double gm_log(double x)
 {
   const double ln2_hi = 0x1.62e42fee00000p-1;
   const double ln2_lo = 0x1.a39ef35793c76p-33;
   const double sqrt2 = 0x1.6a09e667f3bcdp+0;
 
-  if(gm_isnan(x)) return x;
-  if(x < 0) return GM_NAN;
-  if(x == 0) return -GM_INF;
-  if(x == GM_INF) return x;
-
-  uint64_t u = gm_bits(x);
-  int k = 0;
-  if((u >> 52) == 0) { /* subnormal: scale up by 2^54 */
-    x *= 0x1.0p54;
-    u = gm_bits(x);
-    k = -54;
-  }
-  k += (int) (u >> 52) - 1023;
+  const int sub = (gm_bits(x) >> 52) == 0; /* +0 and positive subnormals: scale up by 2^54 */
+  const double xs = sub ? x * 0x1.0p54 : x;
+  const uint64_t u = gm_bits(xs);
+  int k = (sub ? -54 : 0) + (int) ((u >> 52) & 0x7ff) - 1023;
   double m = gm_from_bits((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL); /* [1,2) */
-  if(m > sqrt2) { m *= 0.5; k += 1; }
+  const int up = m > sqrt2;
+  m = up ? m * 0.5 : m;
+  k += up;
 
   double f = m - 1.0;        /* exact (Sterbenz) */
   double s = f / (2.0 + f);  /* (m-1)/(m+1) */
@@ -122,7 +119,8 @@ GM_HD double gm_log(double x)
   double hfsq = 0.5 * f * f;
   double dk = (double) k;
   /* log(1+f) = f - (hfsq - s*(hfsq + R)) */
-  return dk * ln2_hi + ((f - (hfsq - (s * (hfsq + R) + dk * ln2_lo))));
+  const double r = dk * ln2_hi + ((f - (hfsq - (s * (hfsq + R) + dk * ln2_lo))));
+  return gm_isnan(x) ? x : (x < 0 ? GM_NAN : (x == 0 ? -GM_INF : (x == GM_INF ? x : r)));
 }
 
 /* ---------------------------------------------------------------- atan */
@@ -171,30 +169,31 @@ GM_HD double gm_atan2(double y, double x)
   const double pi_hi = 0x1.921fb54442d18p+1, pi_lo = 0x1.1a62633145c07p-53;
   const double pio4 = 0x1.921fb54442d18p-1;
 
-  if(gm_isnan(x) || gm_isnan(y)) return x + y;
   double ax = gm_fabs(x), ay = gm_fabs(y);
   int xneg = gm_signbit(x);
 
-  if(ay == 0.0) /* atan2(+-0, x) */
-    return gm_copysign(xneg ? pi_hi : 0.0, y);
-  if(ax == 0.0) return gm_copysign(pio2_hi, y);
-  if(ax == GM_INF) {
-    if(ay == GM_INF) return gm_copysign(xneg ? 3.0 * pio4 : pio4, y);
-    return gm_copysign(xneg ? pi_hi : 0.0, y);
-  }
-  if(ay == GM_INF) return gm_copysign(pio2_hi, y);
-
   /* t = min/max: ax/ay when ay > ax, else ay/ax (one division, one
    * atan_unit for every lane of a warp; the result does not depend on how
-   * the choice is compiled) */
+   * the choice is compiled).  Zero, infinite and NaN arguments take the
+   * special values selected at the end (their t is not used). */
   const int swap = ay > ax;
+  const int special = gm_isnan(x) || gm_isnan(y) || ay == 0.0 || ax == 0.0 || ax == GM_INF || ay == GM_INF;
   double t = (swap ? ax : ay) / (swap ? ay : ax);
+  t = special ? 0.0 : t;
   double a = gm_atan_unit(t);
   double b = (pio2_hi - a) + pio2_lo;
   a = swap ? b : a;
   double c = (pi_hi - a) + pi_lo;
   a = xneg ? c : a;
-  return gm_copysign(a, y);
+  const double regular = gm_copysign(a, y);
+  /* atan2(+-0, x), atan2(y, +-0), the infinite cases, NaN */
+  const double sv = (gm_isnan(x) || gm_isnan(y)) ? x + y
+                    : (ay == 0.0)                 ? gm_copysign(xneg ? pi_hi : 0.0, y)
+                    : (ax == 0.0)                 ? gm_copysign(pio2_hi, y)
+                    : (ax == GM_INF)              ? (ay == GM_INF ? gm_copysign(xneg ? 3.0 * pio4 : pio4, y)
+                                                                  : gm_copysign(xneg ? pi_hi : 0.0, y))
+                                                  : gm_copysign(pio2_hi, y);
+  return special ? sv : regular;
 }
 
 /* ---------------------------------------------------------------- sin/cos */
@@ -272,22 +271,16 @@ GM_HD double gm_cos(double x)
  * gm_cos(x) bit for bit */
 GM_HD void gm_sincos(double x, double *s, double *c)
 {
-  if(gm_isnan(x) || gm_fabs(x) == GM_INF) {
-    *s = GM_NAN;
-    *c = GM_NAN;
-    return;
-  }
-  if(gm_fabs(x) < 0x1.0p-27) {
-    *s = x;
-    *c = 1.0;
-    return;
-  }
+  const int bad = gm_isnan(x) || gm_fabs(x) == GM_INF;
+  const int tiny = gm_fabs(x) < 0x1.0p-27;
   double r;
-  const int q = gm_reduce_pio2(x, &r);
+  const int q = gm_reduce_pio2(bad ? 0.0 : x, &r);
   const double ps = gm_sin_poly(r), pc = gm_cos_poly(r);
   const double sv = (q & 1) ? pc : ps, cv = (q & 1) ? ps : pc;
-  *s = (q & 2) ? -sv : sv;            /* quadrants 2, 3: -sin, -cos poly */
-  *c = ((q + 1) & 2) ? -cv : cv;      /* quadrants 1, 2: -sin, -cos poly */
+  const double sr = (q & 2) ? -sv : sv;       /* quadrants 2, 3: -sin, -cos poly */
+  const double cr = ((q + 1) & 2) ? -cv : cv; /* quadrants 1, 2: -sin, -cos poly */
+  *s = bad ? GM_NAN : (tiny ? x : sr);
+  *c = bad ? GM_NAN : (tiny ? 1.0 : cr);
 }
 
 /* ---------------------------------------------------------------- exp */

@@ -60,13 +60,14 @@ size_t job_count(const galic_job_t &d)
 }
 
 // device bytes of the per-orbit grids of one window of repetitions: the
-// whole iteration, capped at 4 GiB (at least one repetition)
+// whole iteration, capped at 2 GiB (at least one repetition); a job holds
+// two windows at once (galic_optimize_reps)
 size_t job_window_bytes(const galic_job_t &d)
 {
   const size_t G = (size_t) 1 << (2 * d.prm->DG_MaxLevel);
   const size_t per_rep = job_count(d) * 2 * (5 * G * 8 + 128);
   const size_t iter = per_rep * (size_t) std::max(d.reps_per_iteration, 1);
-  return std::max(per_rep, std::min(iter, (size_t) 4 << 30));
+  return std::max(per_rep, std::min(iter, (size_t) 2 << 30));
 }
 
 int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const std::function<double()> &now)
@@ -112,7 +113,7 @@ int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const 
     }
     if(d.reps_per_iteration > 0) {
       if((st = galic_optimize_reps(ctx, idx.data(), n_per, d.reps_per_iteration, d.seed, rep_serial, d.form,
-                                   window)))
+                                   window, nullptr)))
         return done(st);
       r.orbit_steps += galic_last_orbit_steps(ctx);
       rep_serial += (uint32_t) d.reps_per_iteration;
@@ -201,7 +202,7 @@ extern "C" size_t galic_job_device_bytes(const galic_job_t *job)
   size_t b = n * 160;                       // particle state (allvars.h:844-868) and processing order
   b += NF * (16 + 8 + 3 * 8 + 3 * 64);      // FP64 force tables, streaming velocities, FP32 quad tables
   b += G * (8 + 4 + 320 + 640) + Ns * 520;  // geometry, committed grids, fixed point, stacks, targets
-  b += job_window_bytes(*job) + job_count(*job) * 64;  // per-orbit grids of a window of repetitions
+  b += 2 * job_window_bytes(*job) + job_count(*job) * 64;  // per-orbit grids of two windows of repetitions
   b += (size_t) 16 << 20;                   // fit scratch, allocator granularity
   return b;
 }

@@ -177,14 +177,17 @@ int galic_optimize_rep(galic_ctx *ctx, const int *idx, int count, uint64_t seed,
  * orbits of a window of repetitions in one launch (a proposal depends only
  * on P[n].Pos, the targets and its stream, and the old orbit on P[n].Vel,
  * which only n's own optimisation changes), then evaluates, accepts and
- * commits the repetitions in order.  A window ends before a particle
- * repeats and when its per-orbit grids (2 x 5 x DG_Ngrid doubles per
- * particle) would pass window_bytes (0: 4 GiB; at least one repetition).
- * No counterpart function in the reference: it replaces the loop of
- * main.c:94-100 (optimize_some_particles, main.c:120-146, is the caller's
- * choice of idx). */
+ * commits the repetitions in order; the orbits of the next window run on a
+ * second stream meanwhile.  A window ends before a particle repeats and when
+ * its per-orbit grids (2 x 5 x DG_Ngrid doubles per particle) would pass
+ * window_bytes (0: 4 GiB; at least one repetition); two windows' grids are
+ * held at once.  fits, when not NULL, receives the 4 x 7 galic_get_fit
+ * values after every repetition ([reps][4][7]; GALIC logs them per
+ * iteration, main.c:1220-1285).  No counterpart function in the reference:
+ * it replaces the loop of main.c:94-100 (optimize_some_particles,
+ * main.c:120-146, is the caller's choice of idx). */
 int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, int reps, uint64_t seed, uint32_t rep_serial,
-                        int form, size_t window_bytes);
+                        int form, size_t window_bytes, double *fits);
 
 /* Merit values of the last calc_global_fit: per type (index 1..3)
  * S, Sdisp_r, Sdisp_t, Sdisp_p, Sdisp_q, Srelfac, Srelfac_count

@@ -102,3 +102,23 @@ def test_invalid_windows_rejected():
                 ctx.optimize_reps(np.array(bad), 1, 0)
             assert e.value.status == 1
         ctx.optimize_reps(np.zeros((3, 0), dtype=np.int32), 1, 0)
+
+
+def test_windows_report_the_fit_after_every_repetition():
+    """fits=True returns the galic_get_fit values after each repetition: the
+    same as reading the fit after each galic_optimize_rep call."""
+    m = synth.config_halo_disk(n_halo=800, n_disk=300, level=5, seed=54)
+    lists = cycling_lists(m.n, 60, 25, 5)
+    want = []
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.calc_all_response_fields()
+        for r in range(len(lists)):
+            ctx.optimize_rep(lists[r], 3, 10 + r)
+            want.append(ctx.fit())
+    with Context(m.params) as ctx:
+        ctx.load_model(m)
+        ctx.calc_all_response_fields()
+        got = ctx.optimize_reps(lists, 3, 10, window_bytes=4 * 60 * 2 * 5 * 1024 * 8 + 1, fits=True)
+    assert got.shape == (len(lists), 4, 7)
+    assert np.array_equal(got, np.stack(want), equal_nan=True)
