@@ -395,7 +395,7 @@ extern "C" void galic_ctx_destroy(galic_ctx *ctx)
     cudaStreamSynchronize(ctx->stream2);
     cudaStreamDestroy(ctx->stream2);
   }
-  for(int k = 0; k < 3; k++)
+  for(int k = 0; k < 5; k++)
     if(ctx->ev2[k]) cudaEventDestroy(ctx->ev2[k]);
   if(ctx->stream) {
     cudaStreamSynchronize(ctx->stream);
@@ -1199,7 +1199,7 @@ extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, in
   }
   if(!ctx->stream2) {
     CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
-    for(int k = 0; k < 3; k++) CK(cudaEventCreateWithFlags(&ctx->ev2[k], cudaEventDisableTiming));
+    for(int k = 0; k < 5; k++) CK(cudaEventCreateWithFlags(&ctx->ev2[k], cudaEventDisableTiming));
   }
   cudaStream_t so = ctx->stream2;
   // every index of the call in one copy; staged through pinned memory
@@ -1233,11 +1233,11 @@ extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, in
     CK(cudaMemsetAsync(b.status, 0, (size_t) b.count * sizeof(int), so));
     launches += form == GALIC_FORM_FP32 ? launch_rep_orbits(ctx->dm, R, b, so, ctx->d_tab32, ctx->d_cellsize32)
                                         : launch_rep_orbits(ctx->dm, R, b, so);
-    cudaEvent_t orbits_done;
-    CK(cudaEventCreateWithFlags(&orbits_done, cudaEventDisableTiming));
-    CK(cudaEventRecord(orbits_done, so));
-    CK(cudaStreamWaitEvent(s, orbits_done, 0));
-    CK(cudaEventDestroy(orbits_done));
+    // ev2[3 + half]: this window's orbits are done (a wait takes the event's
+    // state at the time of the wait, so the event can be recorded again for
+    // the window after next)
+    CK(cudaEventRecord(ctx->ev2[3 + half], so));
+    CK(cudaStreamWaitEvent(s, ctx->ev2[3 + half], 0));
     // each repetition's evaluation against the state its predecessors
     // committed, acceptance and commit, in order
     for(int j = 0; j < W; j++) {

@@ -19,9 +19,10 @@ struct galic_ctx {
   cudaStream_t stream = nullptr;
   // second stream of galic_optimize_reps (the orbits of the next window of
   // repetitions) and its events: [0], [1] a half of the scratch committed,
-  // [2] the context's stream reached the call's start
+  // [2] the context's stream reached the call's start, [3], [4] a half's
+  // orbits done
   cudaStream_t stream2 = nullptr;
-  cudaEvent_t ev2[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev2[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int *d_idx_all = nullptr;               // every particle index of a galic_optimize_reps call
   size_t idx_cap = 0;
   double *d_fit_hist = nullptr;           // [reps][4][7] fits after each repetition

@@ -375,10 +375,18 @@ __device__ __forceinline__ bool orbit_step(const DevModel &M, const LogConsts &L
   sink(make_deposit(dt, s.cell, s.proj));
   for(int i = 0; i < 3; i++) s.v[i] += 0.5 * dt * s.a[i];
   for(int i = 0; i < 3; i++) s.x[i] += dt * s.v[i];
-  FgCoord fc = fg_coord(M, L, s.x);
+  // the four log coordinates of the new position (force grid: grid.c:130-136;
+  // density grid: grid.c:494-534) in one block, so that their independent
+  // chains interleave; the same expressions as fg_coord and density_cell
+  const double Rxy = sqrt(s.x[0] * s.x[0] + s.x[1] * s.x[1]), az = gm_fabs(s.x[2]);
+  const double lf0 = gm_log(Rxy / M.FG_Rmin + 1.0), lf1 = gm_log(az / M.FG_Rmin + 1.0);
+  const double ld0 = gm_log(Rxy / M.DG_Rmin + 1.0), ld1 = gm_log(az / M.DG_Rmin + 1.0);
+  FgCoord fc;
+  fc.jdbl = lf0 / L.lfg;
+  fc.idbl = lf1 / L.lfg;
   forcegrid_acc(M, fc, s.x, s.a);
   for(int i = 0; i < 3; i++) s.v[i] += 0.5 * dt * s.a[i];
-  s.cell = density_cell(M, L, s.x);
+  s.cell = cell_from_b((ld0 / L.ldg) - 0.5, (ld1 / L.ldg) - 0.5, M.DG_Nbin);
   if(with_proj) s.proj = project(M, s.tovs, s.type, fc, s.x, s.v);
   sink(make_deposit(dt, s.cell, s.proj));
   s.tall += dt;
