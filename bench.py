@@ -1062,6 +1062,12 @@ def ours_arm(args, rank, world, local_rank):
 
 
 def main():
+    # every context drives two streams (galic_optimize_reps overlaps the next
+    # window's orbits with the current window's commits) and the serving loop
+    # runs up to 16 contexts: give the process 32 hardware work queues
+    # instead of the default 8, so that a stream waiting on an event does not
+    # hold up the streams that share its queue (read when CUDA starts)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -273,7 +273,19 @@ extern "C" int galic_get_params(const galic_ctx *ctx, galic_params_t *out)
 
 extern "C" int galic_last_status(const galic_ctx *ctx) { return ctx ? ctx->status : GALIC_ERR_INVALID_ARGUMENT; }
 
+namespace galic_internal {
+int ctx_create(const galic_params_t *prm, int priority, galic_ctx **out);
+}
+
 extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
+{
+  return galic_internal::ctx_create(prm, 0, out);
+}
+
+// priority: of the context's streams (cudaStreamCreateWithPriority; 0 is the
+// default, lower numbers run first): the serving loop gives jobs admitted
+// while few others run precedence over later ones
+int galic_internal::ctx_create(const galic_params_t *prm, int priority, galic_ctx **out)
 {
   galic_ctx *ctx = nullptr;
   if(!out) return GALIC_ERR_INVALID_ARGUMENT;
@@ -289,7 +301,8 @@ extern "C" int galic_ctx_create(const galic_params_t *prm, galic_ctx **out)
   ctx->prm = *prm;
   cudaGetDevice(&ctx->device);
   CK(keep_pool_memory(ctx->device));
-  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  ctx->priority = priority;
+  CK(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, priority));
   for(int k = 0; k < 3; k++) CK(cudaEventCreate(&ctx->ev[k]));
   CK(prepare_fit_kernels());
   ctx->L = prm->DG_MaxLevel;
@@ -1198,7 +1211,7 @@ extern "C" int galic_optimize_reps(galic_ctx *ctx, const int *idx, int count, in
     ctx->idx_cap = (size_t) reps * count;
   }
   if(!ctx->stream2) {
-    CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, ctx->priority));
     for(int k = 0; k < 5; k++) CK(cudaEventCreateWithFlags(&ctx->ev2[k], cudaEventDisableTiming));
   }
   cudaStream_t so = ctx->stream2;

@@ -17,6 +17,7 @@ struct galic_ctx {
   int status = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  int priority = 0;  // of the context's streams
   // second stream of galic_optimize_reps (the orbits of the next window of
   // repetitions) and its events: [0], [1] a half of the scratch committed,
   // [2] the context's stream reached the call's start, [3], [4] a half's
@@ -98,6 +99,8 @@ struct galic_ctx {
 };
 
 namespace galic_internal {
+// galic_ctx_create with a stream priority (the serving loop's jobs)
+int ctx_create(const galic_params_t *prm, int priority, galic_ctx **out);
 // fixed-point shift of every committed grid of the context for `form`
 void set_shifts(galic_ctx *ctx, int *shift, int form);
 // FP32 force tables of the context, rebuilt after any table upload

@@ -31,6 +31,11 @@
 
 #include "galic_gpu.h"
 
+namespace galic_internal {
+// galic_ctx_create with a stream priority (api.cu)
+int ctx_create(const galic_params_t *prm, int priority, galic_ctx **out);
+}
+
 namespace {
 
 struct Job {
@@ -70,10 +75,11 @@ size_t job_window_bytes(const galic_job_t &d)
   return std::max(per_rep, std::min(iter, (size_t) 2 << 30));
 }
 
-int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const std::function<double()> &now)
+int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const std::function<double()> &now,
+            int priority)
 {
   galic_ctx *ctx = nullptr;
-  int st = galic_ctx_create(d.prm, &ctx);
+  int st = galic_internal::ctx_create(d.prm, priority, &ctx);
   if(st) return st;
   auto done = [&](int status) {
     galic_ctx_destroy(ctx);
@@ -158,11 +164,14 @@ struct galic_server {
     return nullptr;
   }
 
+  int prio_least = 0, prio_greatest = 0;  // cudaDeviceGetStreamPriorityRange
+
   void worker()
   {
     cudaSetDevice(device);
     for(;;) {
       Job *j = nullptr;
+      int prio = 0;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return (j = pick()) != nullptr || (stopping && queue.empty()); });
@@ -173,9 +182,14 @@ struct galic_server {
         peak_running = std::max(peak_running, running);
         j->state = 1;
         j->res.t_admit = now();
+        // a job admitted while k others run gets the k-th highest stream
+        // priority: earlier jobs run first where they compete (approximates
+        // first-come first-served, which lowers the median time to
+        // convergence; every job keeps progressing)
+        prio = std::min(prio_least, prio_greatest + (running - 1));
       }
       double t_first = -1;
-      const int st = run_job(j->desc, j->res, &t_first, [&] { return now(); });
+      const int st = run_job(j->desc, j->res, &t_first, [&] { return now(); }, prio);
       {
         std::lock_guard<std::mutex> lk(mu);
         j->res.status = st;
@@ -217,6 +231,10 @@ extern "C" int galic_server_create(size_t hbm_budget_bytes, int workers, galic_s
   if(cudaGetDeviceCount(&count) != cudaSuccess || count < 1) return GALIC_ERR_NO_DEVICE;
   galic_server *s = new galic_server();
   s->device = dev;
+  if(cudaDeviceGetStreamPriorityRange(&s->prio_least, &s->prio_greatest) != cudaSuccess) {
+    cudaGetLastError();
+    s->prio_least = s->prio_greatest = 0;
+  }
   s->budget = hbm_budget_bytes;
   for(int w = 0; w < workers; w++) s->workers.emplace_back([s] { s->worker(); });
   *out = s;
