@@ -65,14 +65,14 @@ size_t job_count(const galic_job_t &d)
 }
 
 // device bytes of the per-orbit grids of one window of repetitions: the
-// whole iteration, capped at 2 GiB (at least one repetition); a job holds
+// whole iteration, capped at 8 GiB (at least one repetition); a job holds
 // two windows at once (galic_optimize_reps)
 size_t job_window_bytes(const galic_job_t &d)
 {
   const size_t G = (size_t) 1 << (2 * d.prm->DG_MaxLevel);
   const size_t per_rep = job_count(d) * 2 * (5 * G * 8 + 128);
   const size_t iter = per_rep * (size_t) std::max(d.reps_per_iteration, 1);
-  return std::max(per_rep, std::min(iter, (size_t) 2 << 30));
+  return std::max(per_rep, std::min(iter, (size_t) 8 << 30));
 }
 
 int run_job(const galic_job_t &d, galic_job_result_t &r, double *t_first, const std::function<double()> &now,
