@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--serve-gap", type=float, default=0.5, help="mean Poisson gap between requests, s")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="particle-count factor of the requests")
     ap.add_argument("--serve-workers", type=int, default=16, help="concurrent jobs of the serving loop")
+    ap.add_argument("--serve-hbm-fraction", type=float, default=0.5,
+                    help="share of the free HBM the serving loop may hold for its jobs")
     ap.add_argument("--construction", default="halo", choices=["halo", "composite", "none"],
                     help="full model construction measured in the bench line (calc_all + iterations x "
                          "repetitions, both forms); with --row construction it is the one measured")
@@ -617,7 +619,7 @@ SERVE_SCHEDULE = {"iterations_max": 20, "reps_per_iteration": 100, "fraction_per
                   "converge_rel": 0.01}
 
 
-def measure_serving(count, mean_gap, scale, torch, workers=16):
+def measure_serving(count, mean_gap, scale, torch, workers=16, hbm_fraction=0.5):
     """The serving stream's first `count` requests (Poisson arrivals, mean gap
     `mean_gap`) through the serving loop: admission by HBM budget, concurrent
     jobs on one GPU, each job calc_all plus iterations of 100 repetitions
@@ -633,7 +635,7 @@ def measure_serving(count, mean_gap, scale, torch, workers=16):
     rng = np.random.default_rng(6)
     arrivals = np.cumsum(rng.exponential(mean_gap, count))
     free, total = torch.cuda.mem_get_info()
-    budget = int(0.5 * free)
+    budget = int(hbm_fraction * free)
     sch = SERVE_SCHEDULE
     schedule = dict(form=GALIC_FORM_FP32, max_iterations=sch["iterations_max"],
                     reps_per_iteration=sch["reps_per_iteration"], fraction_per_rep=sch["fraction_per_rep"],
@@ -999,7 +1001,8 @@ def ours_arm(args, rank, world, local_rank):
         construction = (measure_construction(args.construction, args.construction_scale,
                                              world == 1 and args.cpu_seconds > 0)
                         if args.construction != "none" else None)
-        serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
+        serving = (measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers,
+                                   args.serve_hbm_fraction)
                    if args.serve_requests > 0 else None)
         achieved = steps[-1] * FLOP_PER_STEP / (kern_avg * 1e-3) / 1e12
         fp32_err = fp32_error(ctx, model)
@@ -1108,7 +1111,8 @@ def row_alone(args):
                    "orbit_steps_per_s": ctx.last_orbit_steps() / (statistics.mean(ms) * 1e-3),
                    "max_energy_error": ctx.last_max_energy_error()}
     elif args.row == "serving":
-        res = measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers)
+        res = measure_serving(args.serve_requests, args.serve_gap, args.serve_scale, torch, args.serve_workers,
+                              args.serve_hbm_fraction)
     elif args.row == "construction":
         res = measure_construction(args.construction, args.construction_scale, args.cpu_seconds > 0,
                                    args.construction_window_gib)
