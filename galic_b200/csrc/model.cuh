@@ -31,6 +31,9 @@ struct DevModel {
   // grid geometry
   int FG_Nbin, DG_Nbin, DG_L, EG_L, DG_Ngrid, DG_Nstack;
   double FG_Rmin, FG_Fac, DG_Rmin, DG_Fac, EG_Rmin, EG_Fac;
+  // correctly rounded reciprocals of the orbit step's per-model divisors
+  // FG_Rmin, DG_Rmin, log(FG_Fac), log(DG_Fac) (set_step_reciprocals)
+  double inv_FG_Rmin, inv_DG_Rmin, inv_lfg, inv_ldg;
   // tables (device pointers, reference layouts)
   const double2 *fg_acc;  // {FG_DPotDR, FG_DPotDz}[iz*FG_Nbin+iR]
   const double *fg_pot;
@@ -38,6 +41,32 @@ struct DevModel {
   const double *cellsize;  // DG_CellSize
   long long step_cap;
 };
+
+// Host side: the reciprocals div_by needs, from the same values the step
+// divides by (gm_log is the same function on host and device).
+inline void set_step_reciprocals(DevModel &M)
+{
+  M.inv_FG_Rmin = 1.0 / M.FG_Rmin;
+  M.inv_DG_Rmin = 1.0 / M.DG_Rmin;
+  M.inv_lfg = 1.0 / gm_log(M.FG_Fac);
+  M.inv_ldg = 1.0 / gm_log(M.DG_Fac);
+}
+
+// a / b for a divisor b fixed per model, given y = 1/b correctly rounded:
+// q0 = a*y, then one correction q0 + (a - b*q0)*y with both steps fused
+// (Markstein, IBM J. Res. Develop. 34(1), 1990).  It returns the correctly
+// rounded quotient a / b whenever b, y and a/b are normal numbers: checked for
+// every pair of significands at precisions 6 to 12 and on 1e8 random binary64
+// pairs (tests/test_gmath.py), and by the per-orbit bit-exact parity tests.
+// Where the step uses it, a tiny or subnormal quotient is added to 1.0 and an
+// infinite one (NaN here) only ever fails an in-grid test, so the step's
+// results are those of the division in every case.  Three dependent FP64
+// operations instead of an IEEE division's iteration and range checks.
+__device__ __forceinline__ double div_by(double a, double b, double y)
+{
+  const double q0 = a * y;
+  return fma(fma(-q0, b, a), y, q0);
+}
 
 // ------------------------------------------------------------ analytic parts
 
@@ -379,14 +408,16 @@ __device__ __forceinline__ bool orbit_step(const DevModel &M, const LogConsts &L
   // density grid: grid.c:494-534) in one block, so that their independent
   // chains interleave; the same expressions as fg_coord and density_cell
   const double Rxy = sqrt(s.x[0] * s.x[0] + s.x[1] * s.x[1]), az = gm_fabs(s.x[2]);
-  const double lf0 = gm_log(Rxy / M.FG_Rmin + 1.0), lf1 = gm_log(az / M.FG_Rmin + 1.0);
-  const double ld0 = gm_log(Rxy / M.DG_Rmin + 1.0), ld1 = gm_log(az / M.DG_Rmin + 1.0);
+  const double lf0 = gm_log(div_by(Rxy, M.FG_Rmin, M.inv_FG_Rmin) + 1.0);
+  const double lf1 = gm_log(div_by(az, M.FG_Rmin, M.inv_FG_Rmin) + 1.0);
+  const double ld0 = gm_log(div_by(Rxy, M.DG_Rmin, M.inv_DG_Rmin) + 1.0);
+  const double ld1 = gm_log(div_by(az, M.DG_Rmin, M.inv_DG_Rmin) + 1.0);
   FgCoord fc;
-  fc.jdbl = lf0 / L.lfg;
-  fc.idbl = lf1 / L.lfg;
+  fc.jdbl = div_by(lf0, L.lfg, M.inv_lfg);
+  fc.idbl = div_by(lf1, L.lfg, M.inv_lfg);
   forcegrid_acc(M, fc, s.x, s.a);
   for(int i = 0; i < 3; i++) s.v[i] += 0.5 * dt * s.a[i];
-  s.cell = cell_from_b((ld0 / L.ldg) - 0.5, (ld1 / L.ldg) - 0.5, M.DG_Nbin);
+  s.cell = cell_from_b(div_by(ld0, L.ldg, M.inv_ldg) - 0.5, div_by(ld1, L.ldg, M.inv_ldg) - 0.5, M.DG_Nbin);
   if(with_proj) s.proj = project(M, s.tovs, s.type, fc, s.x, s.v);
   sink(make_deposit(dt, s.cell, s.proj));
   s.tall += dt;

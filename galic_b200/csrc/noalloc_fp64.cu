@@ -282,6 +282,7 @@ extern "C" int galic_orbit_responses_noalloc(const galic_params_t *prm, const do
   M.DG_Fac = prm->DG_Fac;
   M.EG_Rmin = prm->EG_Rmin;
   M.EG_Fac = prm->EG_Fac;
+  set_step_reciprocals(M);
   M.fg_acc = (const double2 *) d_fg_acc2;
   M.fg_pot = d_fg_pot;
   M.cellsize = d_cellsize;
