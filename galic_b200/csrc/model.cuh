@@ -272,12 +272,15 @@ __device__ __forceinline__ double vstream_at(const DevModel &M, const FgCoord &c
          __ldg(&V[(k.iz + 1) * N + (k.iR + 1)]) * (k.fR) * (k.fz);
 }
 
-// velocity projections of orbit_response.c:222-273 (= 338-391)
+// velocity projections of orbit_response.c:222-273 (= 338-391).  Rxy is
+// sqrt(x[0]*x[0] + x[1]*x[1]), which the caller has already formed: it is the
+// reference's q = sqrt(q2) bit for bit whenever x is finite (with
+// Z = (0, 0, -1), Q = (-x1, x0, +-0) exactly, so q2 = x1*x1 + x0*x0 + 0).
 struct Proj {
   double vr2, vt2, vq2, vp2;
 };
 __device__ __forceinline__ Proj project(const DevModel &M, int tovs, int type, const FgCoord &fc, const double *x,
-                                        const double *v)
+                                        const double *v, double Rxy)
 {
   Proj o;
   double r2, v_dot_x, q, q2, vq, v_dot_Q, t2, v_dot_T, vstr;
@@ -291,7 +294,7 @@ __device__ __forceinline__ Proj project(const DevModel &M, int tovs, int type, c
     Q1 = x[0];
     q2 = Q0 * Q0 + Q1 * Q1;
     v_dot_Q = v[0] * Q0 + v[1] * Q1;
-    q = sqrt(q2);
+    q = Rxy;  // sqrt(q2): the same sum in the other order
     vq = v_dot_Q / q;
     o.vq2 = vq * vq;
     vstr = vstream_at(M, fc, type);
@@ -306,7 +309,8 @@ __device__ __forceinline__ Proj project(const DevModel &M, int tovs, int type, c
     Q2 = x[0] * Z1 - x[1] * Z0;
     q2 = Q0 * Q0 + Q1 * Q1 + Q2 * Q2;
     v_dot_Q = v[0] * Q0 + v[1] * Q1 + v[2] * Q2;
-    q = sqrt(q2);
+    q = Rxy;
+    if(!(gm_fabs(x[0] + x[1] + x[2]) < GM_INF)) q = sqrt(q2);  // non-finite (or huge) x: as the reference
     vq = v_dot_Q / q;
     o.vq2 = vq * vq;
     vstr = vstream_at(M, fc, type);
@@ -384,7 +388,7 @@ __device__ __forceinline__ void orbit_begin(const DevModel &M, const LogConsts &
   forcegrid_acc(M, fc, s.x, s.a);
   s.cell = density_cell(M, L, s.x);
   s.E0 = 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]) + forcegrid_pot(M, L, s.x);
-  if(with_proj) s.proj = project(M, s.tovs, type, fc, s.x, s.v);
+  if(with_proj) s.proj = project(M, s.tovs, type, fc, s.x, s.v, sqrt(s.x[0] * s.x[0] + s.x[1] * s.x[1]));
 }
 
 // One iteration of the do-loop of orbit_response.c:211-458 (with_proj) or
@@ -418,7 +422,7 @@ __device__ __forceinline__ bool orbit_step(const DevModel &M, const LogConsts &L
   forcegrid_acc(M, fc, s.x, s.a);
   for(int i = 0; i < 3; i++) s.v[i] += 0.5 * dt * s.a[i];
   s.cell = cell_from_b(div_by(ld0, L.ldg, M.inv_ldg) - 0.5, div_by(ld1, L.ldg, M.inv_ldg) - 0.5, M.DG_Nbin);
-  if(with_proj) s.proj = project(M, s.tovs, s.type, fc, s.x, s.v);
+  if(with_proj) s.proj = project(M, s.tovs, s.type, fc, s.x, s.v, Rxy);
   sink(make_deposit(dt, s.cell, s.proj));
   s.tall += dt;
   double radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];

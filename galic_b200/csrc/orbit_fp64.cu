@@ -184,13 +184,15 @@ struct NodeSink64 {
     const double z0r0 = oz ? d.m01 : d.m00, z0r1 = oz ? d.m11 : d.m10;  // slot z-parity 0: dz = oz
     const double z1r0 = oz ? d.m00 : d.m01, z1r1 = oz ? d.m10 : d.m11;
     const double w[4] = {orr ? z0r1 : z0r0, orr ? z0r0 : z0r1, orr ? z1r1 : z1r0, orr ? z1r0 : z1r1};
+    // the node sums are this form's own partial sums (the reference adds
+    // every product to the grid bin in turn): fused, one rounding per term
 #pragma unroll
     for(int k = 0; k < 4; k++) {
       a[k][0] += w[k];
-      a[k][1] += w[k] * d.p.vr2;
-      a[k][2] += w[k] * d.p.vt2;
-      a[k][3] += w[k] * d.p.vq2;
-      a[k][4] += w[k] * d.p.vp2;
+      a[k][1] = fma(w[k], d.p.vr2, a[k][1]);
+      a[k][2] = fma(w[k], d.p.vt2, a[k][2]);
+      a[k][3] = fma(w[k], d.p.vq2, a[k][3]);
+      a[k][4] = fma(w[k], d.p.vp2, a[k][4]);
     }
   }
 };
