@@ -372,7 +372,7 @@ int galic_internal::ctx_create(const galic_params_t *prm, int priority, galic_ct
   M.DG_Fac = prm->DG_Fac;
   M.EG_Rmin = prm->EG_Rmin;
   M.EG_Fac = prm->EG_Fac;
-  set_step_reciprocals(M);
+  set_step_constants(M);
   M.fg_acc = ctx->d_fg_acc;
   M.fg_pot = ctx->d_fg_pot;
   for(int t = 0; t < 4; t++) M.vstream[t] = ctx->d_vstream[t];

@@ -31,8 +31,10 @@ struct DevModel {
   // grid geometry
   int FG_Nbin, DG_Nbin, DG_L, EG_L, DG_Ngrid, DG_Nstack;
   double FG_Rmin, FG_Fac, DG_Rmin, DG_Fac, EG_Rmin, EG_Fac;
-  // correctly rounded reciprocals of the orbit step's per-model divisors
-  // FG_Rmin, DG_Rmin, log(FG_Fac), log(DG_Fac) (set_step_reciprocals)
+  // log(FG_Fac), log(DG_Fac), log(EG_Fac) and the correctly rounded
+  // reciprocals of the orbit step's per-model divisors FG_Rmin, DG_Rmin,
+  // log(FG_Fac), log(DG_Fac) (set_step_constants)
+  double lfg, ldg, leg;
   double inv_FG_Rmin, inv_DG_Rmin, inv_lfg, inv_ldg;
   // tables (device pointers, reference layouts)
   const double2 *fg_acc;  // {FG_DPotDR, FG_DPotDz}[iz*FG_Nbin+iR]
@@ -42,14 +44,18 @@ struct DevModel {
   long long step_cap;
 };
 
-// Host side: the reciprocals div_by needs, from the same values the step
-// divides by (gm_log is the same function on host and device).
-inline void set_step_reciprocals(DevModel &M)
+// Host side: the logs of the grid factors (gm_log is the same function on
+// host and device, so these equal make_log_consts' values) and the
+// reciprocals div_by needs, from the same values the step divides by.
+inline void set_step_constants(DevModel &M)
 {
+  M.lfg = gm_log(M.FG_Fac);
+  M.ldg = gm_log(M.DG_Fac);
+  M.leg = gm_log(M.EG_Fac);
   M.inv_FG_Rmin = 1.0 / M.FG_Rmin;
   M.inv_DG_Rmin = 1.0 / M.DG_Rmin;
-  M.inv_lfg = 1.0 / gm_log(M.FG_Fac);
-  M.inv_ldg = 1.0 / gm_log(M.DG_Fac);
+  M.inv_lfg = 1.0 / M.lfg;
+  M.inv_ldg = 1.0 / M.ldg;
 }
 
 // a / b for a divisor b fixed per model, given y = 1/b correctly rounded:
@@ -105,6 +111,16 @@ __device__ __forceinline__ double bulge_pot(const DevModel &M, const double *pos
 struct LogConsts {
   double lfg, ldg, leg;
 };
+// the same values from the parameter space, where set_step_constants put
+// them (kernels whose model went through it: no registers held for them)
+__device__ __forceinline__ LogConsts step_log_consts(const DevModel &M)
+{
+  LogConsts c;
+  c.lfg = M.lfg;
+  c.ldg = M.ldg;
+  c.leg = M.leg;
+  return c;
+}
 __device__ __forceinline__ LogConsts make_log_consts(const DevModel &M)
 {
   LogConsts c;

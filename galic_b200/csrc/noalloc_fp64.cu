@@ -138,7 +138,7 @@ enum { ST_ACTIVE = 0, ST_FINISH = 1, ST_DONE = 2 };
 __global__ void __launch_bounds__(128, 3) k_noalloc_orbits(DevModel M, NoAllocArgs A)
 {
   __shared__ Slots queues[4];
-  LogConsts L = make_log_consts(M);
+  LogConsts L = step_log_consts(M);
   const int G = M.DG_Ngrid;
   OrbitState s;
   ParkSink sink;
@@ -282,7 +282,7 @@ extern "C" int galic_orbit_responses_noalloc(const galic_params_t *prm, const do
   M.DG_Fac = prm->DG_Fac;
   M.EG_Rmin = prm->EG_Rmin;
   M.EG_Fac = prm->EG_Fac;
-  set_step_reciprocals(M);
+  set_step_constants(M);
   M.fg_acc = (const double2 *) d_fg_acc2;
   M.fg_pot = d_fg_pot;
   M.cellsize = d_cellsize;

@@ -64,7 +64,7 @@ __global__ void k_orbits_dense(DevModel M, OrbitBatch b)
 {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if(k >= b.count) return;
-  LogConsts L = make_log_consts(M);
+  LogConsts L = step_log_consts(M);
   const size_t G = (size_t) M.DG_Ngrid;
   double *base = b.grids + (size_t) k * NF_ORBIT * G;
   DenseSink sink{base + F_M * G, base + F_R * G, base + F_T * G, base + F_Q * G, base + F_P * G, M.DG_Nbin,
@@ -213,7 +213,7 @@ template <int MINB>
 __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(DevModel M, CalcAllArgs A)
 {
   __shared__ WarpQueueT<kPer64, double> queues[CALC_ALL_BLOCK_FP64 / 32];
-  LogConsts L = make_log_consts(M);
+  LogConsts L = step_log_consts(M);
   const int G = M.DG_Ngrid;
   OrbitState s;
   NodeSink64<kPer64> sink;
@@ -283,7 +283,7 @@ __global__ void k_instantaneous(DevModel M, int n, int first, int stride, const 
 {
   int k = first + (blockIdx.x * blockDim.x + threadIdx.x) * stride;
   if(k >= n) return;
-  LogConsts L = make_log_consts(M);
+  LogConsts L = step_log_consts(M);
   int t = type[k];
   double d[4];
   disp_components(M, L, t, &pos[3 * k], &vel[3 * k], d);
