@@ -375,7 +375,8 @@ __device__ __forceinline__ Deposit make_deposit(double dt, const Cell &k, const 
 // Orbit state of produce_orbit_response_field_mod (orbit_response.c:170-209)
 struct OrbitState {
   double x[3], v[3], a[3];
-  double tall, timespan, radsign_previous, E0;
+  double tall, timespan, E0;
+  bool rad_in;  // radsign_previous < 0: all the reference reads of it
   Cell cell;
   Proj proj;
   long long steps;
@@ -393,7 +394,7 @@ __device__ __forceinline__ void orbit_begin(const DevModel &M, const LogConsts &
   }
   s.tall = 0;
   s.timespan = timespan;
-  s.radsign_previous = 0;
+  s.rad_in = false;
   s.norbit = 0;
   s.flag = 0;
   s.steps = 0;
@@ -442,8 +443,8 @@ __device__ __forceinline__ bool orbit_step(const DevModel &M, const LogConsts &L
   sink(make_deposit(dt, s.cell, s.proj));
   s.tall += dt;
   double radsign = s.v[0] * s.x[0] + s.v[1] * s.x[1] + s.v[2] * s.x[2];
-  if(radsign > 0 && s.radsign_previous < 0) s.norbit++;
-  s.radsign_previous = radsign;
+  if(radsign > 0 && s.rad_in) s.norbit++;
+  s.rad_in = radsign < 0;
   s.steps++;
   if(!(s.tall == s.tall) || !(dt == dt)) {
     s.status = ORBIT_NONFINITE;
@@ -463,6 +464,16 @@ __device__ __forceinline__ double orbit_energy_error(const DevModel &M, const Lo
 {
   double E1 = 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]) + forcegrid_pot(M, L, s.x);
   return gm_fabs((E1 - s.E0) / s.E0);
+}
+// the same, with E0 formed again from the orbit's initial position and
+// velocity (orbit_begin's expression, so the same value), for kernels that
+// would rather not hold E0 for the whole orbit
+__device__ __forceinline__ double orbit_energy_error_from(const DevModel &M, const LogConsts &L, const OrbitState &s,
+                                                          const double *pos0, const double *vel0)
+{
+  const double E0 = 0.5 * (vel0[0] * vel0[0] + vel0[1] * vel0[1] + vel0[2] * vel0[2]) + forcegrid_pot(M, L, pos0);
+  double E1 = 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]) + forcegrid_pot(M, L, s.x);
+  return gm_fabs((E1 - E0) / E0);
 }
 
 // calc_disp_components_for_particle (disp_fields.c:200-372); out = vr2, vt2, vp2, vq2

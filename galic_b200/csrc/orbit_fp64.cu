@@ -108,7 +108,7 @@ struct NodeSink64 {
   WarpQueueT<PER, double> *q;
   int lane, Nb;
   int cnt;  // records parked in this lane's column since the last drain
-  int cur, cur_iR, cur_iz;
+  int cur_iR, cur_iz;  // the current cell; cur_iz < 0: none
   double a[4][5];
   // fac x 2^(shift - 24) of the mass and the energy fields (exact scalings)
   __device__ __forceinline__ void set_orbit(int gbase, double scale_m, double scale_e)
@@ -116,7 +116,7 @@ struct NodeSink64 {
     q->gbase[lane] = gbase;
     q->scale[0][lane] = scale_m;
     q->scale[1][lane] = scale_e;
-    cur = -1;
+    cur_iz = -1;
   }
   // slot s of cell (iz, iR) holds node (iz + node_dz(s, iz), iR + node_dr(s, iR))
   __device__ __forceinline__ static int node_dz(int s, int iz) { return ((s >> 1) ^ iz) & 1; }
@@ -145,15 +145,15 @@ struct NodeSink64 {
   }
   __device__ __forceinline__ void park()
   {
-    if(cur < 0) return;
+    if(cur_iz < 0) return;
     const bool all[4] = {true, true, true, true};
     park_masked(all);
-    cur = -1;
+    cur_iz = -1;
   }
   __device__ __forceinline__ void move_to(int iR, int iz)
   {
     bool out[4];
-    if(cur >= 0) {
+    if(cur_iz >= 0) {
       // along one axis a move by d leaves the node whose parity is that of
       // the boundary left behind, both nodes when |d| > 1, none when d = 0
       const int dz = iz - cur_iz, dr = iR - cur_iR;
@@ -171,13 +171,12 @@ struct NodeSink64 {
     for(int s = 0; s < 4; s++)
 #pragma unroll
       for(int f = 0; f < 5; f++) a[s][f] = out[s] ? 0.0 : a[s][f];
-    cur = iz * Nb + iR;
     cur_iR = iR;
     cur_iz = iz;
   }
   __device__ __forceinline__ void operator()(const Deposit &d)
   {
-    if(d.iz * Nb + d.iR != cur) move_to(d.iR, d.iz);
+    if(d.iz != cur_iz || d.iR != cur_iR) move_to(d.iR, d.iz);
     // slot s holds corner (dz, dr) = ((s >> 1) ^ (iz & 1), (s & 1) ^ (iR & 1));
     // corner weights: (0,0) m00, (0,1) m10, (1,0) m01, (1,1) m11
     const bool oz = d.iz & 1, orr = d.iR & 1;
@@ -213,6 +212,17 @@ template <int MINB>
 __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(DevModel M, CalcAllArgs A)
 {
   __shared__ WarpQueueT<kPer64, double> queues[CALC_ALL_BLOCK_FP64 / 32];
+  // the CTA's step count, largest energy error (as bits: non-negative
+  // doubles order like them) and worst status, added to at each orbit's end
+  // instead of being held in every thread's registers
+  __shared__ unsigned long long cta_steps, cta_err_bits;
+  __shared__ int cta_status;
+  if(threadIdx.x == 0) {
+    cta_steps = 0;
+    cta_err_bits = 0;
+    cta_status = 0;
+  }
+  __syncthreads();
   LogConsts L = step_log_consts(M);
   const int G = M.DG_Ngrid;
   OrbitState s;
@@ -220,12 +230,9 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(Dev
   sink.q = &queues[threadIdx.x >> 5];
   sink.lane = threadIdx.x & 31;
   sink.Nb = M.DG_Nbin;
-  sink.cur = -1;
+  sink.cur_iz = -1;
   sink.cnt = 0;
   int p = -1;
-  unsigned long long my_steps = 0;
-  double my_err = 0;
-  int my_status = 0;
 
   // fetch the next orbit for this lane; returns false when none is left
   auto fetch = [&]() -> bool {
@@ -258,21 +265,24 @@ __global__ void __launch_bounds__(CALC_ALL_BLOCK_FP64, MINB) k_calc_all_fp64(Dev
     } else if(state == LANE_FINISH) {
       sink.park();
       A.orbits[p] = s.norbit;
-      my_steps += (unsigned long long) s.steps;
+      atomicAdd(&cta_steps, (unsigned long long) s.steps);
       if(s.status != ORBIT_OK)
-        my_status = max(my_status, s.status);
+        atomicMax(&cta_status, s.status);
       else {
-        double e = orbit_energy_error(M, L, s);
-        if(e > my_err) my_err = e;
+        const double e = orbit_energy_error_from(M, L, s, &A.pos[3 * p], &A.vel[3 * p]);
+        if(e >= 0) atomicMax(&cta_err_bits, (unsigned long long) __double_as_longlong(e));
       }
       state = LANE_START;
     } else if(state == LANE_START) {
       state = fetch() ? LANE_ACTIVE : LANE_DONE;
     }
   }
-  if(my_steps) atomicAdd(A.steps_total, my_steps);
-  atomic_max_nonneg(A.max_egy_err, my_err);
-  if(my_status) atomicMax(A.status, my_status);
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    if(cta_steps) atomicAdd(A.steps_total, cta_steps);
+    atomic_max_nonneg(A.max_egy_err, __longlong_as_double((long long) cta_err_bits));
+    if(cta_status) atomicMax(A.status, cta_status);
+  }
 }
 
 // main.c:226-229 for every particle: vdisp = projections of the current
