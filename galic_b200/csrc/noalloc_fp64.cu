@@ -228,6 +228,9 @@ extern "C" int galic_orbit_responses_noalloc(const galic_params_t *prm, const do
     return GALIC_ERR_INVALID_ARGUMENT;
   if(prm->DG_MaxLevel != prm->EG_MaxLevel || prm->DG_MaxLevel < 1 || prm->FG_Nbin < 2 || !(prm->Halo_Mass > 0))
     return GALIC_ERR_INVALID_ARGUMENT;
+  if(!(prm->FG_Rmin > 0) || !(prm->FG_Fac > 1) || !(prm->DG_Rmin > 0) || !(prm->DG_Fac > 1) || !(prm->EG_Rmin > 0) ||
+     !(prm->EG_Fac > 1))
+    return GALIC_ERR_INVALID_ARGUMENT;
   const int L = prm->DG_MaxLevel;
   if(L > 7) return GALIC_ERR_BUDGET;  // 4^L bins per grid must fit the fixed scratch array
   const int G = 1 << (2 * L);
