@@ -34,7 +34,7 @@ FLOP_PER_STEP = 365  # algorithmic FP ops per orbit-step (orbit_response.c:211-4
 # DRAM bytes per orbit of the orbit kernels (ncu, one launch at 0.1 of the
 # workload's particles; the count scales with the orbits: particle state in,
 # orbit counts out, the grids and tables stay in L2)
-KERNEL_DRAM_BYTES_PER_ORBIT = {"k_calc_all_fp64": (13.078016e6 + 0.55552e6) / 120_000,
+KERNEL_DRAM_BYTES_PER_ORBIT = {"k_calc_all_fp64": (12.605952e6 + 0.0) / 120_000,
                                "k_calc_all_fp32": (16.947712e6 + 0.0) / 120_000}
 REF_BUILD = "-O3 -march=native (its Makefile.template flags), one single-rank process per host core"
 WORKLOAD = "halo+disk: Hernquist halo M=95 a=30 N=1e6 + exp disk M=5 h=3.5 z0=0.7 N=2e5, 128x128 DG/EG, 256^2 FG"
