@@ -23,40 +23,69 @@ struct DenseSink {
   double *m, *r, *t, *q, *p;
   int Nb;
   int with_egy;
-  // bin += value for the 4 corners of the deposit's cell in each grid, in the
-  // reference's order per bin; the 4 corner bins are distinct and the 5
-  // grids are separate arrays, so all loads are issued before the adds and
-  // stores (their latencies overlap instead of following one another)
+  // The bins of the cell the orbit is in, held in registers: c[f][corner]
+  // for corners 00, 10, 01, 11.  A deposit adds to them in the reference's
+  // order per bin (bin += value); when a deposit falls in another cell the
+  // held bins are stored and the new cell's bins loaded (a bin two cells
+  // share is stored before it is loaded again), and finish() stores the
+  // last cell's.  Each orbit's grids are its own, so every bin receives the
+  // reference's sequence of roundings, and the thread waits for the grid
+  // only when the orbit changes cell instead of at every deposit.
+  int cur = -1;  // grid index of the held cell's corner 00; -1: none
+  double c[5][4];
+  __device__ __forceinline__ double *field(int f) const
+  {
+    return f == 0 ? m : f == 1 ? r : f == 2 ? t : f == 3 ? q : p;
+  }
+  __device__ __forceinline__ void store_cell()
+  {
+    const int idx[4] = {cur, cur + 1, cur + Nb, cur + Nb + 1};
+    const int nf = with_egy ? 5 : 1;
+#pragma unroll
+    for(int f = 0; f < 5; f++)
+      if(f < nf) {
+        double *g = field(f);
+#pragma unroll
+        for(int k = 0; k < 4; k++) g[idx[k]] = c[f][k];
+      }
+  }
+  __device__ __forceinline__ void load_cell(int i00)
+  {
+    const int idx[4] = {i00, i00 + 1, i00 + Nb, i00 + Nb + 1};
+    const int nf = with_egy ? 5 : 1;
+#pragma unroll
+    for(int f = 0; f < 5; f++)
+      if(f < nf) {
+        const double *g = field(f);
+#pragma unroll
+        for(int k = 0; k < 4; k++) c[f][k] = g[idx[k]];
+      }
+    cur = i00;
+  }
   __device__ __forceinline__ void operator()(const Deposit &d)
   {
-    const int i00 = d.iz * Nb + d.iR, i10 = d.iz * Nb + (d.iR + 1);
-    const int i01 = (d.iz + 1) * Nb + d.iR, i11 = (d.iz + 1) * Nb + (d.iR + 1);
-    const int idx[4] = {i00, i10, i01, i11};
-    const double w[4] = {d.m00, d.m10, d.m01, d.m11};
-    double vm[4];
-#pragma unroll
-    for(int c = 0; c < 4; c++) vm[c] = m[idx[c]];
-    if(with_egy) {
-      double vr[4], vt[4], vq[4], vp[4];
-#pragma unroll
-      for(int c = 0; c < 4; c++) {
-        vr[c] = r[idx[c]];
-        vt[c] = t[idx[c]];
-        vq[c] = q[idx[c]];
-        vp[c] = p[idx[c]];
-      }
-#pragma unroll
-      for(int c = 0; c < 4; c++) {
-        m[idx[c]] = vm[c] + w[c];
-        r[idx[c]] = vr[c] + w[c] * d.p.vr2;
-        t[idx[c]] = vt[c] + w[c] * d.p.vt2;
-        q[idx[c]] = vq[c] + w[c] * d.p.vq2;
-        p[idx[c]] = vp[c] + w[c] * d.p.vp2;
-      }
-    } else {
-#pragma unroll
-      for(int c = 0; c < 4; c++) m[idx[c]] = vm[c] + w[c];
+    const int i00 = d.iz * Nb + d.iR;
+    if(i00 != cur) {
+      if(cur >= 0) store_cell();
+      load_cell(i00);
     }
+    const double w[4] = {d.m00, d.m10, d.m01, d.m11};
+#pragma unroll
+    for(int k = 0; k < 4; k++) c[0][k] = c[0][k] + w[k];
+    if(with_egy) {
+#pragma unroll
+      for(int k = 0; k < 4; k++) {
+        c[1][k] = c[1][k] + w[k] * d.p.vr2;
+        c[2][k] = c[2][k] + w[k] * d.p.vt2;
+        c[3][k] = c[3][k] + w[k] * d.p.vq2;
+        c[4][k] = c[4][k] + w[k] * d.p.vp2;
+      }
+    }
+  }
+  __device__ __forceinline__ void finish()
+  {
+    if(cur >= 0) store_cell();
+    cur = -1;
   }
 };
 
@@ -73,6 +102,7 @@ __global__ void k_orbits_dense(DevModel M, OrbitBatch b)
   orbit_begin(M, L, s, &b.pos[3 * k], &b.vel[3 * k], b.timespan[k], b.type[k], b.with_egy != 0);
   while(orbit_step(M, L, s, b.with_egy != 0, sink)) {
   }
+  sink.finish();
   b.tall[k] = s.tall;
   b.norbit[k] = s.norbit;
   b.steps[k] = s.steps;
