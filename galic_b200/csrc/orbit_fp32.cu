@@ -640,7 +640,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_ensemble_fp32(const __grid_cons
 }
 
 // Dense sink of one orbit: the node sums of NodeAcc, added into the orbit's
-// own FP64 grids [5][Ngrid] when their node leaves the current cell.
+// own FP64 grids [5][Ngrid] when their node leaves the current cell, as
+// reductions that return nothing (the thread does not wait for the grid's
+// lines; one thread's reductions to one address apply in program order, so
+// the bins are those of a load-add-store).
 struct DenseSink32 : NodeAcc {
   double *grid;
   int G, Nb;
@@ -652,7 +655,7 @@ struct DenseSink32 : NodeAcc {
       const int node = (cur_iz + node_dz(s, cur_iz)) * Nb + cur_iR + node_dr(s, cur_iR);
 #pragma unroll
       for(int f = 0; f < 5; f++)
-        if(a[s][f] != 0.f) grid[(size_t) f * G + node] += (double) a[s][f];
+        if(a[s][f] != 0.f) atomicAdd(&grid[(size_t) f * G + node], (double) a[s][f]);
     }
   }
   __device__ __forceinline__ void flush()
