@@ -51,6 +51,31 @@ def test_params_validation_before_device():
         assert lib.galic_ctx_create(C.byref(p), C.byref(h)) == 4  # GALIC_ERR_NO_DEVICE
 
 
+def test_noalloc_validation_before_device():
+    """The allocation-free entry point rejects bad grid parameters before it
+    touches a device, as galic_ctx_create does (the pointers are never read)."""
+    lib = _ffi.load_library()
+    p, _, _ = synth.make_params([synth.Component("halo", 100.0, 30.0, 100)], level=6, fg_nbin=64)
+    dummy = (C.c_double * 8)()
+    d = C.addressof(dummy)
+
+    def call(prm):
+        return lib.galic_orbit_responses_noalloc(C.byref(prm), d, d, d, d, 1.0, 0, None, None, None, None, None, d,
+                                                 None, None)
+
+    for field, value in (("FG_Rmin", 0.0), ("DG_Rmin", -1.0), ("EG_Rmin", float("nan")), ("FG_Fac", 1.0),
+                         ("DG_Fac", 0.5), ("EG_Fac", 1.0)):
+        bad = p.copy()
+        setattr(bad, field, value)
+        assert call(bad) == 1, field  # GALIC_ERR_INVALID_ARGUMENT
+    bad = p.copy()
+    bad.EG_MaxLevel = 5
+    assert call(bad) == 1
+    big = p.copy()
+    big.DG_MaxLevel = big.EG_MaxLevel = 8
+    assert call(big) == 5  # GALIC_ERR_BUDGET: beyond the fixed scratch array
+
+
 @pytest.mark.parametrize("outer,inner,fg,L", [(0.980296, 9.80296e-5, 256, 6), (0.49, 1e-7, 256, 7),
                                               (0.999, 1e-7, 256, 7), (0.9, 1e-4, 64, 5)])
 def test_grid_geometry_matches_oracle(outer, inner, fg, L):
